@@ -1,0 +1,354 @@
+"""Benchmark of the OLAP-core star-join on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one star-join query (4-dimension probe, group-by SUM(m1) and
+SUM(m1*m2) in int64) over the whole device-resident fact table of this rank:
+600,000,000 rows x (4 int32 FKs + 2 int32 measures) = 14.4 GB per GPU,
+dimensions of 3,000,000 / 200,000 / 1,400,000 / 2,556 rows (selectivity
+0.5/0.2/0.1/1.0, 8 groups each: 4096 groups, joint selectivity 0.01).  Inputs
+are larger than L2 (126 MB), so no flush is needed between steps.
+
+Under torchrun each rank holds its own 600M-row shard (weak scaling) and the
+step ends with the one real exchange of a distributed star-join: an NCCL
+all-reduce of the int64 group vector.  Time is measured with CUDA events on
+the launching stream and reduced as the max over ranks.
+
+``--impl reference`` times the reference's own CPU OLAPcore (compiled from
+its sources into oracle/_ref) on this host's cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "star-join fact rows/sec & HBM GB/s vs peak; queries/sec with p50/p99 latency"
+WORKLOAD = ("OLAP-core star-join at scale: 600M fact rows/GPU, 4 int32 FK + 2 int32 measures "
+            "(14.4 GB), dims 3,000,000/200,000/1,400,000/2,556, uniform FKs, per-dim selectivity "
+            "0.5/0.2/0.1/1.0 (joint 0.01), 8x8x8x8 = 4096 groups, int64 SUM(m1) and SUM(m1*m2)")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--rows", type=int, default=600_000_000)
+    ap.add_argument("--sele", type=float, nargs=4, default=[0.5, 0.2, 0.1, 1.0])
+    ap.add_argument("--groups", type=int, nargs=4, default=[8, 8, 8, 8])
+    ap.add_argument("--fk-dist", default="uniform", choices=["uniform", "zipf"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample-rows", type=int, default=100_000_000)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tune", type=str, default="", help="knob=value,... (olap_ctx_set_tuning)")
+    return ap.parse_args()
+
+
+DIM_SIZES = (3_000_000, 200_000, 1_400_000, 2_556)
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows: list[list[str]] = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                mhz.append(float(r[1]))
+                mx = float(r[2])
+                for name, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def measured_peak_gbs() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference's own OLAPcore on this host (bounded sample)
+# ---------------------------------------------------------------------------
+def cpu_reference(rows: int, sele, groups, steps: int, warmup: int, seed: int = 42) -> dict:
+    """Time the reference's OLAPcore_vwm_sv (all host threads) on a sample of
+    the workload; returns the cpu_baseline dict (rows/s)."""
+    import ctypes as C
+    import numpy as np
+    import oracle
+    from memory_database_b200 import workloads
+    cores = os.cpu_count() or 1
+    s = workloads.host_star_schema(rows, DIM_SIZES, sele, groups, seed=seed)
+    kind = "reference" if oracle.ref_available() else "port"
+    nd, G = s.dimvec_nums, s.group_nums
+    o = np.array(s.orders + [0] * (4 - nd), np.int32)
+    f = np.array(s.factor + [0] * (4 - nd), np.int32)
+    if kind == "reference":
+        ref = oracle.ref_lib()
+        dva, fka = oracle._ptr_array(s.dimvec), oracle._ptr_array(s.fk)
+
+        def run():
+            return ref.ref_OLAPcore_vwm_sv(dva, fka, oracle._p(o), nd, oracle._p(f), rows, G,
+                                           oracle._p(s.m1), oracle._p(s.m2), cores)
+        threads = cores
+        what = "OLAPcore_vwm_sv (reference source, -O3 -march=native)"
+    else:
+        def run():
+            return oracle.starjoin(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G)
+        threads = 1
+        what = "oracle restatement (single thread)"
+    for _ in range(warmup):
+        run()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        run()
+    dt = (time.perf_counter() - t0) / steps
+    return {"value": rows / dt, "unit": "rows/s", "cores": threads, "kind": kind,
+            "sample": f"{rows:,} rows of the same workload ({what}), {steps} timed runs after {warmup} warm-up",
+            "ms_per_step": dt * 1e3}
+
+
+def run_reference_arm(a) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    rows = min(a.rows, a.cpu_sample_rows)
+    cb = cpu_reference(rows, a.sele, a.groups, max(1, a.steps), max(1, a.warmup))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "rows/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": cb["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded counter-based generator)",
+        "config": {"workload": WORKLOAD, "rows_timed_per_step": rows},
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def main() -> None:
+    a = parse()
+    if a.impl == "reference":
+        run_reference_arm(a)
+        return
+    import torch
+    import torch.distributed as dist
+    from memory_database_b200 import _lib, olapcore, workloads
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    ctx = olapcore.Context(local, scratch_bytes=512 << 20)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream)
+    for kv in filter(None, a.tune.split(",")):
+        k, v = kv.split("=")
+        ctx.set_tuning(int(k), int(v))
+
+    s = workloads.make_star_schema(ctx, a.rows, DIM_SIZES, a.sele, a.groups, fk_dist=a.fk_dist,
+                                   seed=42 + rank)
+    aggs = (olapcore.AGG_M1, olapcore.AGG_M1_TIMES_M2)
+    G = s.group_nums
+    gs = torch.empty((2, G), dtype=torch.int64, device="cuda")
+    tot = torch.empty((2,), dtype=torch.int64, device="cuda")
+
+    def step():
+        olapcore.starjoin_groupsum(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,
+                                   dimvec_lens=s.probe_lens, ctx=ctx, out=gs, totals_out=tot)
+        if world > 1:
+            dist.all_reduce(gs)
+
+    for _ in range(max(3, a.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for k in range(a.steps):
+            ev[k][0].record()
+            olapcore.starjoin_groupsum(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G,
+                                       aggs=aggs, dimvec_lens=s.probe_lens, ctx=ctx, out=gs,
+                                       totals_out=tot)
+            ev[k][1].record()
+            if world > 1:
+                dist.all_reduce(gs)
+        t1.record()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    elapsed_ms = t0.elapsed_time(t1)
+    kernel_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+    if world > 1:
+        t = torch.tensor([elapsed_ms, kernel_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms, kernel_ms = t.tolist()
+    ms_per_step = elapsed_ms / a.steps
+    rows_all = a.rows * world * a.steps
+    value = rows_all / (elapsed_ms / 1e3)
+
+    algo_bytes = a.rows * s.bytes_per_row(2)
+    peak, peak_src = measured_peak_gbs()
+    achieved = algo_bytes / (kernel_ms / 1e3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "starjoin_traffic.json"
+    if prof.exists():
+        try:
+            tr = json.loads(prof.read_text())
+            traffic = tr["bytes_per_row"] * a.rows if tr.get("workload") == WORKLOAD else None
+        except Exception:
+            traffic = None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": a.steps,
+        "warmup": max(3, a.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded counter-based generator, generated in HBM)",
+        "config": {"workload": WORKLOAD, "rows_per_gpu": a.rows, "dim_sizes": list(DIM_SIZES),
+                   "sele": a.sele, "groups": a.groups, "fk_dist": a.fk_dist,
+                   "group_nums": G, "l2": "inputs 14.4 GB/GPU > 126 MB L2; no flush",
+                   "parallelism": f"row shards x{world}" + (", NCCL all-reduce of group vector" if world > 1 else "")},
+        "hbm_gbs": achieved,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_src} MEASURED_PEAKS.json hbm_gbs" if peak_src == "measured" else "fallback 6650 GB/s",
+                     "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms": kernel_ms},
+        "gpu_launches": a.steps,
+        "clocks": clk.summary(),
+    }
+
+    # e2e: the same query through the host-memory C-ABI entry point, with the
+    # fact table in pinned host memory; H2D copies and the D2H of the group
+    # sums are inside the timed region.
+    if not a.no_e2e:
+        line["e2e"] = e2e_host(a, s, ctx, aggs, world)
+        line["gpu_launches"] = a.steps + line["e2e"].pop("_launches")
+    if rank == 0 and world == 1 and not a.no_cpu:
+        try:
+            cb = cpu_reference(min(a.rows, a.cpu_sample_rows), a.sele, a.groups, 3, 1)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as e:  # the baseline is reported, never the target
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def e2e_host(a, s, ctx, aggs, world) -> dict:
+    import ctypes as C
+    import numpy as np
+    import torch
+    from memory_database_b200 import _lib, olapcore
+    n = a.rows
+    pin = [torch.empty(n, dtype=torch.int32, pin_memory=True) for _ in range(4)]
+    pm1 = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    pm2 = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    for t in range(4):
+        pin[t].copy_(s.fk[t])
+    pm1.copy_(s.m1)
+    pm2.copy_(s.m2)
+    dims_host = [d.cpu().numpy() for d in s.dimvec]
+    G = s.group_nums
+    hctx = olapcore.Context(ctx.device, scratch_bytes=1 << 30)
+
+    def run():
+        # the public call with host (pinned) buffers: olap_starjoin_groupsum_host
+        return olapcore.starjoin_groupsum([dims_host[t] for t in s.orders], [pin[t] for t in s.orders],
+                                          s.factor, pm1, pm2, G, aggs=aggs,
+                                          dimvec_lens=[DIM_SIZES[t] for t in s.orders], ctx=hctx)
+
+    run()
+    steps = max(1, a.e2e_steps)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        run()
+    dt = (time.perf_counter() - t0) / steps
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt = t.item()
+    chunk = 1 << 22
+    nchunks = (n + chunk - 1) // chunk
+    h2d = n * 4 * (s.dimvec_nums + 2) + sum(DIM_SIZES[t] for t in s.orders)
+    hctx.close()
+    return {"value": n * world / dt, "unit": "rows/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": 8 * 2 * G + 16, "ms_per_step": dt * 1e3, "steps": steps,
+            "path": "olap_starjoin_groupsum_host, pinned host columns, chunked H2D overlapped with the scan",
+            "_launches": steps * nchunks}
+
+
+if __name__ == "__main__":
+    main()

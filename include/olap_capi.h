@@ -1,0 +1,185 @@
+/*
+ * olap_capi.h — C-ABI of the B200 (sm_100a) OLAP-core library
+ * (libolapcore_b200.so).
+ *
+ * The reference (panjd123/memory_database) exposes its operators as free C++
+ * functions with raw column pointers, C++ linkage and overloaded names.  This
+ * header exposes the same computations with distinct C names, plain pointers
+ * and sizes, and an int status instead of exit().  Each entry point names the
+ * reference function it replaces (path:line inside the reference project).
+ *
+ * Conventions
+ *  - Every call takes an olap_ctx (device, stream, scratch arena).  Calls with
+ *    device pointers are stream-ordered on the context's stream and return
+ *    once the work is enqueued, unless documented as synchronous.
+ *  - Entry points whose name ends in _host take host pointers and are
+ *    synchronous; they stream the columns through the GPU themselves.
+ *  - Sums are int64 (the reference accumulates uint32 and returns int; the
+ *    int64 result equals the reference's modulo 2^32).
+ *  - Status: OLAP_OK (0) or a negative OLAP_ERR_* code; olap_ctx_last_error()
+ *    returns the message of the last failure on a context.
+ *  - There is no CPU fallback: without a usable CUDA device every compute call
+ *    fails with OLAP_ERR_NO_DEVICE.
+ */
+#ifndef OLAP_CAPI_H
+#define OLAP_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define OLAP_API __attribute__((visibility("default")))
+#else
+#define OLAP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Sentinels and sizes shared with the reference (include/metadata.h). */
+#define OLAP_DIM_NULL 127      /* metadata.h:69  DIM_NULL = INT8_MAX            */
+#define OLAP_GROUP_NULL 32767  /* metadata.h:70  GROUP_NULL = INT16_MAX         */
+#define OLAP_VECTOR_SIZE 1024  /* metadata.h:68  size_v (vector-wise chunk)     */
+#define OLAP_MAX_DIMS 4        /* customer, supplier, part, date (metadata.h:288) */
+
+/* Status codes. */
+#define OLAP_OK 0
+#define OLAP_ERR_INVALID (-1)     /* bad argument                                  */
+#define OLAP_ERR_CUDA (-2)        /* CUDA runtime error                            */
+#define OLAP_ERR_NO_DEVICE (-3)   /* no usable CUDA device                         */
+#define OLAP_ERR_NOMEM (-4)       /* device or pinned allocation failed            */
+#define OLAP_ERR_RANGE (-5)       /* rows dropped: fk or group id out of range     */
+#define OLAP_ERR_CAPACITY (-6)    /* scratch arena or table capacity exceeded      */
+#define OLAP_ERR_TIMEOUT (-7)     /* a bounded device wait expired                 */
+#define OLAP_ERR_UNSUPPORTED (-8) /* shape not supported by this build             */
+
+/* Aggregate expressions of the star-join (per surviving fact row). */
+#define OLAP_AGG_M1_PLUS_M2 0  /* M1 + M2: the reference's SUM (cpp:360, :428) */
+#define OLAP_AGG_M1 1
+#define OLAP_AGG_M2 2
+#define OLAP_AGG_M1_TIMES_M2 3 /* 64-bit product                               */
+#define OLAP_AGG_COUNT 4
+
+/* Tuning knobs (olap_ctx_set_tuning); 0 restores the automatic choice. */
+#define OLAP_TUNE_BLOCK_THREADS 0   /* threads per block of the scan kernels     */
+#define OLAP_TUNE_BLOCKS_PER_SM 1   /* resident blocks per SM (persistent grid)  */
+#define OLAP_TUNE_SMEM_DIM_BYTES 2  /* bytes of dimension vectors staged in smem */
+#define OLAP_TUNE_SMEM_ACC_BYTES 3  /* bytes of group accumulators kept in smem  */
+#define OLAP_TUNE_HOST_CHUNK_ROWS 4 /* rows per H2D chunk of the _host calls     */
+#define OLAP_TUNE_UNROLL 5          /* 4-row groups in flight per thread (1, 2)  */
+
+typedef struct olap_ctx olap_ctx;
+
+/* ---- context ---------------------------------------------------------------
+ * A context binds one device, one stream (its own unless set), a device
+ * scratch arena (scratch_bytes, 0 = 64 MiB) and a pinned host staging buffer
+ * for the _host entry points.  Calls on one context are serialised by a
+ * mutex; use one context per host thread for concurrent submission. */
+OLAP_API int olap_ctx_create(int device, size_t scratch_bytes, olap_ctx** out);
+OLAP_API int olap_ctx_destroy(olap_ctx* ctx);
+OLAP_API int olap_ctx_set_stream(olap_ctx* ctx, void* cuda_stream); /* NULL = own stream */
+OLAP_API void* olap_ctx_get_stream(olap_ctx* ctx);
+OLAP_API int olap_ctx_synchronize(olap_ctx* ctx);
+OLAP_API int olap_ctx_set_tuning(olap_ctx* ctx, int knob, int64_t value);
+/* Synchronises, returns and clears the count of rows that kernels dropped
+ * because an fk or a group id was out of range. */
+OLAP_API int olap_ctx_take_range_errors(olap_ctx* ctx, int64_t* count);
+OLAP_API const char* olap_ctx_last_error(const olap_ctx* ctx);
+OLAP_API const char* olap_status_string(int status);
+/* Number of CUDA devices (0 when none; never fails). */
+OLAP_API int olap_device_count(void);
+/* Library build identification ("sm_100a ..."). */
+OLAP_API const char* olap_build_info(void);
+
+/* ---- star-join with multidimensional group-by SUM (the hot path) ---------
+ *
+ * Replaces the fused row-wise / vector-wise OLAP core:
+ *   OLAPcore_rowwise  code/OLAPcore/test_multi_compute_operator.cpp:973-1037
+ *   OLAPcore_vwm_dv   code/OLAPcore/test_multi_compute_operator.cpp:1052-1126
+ *   OLAPcore_vwm_sv   code/OLAPcore/test_multi_compute_operator.cpp:1258-1327
+ * All three compute, for every fact row r in [row_begin, row_end):
+ *   g = sum_j dimvec[j][fk[j][r]] * factor[j]   (dropped if any code is DIM_NULL)
+ *   group_sums[a][g] += agg_a(M1[r], M2[r])
+ * with j over the dimensions in probe order (dimvec[j] is the reference's
+ * dimvec_array[orders[j]]).  Semantics follow OLAPcore_vwm_sv_thread
+ * (cpp:509-568): measures are read at the row's own position.  A row whose fk
+ * is outside [0, dimvec_len[j]) or whose g is outside [0, group_nums) is
+ * dropped and counted as a range error (the reference reads out of bounds). */
+typedef struct olap_starjoin_query {
+  int32_t dimvec_nums;                    /* participating dimensions, 0..4   */
+  int32_t n_aggs;                         /* aggregates per group, 1..2       */
+  int32_t agg[2];                         /* OLAP_AGG_*                       */
+  const int8_t* dimvec[OLAP_MAX_DIMS];    /* int8 group code or DIM_NULL      */
+  int64_t dimvec_len[OLAP_MAX_DIMS];      /* readable entries of dimvec[j]    */
+  const int32_t* fk[OLAP_MAX_DIMS];       /* foreign-key column of dim j      */
+  int32_t factor[OLAP_MAX_DIMS];          /* group-id weight of dim j         */
+  const int32_t* m1;                      /* measure columns (unused: NULL)   */
+  const int32_t* m2;
+  int64_t row_begin;                      /* fact range [row_begin, row_end)  */
+  int64_t row_end;
+  int64_t group_nums;                     /* groups: ids in [0, group_nums)   */
+} olap_starjoin_query;
+
+/* Device pointers; asynchronous on the context stream.  group_sums
+ * ([n_aggs][group_nums], row-major) and totals ([n_aggs]) are overwritten;
+ * either may be NULL when not wanted. */
+OLAP_API int olap_starjoin_groupsum(olap_ctx* ctx, const olap_starjoin_query* q,
+                           int64_t* group_sums, int64_t* totals);
+
+/* Host pointers; synchronous.  The fact columns are streamed through the GPU
+ * in pinned chunks with copies overlapped with the scan.  A dimvec_len[j] of
+ * 0 means "unknown": the library then copies dimvec[j][0 .. max fk] (the
+ * bytes the reference itself would read).  Returns OLAP_ERR_RANGE (results
+ * still written) when rows were dropped. */
+OLAP_API int olap_starjoin_groupsum_host(olap_ctx* ctx, const olap_starjoin_query* q,
+                                int64_t* group_sums, int64_t* totals);
+
+/* Reference-layout entry point, device pointers, synchronous.
+ * dimvec_array / fk_array are host arrays of 4 device pointers indexed by
+ * table (0 customer, 1 supplier, 2 part, 3 date); orders[0..dimvec_nums)
+ * names the tables in probe order and factor[j] belongs to orders[j], exactly
+ * as the reference's main builds them (cpp:1964-1987).  dimvec_len may be
+ * NULL (then every fk must be trusted by the caller: no range check beyond
+ * 2^31).  *count receives the grand total of M1+M2 over all groups (the
+ * reference's return value); group_vector (device, [group_nums]) may be NULL. */
+OLAP_API int olap_OLAPcore(olap_ctx* ctx, int8_t* const* dimvec_array, const int64_t* dimvec_len,
+                  int32_t* const* fk_array, const int* orders, int dimvec_nums,
+                  const int* factor, int64_t size_lineorder, int64_t group_nums,
+                  const int32_t* M1, const int32_t* M2, int64_t* group_vector,
+                  int64_t* count);
+
+/* Plan of the reference's main (cpp:1937-1987): dimensions with groups > 0
+ * participate; orders is sorted by sort_by_rate (cpp:223-233, including its
+ * comparison of sele[i] with sele[j] by position); group_nums = prod groups;
+ * factor[j] = prod_{k>j} groups[orders[k]] when bitmap[orders[j]] != 0, else 1.
+ * Host-only, no device needed. */
+OLAP_API int olap_plan_olapcore(const double sele[4], const int bitmap[4], const int groups[4],
+                       int orders[4], int factor[4], int* dimvec_nums, int64_t* group_nums);
+
+/* ---- seeded synthetic data (counter-based; identical on host and device) --
+ * Value i of stream s under seed k is a pure function of (k, s, i), so any
+ * slice can be generated anywhere.  _dev variants write device memory on the
+ * context stream; the plain variants write host memory with nthreads threads
+ * (0 = all cores). */
+OLAP_API int olap_gen_uniform_i32_dev(olap_ctx* ctx, int32_t* out, int64_t n, uint64_t seed,
+                             uint64_t stream, int32_t lo, int32_t hi);
+OLAP_API int olap_gen_uniform_i32(int32_t* out, int64_t n, uint64_t seed, uint64_t stream,
+                         int32_t lo, int32_t hi, int nthreads);
+/* Zipf(s) keys in [0, n_keys): P(k) proportional to 1/(k+1)^s. */
+OLAP_API int olap_gen_zipf_i32_dev(olap_ctx* ctx, int32_t* out, int64_t n, uint64_t seed,
+                          uint64_t stream, int64_t n_keys, double s);
+OLAP_API int olap_gen_zipf_i32(int32_t* out, int64_t n, uint64_t seed, uint64_t stream,
+                      int64_t n_keys, double s, int nthreads);
+/* Dimension vector: entry i is DIM_NULL with probability 1 - sele, else a
+ * group code uniform in [0, groups). */
+OLAP_API int olap_gen_dimvec_dev(olap_ctx* ctx, int8_t* out, int64_t n, uint64_t seed,
+                        uint64_t stream, double sele, int32_t groups);
+OLAP_API int olap_gen_dimvec(int8_t* out, int64_t n, uint64_t seed, uint64_t stream,
+                    double sele, int32_t groups, int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OLAP_CAPI_H */

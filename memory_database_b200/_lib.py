@@ -1,0 +1,126 @@
+"""ctypes binding of ``libolapcore_b200.so`` (the C-ABI in ``include/olap_capi.h``).
+
+The library is the only compute path: if it is missing this module raises at
+import, and every compute call raises :class:`OlapError` when the library
+reports a failure (there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libolapcore_b200.so"
+
+OLAP_OK = 0
+OLAP_ERR_INVALID = -1
+OLAP_ERR_CUDA = -2
+OLAP_ERR_NO_DEVICE = -3
+OLAP_ERR_NOMEM = -4
+OLAP_ERR_RANGE = -5
+OLAP_ERR_CAPACITY = -6
+OLAP_ERR_TIMEOUT = -7
+OLAP_ERR_UNSUPPORTED = -8
+
+DIM_NULL = 127
+GROUP_NULL = 32767
+VECTOR_SIZE = 1024
+MAX_DIMS = 4
+
+AGG_M1_PLUS_M2 = 0
+AGG_M1 = 1
+AGG_M2 = 2
+AGG_M1_TIMES_M2 = 3
+AGG_COUNT = 4
+
+TUNE_BLOCK_THREADS = 0
+TUNE_BLOCKS_PER_SM = 1
+TUNE_SMEM_DIM_BYTES = 2
+TUNE_SMEM_ACC_BYTES = 3
+TUNE_HOST_CHUNK_ROWS = 4
+TUNE_UNROLL = 5
+
+
+class OlapError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"olap status {status}: {message}")
+        self.status = status
+
+
+class StarjoinQuery(C.Structure):
+    """Mirror of ``olap_starjoin_query``."""
+
+    _fields_ = [
+        ("dimvec_nums", C.c_int32),
+        ("n_aggs", C.c_int32),
+        ("agg", C.c_int32 * 2),
+        ("dimvec", C.c_void_p * MAX_DIMS),
+        ("dimvec_len", C.c_int64 * MAX_DIMS),
+        ("fk", C.c_void_p * MAX_DIMS),
+        ("factor", C.c_int32 * MAX_DIMS),
+        ("m1", C.c_void_p),
+        ("m2", C.c_void_p),
+        ("row_begin", C.c_int64),
+        ("row_end", C.c_int64),
+        ("group_nums", C.c_int64),
+    ]
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m memory_database_b200.build` "
+            "(the CUDA library is the only compute path; there is no fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    vp, i32, i64, u64, f64 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64, C.c_double
+    sigs = {
+        "olap_ctx_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(vp)]),
+        "olap_ctx_destroy": (C.c_int, [vp]),
+        "olap_ctx_set_stream": (C.c_int, [vp, vp]),
+        "olap_ctx_get_stream": (vp, [vp]),
+        "olap_ctx_synchronize": (C.c_int, [vp]),
+        "olap_ctx_set_tuning": (C.c_int, [vp, C.c_int, i64]),
+        "olap_ctx_take_range_errors": (C.c_int, [vp, C.POINTER(i64)]),
+        "olap_ctx_last_error": (C.c_char_p, [vp]),
+        "olap_status_string": (C.c_char_p, [C.c_int]),
+        "olap_device_count": (C.c_int, []),
+        "olap_build_info": (C.c_char_p, []),
+        "olap_starjoin_groupsum": (C.c_int, [vp, C.POINTER(StarjoinQuery), vp, vp]),
+        "olap_starjoin_groupsum_host": (C.c_int, [vp, C.POINTER(StarjoinQuery), vp, vp]),
+        "olap_OLAPcore": (C.c_int, [vp, vp, vp, vp, vp, C.c_int, vp, i64, i64, vp, vp, vp,
+                                    C.POINTER(i64)]),
+        "olap_plan_olapcore": (C.c_int, [vp, vp, vp, vp, vp, C.POINTER(C.c_int), C.POINTER(i64)]),
+        "olap_gen_uniform_i32_dev": (C.c_int, [vp, vp, i64, u64, u64, i32, i32]),
+        "olap_gen_uniform_i32": (C.c_int, [vp, i64, u64, u64, i32, i32, C.c_int]),
+        "olap_gen_zipf_i32_dev": (C.c_int, [vp, vp, i64, u64, u64, i64, f64]),
+        "olap_gen_zipf_i32": (C.c_int, [vp, i64, u64, u64, i64, f64, C.c_int]),
+        "olap_gen_dimvec_dev": (C.c_int, [vp, vp, i64, u64, u64, f64, i32]),
+        "olap_gen_dimvec": (C.c_int, [vp, i64, u64, u64, f64, i32, C.c_int]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(status: int, ctx=None) -> int:
+    """Raise :class:`OlapError` for a negative status; return it otherwise."""
+    if status < 0:
+        msg = lib.olap_status_string(status).decode()
+        if ctx is not None:
+            detail = lib.olap_ctx_last_error(ctx).decode()
+            if detail:
+                msg = f"{msg}: {detail}"
+        raise OlapError(status, msg)
+    return status
+
+
+def device_count() -> int:
+    return int(lib.olap_device_count())
+
+
+def build_info() -> str:
+    return lib.olap_build_info().decode()

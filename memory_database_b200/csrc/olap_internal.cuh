@@ -1,0 +1,171 @@
+// Internal definitions shared by the sm_100a kernels and the C-ABI layer.
+//
+// Everything here is B200-specific: cache-policy hinted loads (streaming fact
+// columns are marked evict-first in L2 and are not allocated in L1, while the
+// small, randomly probed dimension vectors are marked evict-last), persistent
+// grids sized by the SM count, and a per-context scratch arena so that no
+// query allocates device memory on its hot path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include <mutex>
+#include <string>
+
+#include "olap_capi.h"
+
+namespace olap {
+
+// Per-context device scratch words.  Lives in the context's arena, zeroed at
+// creation; kernels add to the counters, host calls read-and-clear them.
+struct DeviceCounters {
+  unsigned long long range_errors;  // rows dropped: fk or group id out of range
+  unsigned long long wait_timeouts;  // bounded device waits that gave up
+  unsigned long long pad[14];
+};
+
+}  // namespace olap
+
+// The opaque context handle of the C-ABI.
+struct olap_ctx {
+  int device = 0;
+  int sm_count = 0;
+  int smem_optin = 0;          // max dynamic shared memory per block (bytes)
+  int64_t l2_bytes = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  // Scratch arena: one cudaMalloc at creation, bump-allocated per call and
+  // reset at the start of each call (calls on one context are stream-ordered).
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  olap::DeviceCounters* counters = nullptr;  // first bytes of the arena
+
+  // Pinned host staging used by the host-memory entry points.
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+
+  // Tuning knobs (0 = automatic); set by olap_ctx_set_tuning.
+  int64_t tune[16] = {0};
+
+  std::mutex mu;               // serialises calls that share this context
+  std::string last_error;
+};
+
+namespace olap {
+
+// Tuning knob indices (public values in olap_capi.h).
+enum {
+  TUNE_BLOCK = OLAP_TUNE_BLOCK_THREADS,
+  TUNE_BLOCKS_PER_SM = OLAP_TUNE_BLOCKS_PER_SM,
+  TUNE_SMEM_DIM_BYTES = OLAP_TUNE_SMEM_DIM_BYTES,
+  TUNE_SMEM_ACC_BYTES = OLAP_TUNE_SMEM_ACC_BYTES,
+  TUNE_CHUNK_ROWS = OLAP_TUNE_HOST_CHUNK_ROWS,
+  TUNE_UNROLL = OLAP_TUNE_UNROLL,
+};
+
+int set_error(olap_ctx* ctx, int status, const std::string& msg);
+int check_cuda(olap_ctx* ctx, cudaError_t e, const char* what);
+
+#define OLAP_CUDA_TRY(ctx, expr)                         \
+  do {                                                   \
+    cudaError_t _e = (expr);                             \
+    if (_e != cudaSuccess) return olap::check_cuda((ctx), _e, #expr); \
+  } while (0)
+
+#define OLAP_REQUIRE(ctx, cond, msg)                     \
+  do {                                                   \
+    if (!(cond)) return olap::set_error((ctx), OLAP_ERR_INVALID, (msg)); \
+  } while (0)
+
+// Bump allocator over the context arena.  Returns nullptr when the arena is
+// exhausted (the caller reports OLAP_ERR_CAPACITY).
+struct Arena {
+  char* base;
+  size_t cap;
+  size_t off;
+  explicit Arena(olap_ctx* c)
+      : base(c->arena), cap(c->arena_bytes), off(sizeof(DeviceCounters)) {}
+  template <class T>
+  T* take(size_t n) {
+    size_t a = (off + 255) & ~size_t(255);
+    size_t bytes = n * sizeof(T);
+    if (a + bytes > cap) return nullptr;
+    off = a + bytes;
+    return reinterpret_cast<T*>(base + a);
+  }
+};
+
+inline int64_t tune_or(const olap_ctx* c, int knob, int64_t dflt) {
+  return c->tune[knob] > 0 ? c->tune[knob] : dflt;
+}
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+
+// L2 cache policies.  Fact columns are read once per query: evict-first keeps
+// them from displacing the dimension vectors and group tables, which are
+// re-read at random and marked evict-last.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// 128-bit streaming load: read-only path, no L1 allocation, L2 evict-first.
+__device__ __forceinline__ int4 ld_stream_v4(const int32_t* p, uint64_t pol) {
+  int4 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_stream_s32(const int32_t* p, uint64_t pol) {
+  int32_t v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
+      : "=r"(v)
+      : "l"(p), "l"(pol));
+  return v;
+}
+// Random probe of a byte vector kept hot in L1/L2 (sign-extended like the
+// reference's `int idx_flag = dimvec[...]`).
+__device__ __forceinline__ int32_t ld_probe_s8(const int8_t* p, uint64_t pol) {
+  int32_t v;
+  asm("ld.global.nc.L2::cache_hint.s8 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_probe_s32(const int32_t* p, uint64_t pol) {
+  int32_t v;
+  asm("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
+// Exact 64-bit accumulation into shared memory with 32-bit atomics: the low
+// word is added atomically and its carry-out is forwarded to the high word.
+// Addition mod 2^64 is commutative, so the final pair is exact whatever the
+// interleaving.  Non-negative addends below 2^32 (the common case: measures,
+// counts) cost a single 32-bit atomic.
+__device__ __forceinline__ void smem_add_u64(unsigned long long* slot, uint64_t v) {
+  uint32_t* w = reinterpret_cast<uint32_t*>(slot);
+  uint32_t lo = static_cast<uint32_t>(v);
+  uint32_t hi = static_cast<uint32_t>(v >> 32);
+  uint32_t old = atomicAdd(w, lo);
+  hi += (old + lo) < old ? 1u : 0u;
+  if (hi) atomicAdd(w + 1, hi);
+}
+
+__device__ __forceinline__ int64_t warp_sum_i64(int64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace olap

@@ -1,0 +1,156 @@
+"""ctypes loader of the CPU oracle (test infrastructure only).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg import this package, and only as the checker.  ``liboracle.so`` is the
+plain-C restatement (``olap_oracle.c``); ``_ref/libref_olapcore.so`` is the
+reference's own OLAPcore source compiled in place (``Makefile``), present
+only where it was built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_OLAPCORE_SO = HERE / "_ref" / "libref_olapcore.so"
+REFERENCE_TREE = Path("/root/reference")
+
+_vp, _i64, _i32 = C.c_void_p, C.c_int64, C.c_int32
+
+
+def build(with_reference: bool | None = None) -> None:
+    """Compile the oracle (and the reference bridge when the tree exists)."""
+    targets = ["oracle"]
+    if with_reference is None:
+        with_reference = REFERENCE_TREE.exists()
+    if with_reference:
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
+
+
+def _load_oracle() -> C.CDLL:
+    if not ORACLE_SO.exists():
+        build(with_reference=False)
+    lib = C.CDLL(str(ORACLE_SO))
+    lib.oracle_plan.argtypes = [_vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_int), C.POINTER(_i64)]
+    lib.oracle_starjoin.argtypes = [C.c_int, _vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp, C.c_int,
+                                    _vp, _i64, _vp, _vp, C.POINTER(_i64)]
+    lib.oracle_size_of_table.argtypes = [C.c_int, C.c_double]
+    lib.oracle_size_of_table.restype = C.c_int
+    lib.oracle_gen_olapcore_compat.argtypes = [C.c_double, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    return lib
+
+
+_ORACLE: C.CDLL | None = None
+_REF: C.CDLL | None = None
+
+
+def oracle_lib() -> C.CDLL:
+    global _ORACLE
+    if _ORACLE is None:
+        _ORACLE = _load_oracle()
+    return _ORACLE
+
+
+def ref_available() -> bool:
+    return REF_OLAPCORE_SO.exists()
+
+
+def ref_lib() -> C.CDLL:
+    """The reference's own OLAPcore functions (built from its sources)."""
+    global _REF
+    if _REF is None:
+        if not REF_OLAPCORE_SO.exists():
+            raise FileNotFoundError(f"{REF_OLAPCORE_SO} not built (needs the reference tree)")
+        lib = C.CDLL(str(REF_OLAPCORE_SO))
+        fan = [_vp, _vp, _vp, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, C.c_int]
+        for name in ("ref_OLAPcore_rowwise", "ref_OLAPcore_vwm_dv", "ref_OLAPcore_vwm_sv",
+                     "ref_OLAPcore_cwm_dv"):
+            getattr(lib, name).argtypes = fan
+            getattr(lib, name).restype = C.c_int
+        lib.ref_OLAPcore_cwm_sv.argtypes = fan[:-1] + [_vp, C.c_int]
+        lib.ref_OLAPcore_cwm_sv.restype = C.c_int
+        lib.ref_vwm_sv_groups.argtypes = [_vp, _vp, _vp, C.c_int, _vp, _i64, _i64, _vp, _vp, _vp]
+        lib.ref_row_groups.argtypes = [_vp, _vp, _vp, C.c_int, _vp, _i64, _vp, _vp, _vp]
+        lib.ref_gen_data_olapcore.argtypes = [C.c_double, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+        _REF = lib
+    return _REF
+
+
+def _p(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def _ptr_array(arrs) -> C.Array:
+    return (C.c_void_p * 4)(*[(_p(a) if a is not None else None) for a in list(arrs) + [None] * (4 - len(arrs))])
+
+
+def plan(sele, bitmap, groups):
+    """The reference main's plan, restated (orders, factor, dimvec_nums, group_nums)."""
+    lib = oracle_lib()
+    s = np.ascontiguousarray(sele, dtype=np.float64)
+    b = np.ascontiguousarray(bitmap, dtype=np.int32)
+    g = np.ascontiguousarray(groups, dtype=np.int32)
+    orders = np.zeros(4, np.int32)
+    factor = np.zeros(4, np.int32)
+    nd = C.c_int()
+    gn = _i64()
+    lib.oracle_plan(_p(s), _p(b), _p(g), _p(orders), _p(factor), C.byref(nd), C.byref(gn))
+    return orders[: nd.value].tolist(), factor[: nd.value].tolist(), nd.value, gn.value
+
+
+def starjoin(dimvecs, fks, factors, m1, m2, group_nums, aggs=(0,), row_range=None,
+             dim_lens=None, want_groups=True):
+    """Oracle star-join over dimensions in probe order.
+
+    Returns (group_sums[n_aggs, group_nums] int64 or None, totals[n_aggs], range_errors)."""
+    lib = oracle_lib()
+    nd = len(dimvecs)
+    dv = [np.ascontiguousarray(d, dtype=np.int8) for d in dimvecs]
+    fk = [np.ascontiguousarray(f, dtype=np.int32) for f in fks]
+    lens = np.array([len(d) if dim_lens is None else dim_lens[j] for j, d in enumerate(dv)] + [0] * (4 - nd), np.int64)
+    fac = np.array(list(factors) + [0] * (4 - nd), np.int32)
+    m1a = None if m1 is None else np.ascontiguousarray(m1, dtype=np.int32)
+    m2a = None if m2 is None else np.ascontiguousarray(m2, dtype=np.int32)
+    n = len(fk[0]) if nd else (len(m1a) if m1a is not None else len(m2a))
+    rb, re = row_range if row_range is not None else (0, n)
+    ag = np.array(list(aggs), np.int32)
+    gs = np.zeros((len(aggs), group_nums), np.int64) if want_groups else None
+    tot = np.zeros(len(aggs), np.int64)
+    err = _i64()
+    lib.oracle_starjoin(nd, _ptr_array(dv), _p(lens), _ptr_array(fk), _p(fac), rb, re,
+                        None if m1a is None else _p(m1a), None if m2a is None else _p(m2a),
+                        len(aggs), _p(ag), group_nums, None if gs is None else _p(gs), _p(tot),
+                        C.byref(err))
+    return gs, tot, err.value
+
+
+def size_of_table(table: int, sf: float) -> int:
+    return int(oracle_lib().oracle_size_of_table(table, sf))
+
+
+def gen_olapcore_compat(sf, sele, bitmap, groups, use_reference=False):
+    """The reference's OLAPcore dataset (glibc rand() from its default seed).
+
+    Returns (dimvecs[4] with size+1 bytes each, fks[4], m1, m2)."""
+    sizes = [size_of_table(t, sf) for t in range(4)]
+    n = size_of_table(4, sf)
+    dv = [np.zeros(s + 1, np.int8) for s in sizes]
+    fk = [np.zeros(n, np.int32) for _ in range(4)]
+    m1 = np.zeros(n, np.int32)
+    m2 = np.zeros(n, np.int32)
+    s = np.ascontiguousarray(sele, dtype=np.float64)
+    b = np.ascontiguousarray(bitmap, dtype=np.int32)
+    g = np.ascontiguousarray(groups, dtype=np.int32)
+    if use_reference:
+        ref_lib().ref_gen_data_olapcore(float(sf), _p(s), _p(b), _p(g), _ptr_array(dv),
+                                        _ptr_array(fk), _p(m1), _p(m2))
+    else:
+        oracle_lib().oracle_gen_olapcore_compat(float(sf), _p(s), _p(b), _p(g), _ptr_array(dv),
+                                                _ptr_array(fk), _p(m1), _p(m2))
+    return dv, fk, m1, m2

@@ -301,7 +301,8 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   // Probe order: dimensions staged in shared memory first (their probes are
   // nearly free and filter rows before any L2 probe), then the caller's
   // order.  Group ids do not depend on the order.
-  const int64_t smem_dim_budget = tune_or(ctx, TUNE_SMEM_DIM_BYTES, 48 * 1024);
+  const int64_t smem_dim_budget =
+      std::min<int64_t>(tune_or(ctx, TUNE_SMEM_DIM_BYTES, 48 * 1024), ctx->smem_optin - 2048);
   int idx[OLAP_MAX_DIMS];
   for (int j = 0; j < nd; ++j) idx[j] = j;
   std::stable_sort(idx, idx + nd, [&](int a, int b) { return q->dimvec_len[a] < q->dimvec_len[b]; });

@@ -41,7 +41,7 @@ WORKLOAD = ("OLAP-core star-join at scale: 600M fact rows/GPU, 4 int32 FK + 2 in
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--rows", type=int, default=600_000_000)
@@ -76,7 +76,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -200,9 +200,9 @@ def main() -> None:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    ctx = olapcore.Context(local, scratch_bytes=512 << 20)
-    stream = torch.cuda.current_stream()
-    ctx.set_stream(stream)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)  # kernels and timing events share this stream
+    ctx = olapcore.Context(local, scratch_bytes=512 << 20, stream=stream)
     for kv in filter(None, a.tune.split(",")):
         k, v = kv.split("=")
         ctx.set_tuning(int(k), int(v))

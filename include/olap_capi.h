@@ -78,7 +78,9 @@ typedef struct olap_ctx olap_ctx;
  * mutex; use one context per host thread for concurrent submission. */
 OLAP_API int olap_ctx_create(int device, size_t scratch_bytes, olap_ctx** out);
 OLAP_API int olap_ctx_destroy(olap_ctx* ctx);
-OLAP_API int olap_ctx_set_stream(olap_ctx* ctx, void* cuda_stream); /* NULL = own stream */
+/* Run later calls on cuda_stream (a cudaStream_t); NULL is CUDA's legacy
+ * default stream.  The context's own stream is released on the first call. */
+OLAP_API int olap_ctx_set_stream(olap_ctx* ctx, void* cuda_stream);
 OLAP_API void* olap_ctx_get_stream(olap_ctx* ctx);
 OLAP_API int olap_ctx_synchronize(olap_ctx* ctx);
 OLAP_API int olap_ctx_set_tuning(olap_ctx* ctx, int knob, int64_t value);

@@ -106,18 +106,15 @@ int olap_ctx_destroy(olap_ctx* ctx) {
 int olap_ctx_set_stream(olap_ctx* ctx, void* cuda_stream) {
   if (!ctx) return OLAP_ERR_INVALID;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  cudaSetDevice(ctx->device);
+  cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+  if (!ctx->own_stream && s == ctx->stream) return OLAP_OK;
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   if (ctx->own_stream && ctx->stream) {
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
   }
-  if (cuda_stream) {
-    ctx->stream = static_cast<cudaStream_t>(cuda_stream);
-    ctx->own_stream = false;
-  } else {
-    OLAP_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    ctx->own_stream = true;
-  }
+  ctx->stream = s;
+  ctx->own_stream = false;
   return OLAP_OK;
 }
 

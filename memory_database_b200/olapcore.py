@@ -73,6 +73,8 @@ class Context:
         check(lib.olap_ctx_create(int(device), int(scratch_bytes), C.byref(h)))
         self._h = h
         self.device = int(device)
+        self._fixed_stream = stream is not None
+        self._cur_stream = None
         if stream is not None:
             self.set_stream(stream)
 
@@ -83,9 +85,24 @@ class Context:
         return self._h
 
     def set_stream(self, stream) -> None:
-        """Use a CUDA stream (torch.cuda.Stream, raw handle, or None for own)."""
-        raw = getattr(stream, "cuda_stream", stream)
+        """Run on a CUDA stream (torch.cuda.Stream or raw handle; 0 / None is
+        the legacy default stream) from now on, instead of following torch's
+        current stream."""
+        raw = getattr(stream, "cuda_stream", stream) or 0
         check(lib.olap_ctx_set_stream(self.handle, C.c_void_p(raw) if raw else None), self.handle)
+        self._fixed_stream = True
+        self._cur_stream = raw
+
+    def follow_torch_stream(self) -> None:
+        """Unless a stream was fixed, run on torch's current stream of this
+        device, so that calls are ordered with the caller's torch work."""
+        if self._fixed_stream:
+            return
+        torch = _torch()
+        raw = torch.cuda.current_stream(self.device).cuda_stream
+        if raw != self._cur_stream:
+            check(lib.olap_ctx_set_stream(self.handle, C.c_void_p(raw) if raw else None), self.handle)
+            self._cur_stream = raw
 
     @property
     def stream_handle(self) -> int:
@@ -185,6 +202,7 @@ def starjoin_groupsum(dimvecs: Sequence, fks: Sequence, factors: Sequence[int], 
     if first is not None and _is_cuda(first):
         torch = _torch()
         dev = first.device
+        ctx.follow_torch_stream()
         gs = None
         if want_groups:
             gs = out if out is not None else torch.empty((n_aggs, group_nums), dtype=torch.int64, device=dev)

@@ -195,7 +195,7 @@ def test_host_entry_point_matches_device(ctx):
 def test_host_entry_point_unknown_dim_lengths(ctx):
     """dimvec_len 0: the library copies dimvec[0 .. max fk], as the reference reads."""
     q = {"sele": [0.2, 0.2, 0.0, 0.857], "bitmap": [1, 1, 0, 1], "groups": [5, 5, 0, 6]}
-    dv, fk, m1, m2 = oracle.gen_olapcore_compat(0.2, q["sele"], q["bitmap"], q["groups"])
+    dv, fk, m1, m2 = oracle.gen_olapcore_compat(1.0, q["sele"], q["bitmap"], q["groups"])
     orders, factor, nd, G = olapcore.plan_olapcore(q["sele"], q["bitmap"], q["groups"])
     o_gs, o_tot, _ = oracle.starjoin([dv[t] for t in orders], [fk[t] for t in orders], factor, m1, m2, G)
     h_gs, h_tot = olapcore.starjoin_groupsum([dv[t] for t in orders], [fk[t] for t in orders], factor,

@@ -67,7 +67,9 @@ extern "C" {
 #define OLAP_TUNE_SMEM_DIM_BYTES 2  /* bytes of dimension vectors staged in smem */
 #define OLAP_TUNE_SMEM_ACC_BYTES 3  /* bytes of group accumulators kept in smem  */
 #define OLAP_TUNE_HOST_CHUNK_ROWS 4 /* rows per H2D chunk of the _host calls     */
-#define OLAP_TUNE_UNROLL 5          /* 4-row groups in flight per thread (1, 2)  */
+#define OLAP_TUNE_UNROLL 5          /* scan mode: 1 plain, 2 pipelined x512, 3 pipelined x256 */
+#define OLAP_TUNE_PROBE_BITS 6      /* global pass bitmaps for unstaged dims: 1 on, 2 off (default) */
+#define OLAP_TUNE_SMEM_BITS_BYTES 7 /* bytes of pass bitmaps staged in smem (default 0)          */
 
 typedef struct olap_ctx olap_ctx;
 
@@ -136,6 +138,15 @@ OLAP_API int olap_starjoin_groupsum(olap_ctx* ctx, const olap_starjoin_query* q,
  * still written) when rows were dropped. */
 OLAP_API int olap_starjoin_groupsum_host(olap_ctx* ctx, const olap_starjoin_query* q,
                                 int64_t* group_sums, int64_t* totals);
+
+/* Autotuner of the launch plan (no counterpart in the reference, whose
+ * thread counts are fixed by the caller): times candidate plans on rows
+ * [row_begin, row_begin + sample_rows) of q (device pointers; 0 = 64Mi rows),
+ * sets the fastest candidate's OLAP_TUNE_* knobs on the context and returns
+ * them in knobs_out[8] (may be NULL) and its time in *best_ms (may be NULL).
+ * Synchronous; the query's outputs are not written. */
+OLAP_API int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q,
+                                    int64_t sample_rows, int64_t* knobs_out, double* best_ms);
 
 /* Reference-layout entry point, device pointers, synchronous.
  * dimvec_array / fk_array are host arrays of 4 device pointers indexed by

@@ -38,6 +38,8 @@ TUNE_SMEM_DIM_BYTES = 2
 TUNE_SMEM_ACC_BYTES = 3
 TUNE_HOST_CHUNK_ROWS = 4
 TUNE_UNROLL = 5
+TUNE_PROBE_BITS = 6
+TUNE_SMEM_BITS_BYTES = 7
 
 
 class OlapError(RuntimeError):
@@ -86,6 +88,8 @@ def _load() -> C.CDLL:
         "olap_build_info": (C.c_char_p, []),
         "olap_starjoin_groupsum": (C.c_int, [vp, C.POINTER(StarjoinQuery), vp, vp]),
         "olap_starjoin_groupsum_host": (C.c_int, [vp, C.POINTER(StarjoinQuery), vp, vp]),
+        "olap_starjoin_autotune": (C.c_int, [vp, C.POINTER(StarjoinQuery), i64, C.POINTER(i64),
+                                             C.POINTER(C.c_double)]),
         "olap_OLAPcore": (C.c_int, [vp, vp, vp, vp, vp, C.c_int, vp, i64, i64, vp, vp, vp,
                                     C.POINTER(i64)]),
         "olap_plan_olapcore": (C.c_int, [vp, vp, vp, vp, vp, C.POINTER(C.c_int), C.POINTER(i64)]),

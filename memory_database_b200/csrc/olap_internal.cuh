@@ -64,6 +64,8 @@ enum {
   TUNE_SMEM_ACC_BYTES = OLAP_TUNE_SMEM_ACC_BYTES,
   TUNE_CHUNK_ROWS = OLAP_TUNE_HOST_CHUNK_ROWS,
   TUNE_UNROLL = OLAP_TUNE_UNROLL,
+  TUNE_PROBE_BITS = OLAP_TUNE_PROBE_BITS,
+  TUNE_SMEM_BITS_BYTES = OLAP_TUNE_SMEM_BITS_BYTES,
 };
 
 int set_error(olap_ctx* ctx, int status, const std::string& msg);
@@ -79,6 +81,7 @@ int check_cuda(olap_ctx* ctx, cudaError_t e, const char* what);
   do {                                                   \
     if (!(cond)) return olap::set_error((ctx), OLAP_ERR_INVALID, (msg)); \
   } while (0)
+
 
 // Bump allocator over the context arena.  Returns nullptr when the arena is
 // exhausted (the caller reports OLAP_ERR_CAPACITY).
@@ -97,6 +100,11 @@ struct Arena {
     return reinterpret_cast<T*>(base + a);
   }
 };
+
+// Star-join on device pointers (starjoin.cu): plans, zeroes the outputs unless
+// `accumulate`, builds pass bitmaps and launches on `stream`; scratch from `ar`.
+int starjoin_device(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_sums,
+                    int64_t* totals, bool accumulate, cudaStream_t stream, Arena& ar);
 
 inline int64_t tune_or(const olap_ctx* c, int knob, int64_t dflt) {
   return c->tune[knob] > 0 ? c->tune[knob] : dflt;

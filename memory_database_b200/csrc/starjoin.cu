@@ -24,19 +24,23 @@
 #include <algorithm>
 #include <cstring>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "olap_internal.cuh"
 
 namespace olap {
 
+// One dimension in probe order.
 struct Probe {
-  const int8_t* vec;
-  const int32_t* fk;
-  uint32_t len;
+  const int8_t* vec;      // int8 group code or DIM_NULL
+  const uint32_t* bits;   // pass bitmap (bit k: vec[k] != DIM_NULL) or null
+  const int32_t* fk;      // foreign-key column
+  uint32_t len;           // readable entries of vec
   int32_t factor;
-  int32_t soff;  // byte offset of the staged copy in shared memory, -1: global
-  int32_t pad;
+  int32_t soff;           // byte offset of a staged int8 copy in shared memory, or -1
+  int32_t boff;           // byte offset of a staged pass bitmap in shared memory, or -1
+  int32_t code_flag;      // index into StarParams::code_nonzero (bitmap dims)
 };
 
 struct StarParams {
@@ -49,12 +53,17 @@ struct StarParams {
   unsigned long long* out;     // [n_aggs][n_groups]
   unsigned long long* totals;  // [n_aggs] or null
   unsigned long long* range_err;
+  const int32_t* code_nonzero; // per bitmap dim: 1 when some live code != 0
   int32_t n_aggs, agg0, agg1;
-  int32_t smem_dim_bytes;      // staged dimension bytes (multiple of 16)
+  int32_t smem_dim_bytes;      // staged dimension bytes and bitmaps (multiple of 16)
   int32_t need_m1, need_m2;
 };
 
 enum { ACC_NONE = 0, ACC_SMEM = 1, ACC_GLOBAL = 2 };
+// Streaming modes of the 128-bit path: plain (64 registers, 2 x 512-thread
+// blocks per SM), or software-pipelined (the next 4-row group's loads are in
+// flight while the current group is probed) with 512 or 256-thread blocks.
+enum { MODE_PLAIN = 0, MODE_PIPE_512 = 1, MODE_PIPE_256 = 2, MODE_SCALAR = 3 };
 
 __device__ __forceinline__ int64_t agg_value(int a, int32_t x, int32_t y) {
   switch (a) {
@@ -66,17 +75,47 @@ __device__ __forceinline__ int64_t agg_value(int a, int32_t x, int32_t y) {
   }
 }
 
-template <int ND, int ACC, bool VEC, int U>
-__global__ void __launch_bounds__(512, U == 1 ? 2 : 1) starjoin_kernel(const StarParams p) {
+// Pass bitmap of one dimension vector: bit k of word k/32 is set when
+// vec[k] != DIM_NULL; *nonzero becomes 1 when a live code is not 0 (then the
+// code must be fetched for surviving rows).  One warp ballot per word.
+__global__ void build_pass_bits(const int8_t* __restrict__ vec, uint32_t len,
+                                uint32_t* __restrict__ bits, int32_t* __restrict__ nonzero) {
+  const uint64_t nwords = (static_cast<uint64_t>(len) + 31) >> 5;
+  const uint64_t total = nwords << 5;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  bool any = false;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += stride) {
+    const int32_t c = i < len ? static_cast<int32_t>(vec[i]) : OLAP_DIM_NULL;
+    const bool live = c != OLAP_DIM_NULL;
+    any |= live && c != 0;
+    const uint32_t w = __ballot_sync(0xffffffffu, live);
+    if ((threadIdx.x & 31) == 0) bits[i >> 5] = w;
+  }
+  if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) atomicOr(nonzero, 1);
+}
+
+template <int ND>
+struct Group4 {
+  int4 f[ND > 0 ? ND : 1];
+  int4 a, b;
+};
+
+template <int ND, int ACC, bool VEC, int MODE>
+__global__ void __launch_bounds__(MODE == MODE_PIPE_256 ? 256 : MODE == MODE_PIPE_512 ? 512 : 1024,
+                                  MODE == MODE_PIPE_256 ? 3 : 1)
+starjoin_kernel(const StarParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long red[32][2];
   __shared__ unsigned int red_bad;
+  __shared__ int32_t s_code_nz[OLAP_MAX_DIMS];
   unsigned char* sdim = smem;
   unsigned long long* sacc = reinterpret_cast<unsigned long long*>(smem + p.smem_dim_bytes);
   const int tid = threadIdx.x;
   const int64_t nacc = p.n_groups * p.n_aggs;
 
   if (tid == 0) red_bad = 0;
+  if (tid < OLAP_MAX_DIMS)
+    s_code_nz[tid] = (tid < ND && p.dim[tid].code_flag >= 0) ? p.code_nonzero[p.dim[tid].code_flag] : 0;
   // Stage small dimension vectors into shared memory.
 #pragma unroll
   for (int j = 0; j < ND; ++j) {
@@ -93,10 +132,24 @@ __global__ void __launch_bounds__(512, U == 1 ? 2 : 1) starjoin_kernel(const Sta
         for (uint32_t i = tid; i < n; i += blockDim.x) dst[i] = src[i];
       }
     }
+    if (p.dim[j].boff >= 0) {
+      // Pass bitmap (built on the same stream before this kernel; the arena
+      // allocation is 256-byte aligned, so 16-byte copies are safe).
+      const uint32_t nw = (p.dim[j].len + 31) >> 5;
+      const uint32_t n4 = nw >> 2;
+      const int4* src = reinterpret_cast<const int4*>(p.dim[j].bits);
+      int4* dst = reinterpret_cast<int4*>(sdim + p.dim[j].boff);
+      for (uint32_t i = tid; i < n4; i += blockDim.x) dst[i] = __ldg(src + i);
+      uint32_t* dw = reinterpret_cast<uint32_t*>(sdim + p.dim[j].boff);
+      for (uint32_t i = (n4 << 2) + tid; i < nw; i += blockDim.x) dw[i] = __ldg(p.dim[j].bits + i);
+    }
   }
   if (ACC == ACC_SMEM)
     for (int64_t i = tid; i < nacc; i += blockDim.x) sacc[i] = 0ull;
   __syncthreads();
+  bool need_code[OLAP_MAX_DIMS];
+#pragma unroll
+  for (int j = 0; j < OLAP_MAX_DIMS; ++j) need_code[j] = s_code_nz[j] != 0;
 
   const uint64_t pol_stream = policy_evict_first();
   const uint64_t pol_keep = policy_evict_last();
@@ -105,32 +158,8 @@ __global__ void __launch_bounds__(512, U == 1 ? 2 : 1) starjoin_kernel(const Sta
   int64_t tot0 = 0, tot1 = 0;
   unsigned int bad = 0;
 
-  auto row = [&](const int32_t* key, int32_t x, int32_t y) {
-    // Every key is range-checked before any probe (registers only), so the
-    // range-error count does not depend on the probe order.
-    bool inb = true;
-#pragma unroll
-    for (int j = 0; j < ND; ++j) inb &= static_cast<uint32_t>(key[j]) < p.dim[j].len;
-    if (!inb) {
-      ++bad;
-      return;
-    }
-    bool ok = true;
-    int64_t g = 0;
-#pragma unroll
-    for (int j = 0; j < ND; ++j) {
-      if (ok) {
-        const uint32_t k = static_cast<uint32_t>(key[j]);
-        const int32_t c = p.dim[j].soff >= 0
-                              ? static_cast<int32_t>(static_cast<int8_t>(sdim[p.dim[j].soff + k]))
-                              : ld_probe_s8(p.dim[j].vec + k, pol_keep);
-        if (c == OLAP_DIM_NULL)
-          ok = false;
-        else
-          g += static_cast<int64_t>(c) * p.dim[j].factor;
-      }
-    }
-    if (!ok) return;
+  // Accumulate one surviving row.
+  auto emit = [&](int64_t g, int32_t x, int32_t y) {
     if (static_cast<uint64_t>(g) >= static_cast<uint64_t>(p.n_groups)) {
       ++bad;
       return;
@@ -148,15 +177,115 @@ __global__ void __launch_bounds__(512, U == 1 ? 2 : 1) starjoin_kernel(const Sta
     }
   };
 
+  // Probe R rows breadth-first: for each dimension, the R independent probes
+  // are issued together before any of them is consumed.  Every key is
+  // range-checked first (registers only), so the range-error count does not
+  // depend on the probe order.
+  auto probe_rows = [&](auto& key, const int32_t* x, const int32_t* y, auto rows_tag) {
+    constexpr int R = decltype(rows_tag)::value;
+    unsigned alive = (1u << R) - 1u;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      bool inb = true;
+#pragma unroll
+      for (int j = 0; j < ND; ++j) inb &= static_cast<uint32_t>(key[r][j]) < p.dim[j].len;
+      if (!inb) {
+        alive &= ~(1u << r);
+        ++bad;
+      }
+    }
+    int64_t g[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) g[r] = 0;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      if (alive == 0) break;
+      const Probe& d = p.dim[j];
+      if (d.soff >= 0) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (alive & (1u << r)) {
+            const int32_t c = static_cast<int8_t>(sdim[d.soff + static_cast<uint32_t>(key[r][j])]);
+            if (c == OLAP_DIM_NULL) alive &= ~(1u << r);
+            else g[r] += static_cast<int64_t>(c) * d.factor;
+          }
+        }
+      } else if (d.boff >= 0) {
+        const uint32_t* sw = reinterpret_cast<const uint32_t*>(sdim + d.boff);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const uint32_t k = static_cast<uint32_t>(key[r][j]);
+          if ((alive & (1u << r)) && !((sw[k >> 5] >> (k & 31)) & 1u)) alive &= ~(1u << r);
+        }
+      } else if (d.bits) {
+        uint32_t w[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          w[r] = (alive & (1u << r)) ? __ldg(d.bits + (static_cast<uint32_t>(key[r][j]) >> 5)) : 0u;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          if (!((w[r] >> (static_cast<uint32_t>(key[r][j]) & 31)) & 1u)) alive &= ~(1u << r);
+      } else {
+        int32_t c[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          c[r] = (alive & (1u << r)) ? ld_probe_s8(d.vec + static_cast<uint32_t>(key[r][j]), pol_keep)
+                                     : OLAP_DIM_NULL;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (c[r] == OLAP_DIM_NULL) alive &= ~(1u << r);
+          else g[r] += static_cast<int64_t>(c[r]) * d.factor;
+        }
+      }
+    }
+    if (alive == 0) return;
+    // Group codes of bitmap-filtered dimensions, for surviving rows only.
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      const Probe& d = p.dim[j];
+      if (d.soff < 0 && d.bits && need_code[j]) {
+        int32_t c[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          c[r] = (alive & (1u << r)) ? ld_probe_s8(d.vec + static_cast<uint32_t>(key[r][j]), pol_keep) : 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) g[r] += static_cast<int64_t>(c[r]) * d.factor;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (alive & (1u << r)) emit(g[r], x[r], y[r]);
+  };
+
   auto scalar_rows = [&](int64_t b, int64_t e, int64_t first, int64_t step) {
     for (int64_t r = b + first; r < e; r += step) {
-      int32_t key[ND > 0 ? ND : 1];
+      int32_t key[1][ND > 0 ? ND : 1];
 #pragma unroll
-      for (int j = 0; j < ND; ++j) key[j] = ld_stream_s32(p.dim[j].fk + r, pol_stream);
+      for (int j = 0; j < ND; ++j) key[0][j] = ld_stream_s32(p.dim[j].fk + r, pol_stream);
       const int32_t x = p.need_m1 ? ld_stream_s32(p.m1 + r, pol_stream) : 0;
       const int32_t y = p.need_m2 ? ld_stream_s32(p.m2 + r, pol_stream) : 0;
-      row(key, x, y);
+      probe_rows(key, &x, &y, std::integral_constant<int, 1>{});
     }
+  };
+
+  auto load4 = [&](Group4<ND>& G, int64_t r) {
+#pragma unroll
+    for (int j = 0; j < ND; ++j) G.f[j] = ld_stream_v4(p.dim[j].fk + r, pol_stream);
+    G.a = p.need_m1 ? ld_stream_v4(p.m1 + r, pol_stream) : make_int4(0, 0, 0, 0);
+    G.b = p.need_m2 ? ld_stream_v4(p.m2 + r, pol_stream) : make_int4(0, 0, 0, 0);
+  };
+  auto process4 = [&](const Group4<ND>& G) {
+    int32_t key[4][ND > 0 ? ND : 1];
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      key[0][j] = G.f[j].x;
+      key[1][j] = G.f[j].y;
+      key[2][j] = G.f[j].z;
+      key[3][j] = G.f[j].w;
+    }
+    const int32_t x[4] = {G.a.x, G.a.y, G.a.z, G.a.w};
+    const int32_t y[4] = {G.b.x, G.b.y, G.b.z, G.b.w};
+    probe_rows(key, x, y, std::integral_constant<int, 4>{});
   };
 
   const int64_t gtid = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid;
@@ -169,45 +298,24 @@ __global__ void __launch_bounds__(512, U == 1 ? 2 : 1) starjoin_kernel(const Sta
     }
     const int64_t nvec = (p.vec_end - p.vec_begin) >> 2;
     const int64_t base = p.vec_begin;
-    // U groups of 4 rows per iteration: every 128-bit load of all U groups is
-    // issued before the first dependent probe.
     int64_t i = gtid;
-    for (; i + (U - 1) * gstride < nvec; i += U * gstride) {
-      int4 f[U][ND > 0 ? ND : 1];
-      int4 a[U], b[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int64_t r = base + 4 * (i + u * gstride);
-#pragma unroll
-        for (int j = 0; j < ND; ++j) f[u][j] = ld_stream_v4(p.dim[j].fk + r, pol_stream);
-        a[u] = p.need_m1 ? ld_stream_v4(p.m1 + r, pol_stream) : make_int4(0, 0, 0, 0);
-        b[u] = p.need_m2 ? ld_stream_v4(p.m2 + r, pol_stream) : make_int4(0, 0, 0, 0);
+    if (MODE == MODE_PIPE_512 || MODE == MODE_PIPE_256) {
+      Group4<ND> cur;
+      if (i < nvec) load4(cur, base + 4 * i);
+      for (; i < nvec; i += gstride) {
+        Group4<ND> nxt;
+        const int64_t in = i + gstride;
+        if (in < nvec) load4(nxt, base + 4 * in);
+        process4(cur);
+        cur = nxt;
       }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        int32_t k[ND > 0 ? ND : 1];
-#define OLAP_ROW(C)                                                        \
-  {                                                                        \
-    _Pragma("unroll") for (int j = 0; j < ND; ++j) k[j] = f[u][j].C;       \
-    row(k, a[u].C, b[u].C);                                                \
-  }
-        OLAP_ROW(x) OLAP_ROW(y) OLAP_ROW(z) OLAP_ROW(w)
+    } else {
+      for (; i < nvec; i += gstride) {
+        Group4<ND> cur;
+        load4(cur, base + 4 * i);
+        process4(cur);
       }
     }
-    // Remaining groups (fewer than U per thread).
-    for (; i < nvec; i += gstride) {
-      int4 f[1][ND > 0 ? ND : 1];
-      int4 a[1], b[1];
-      const int u = 0;
-      const int64_t r = base + 4 * i;
-#pragma unroll
-      for (int j = 0; j < ND; ++j) f[0][j] = ld_stream_v4(p.dim[j].fk + r, pol_stream);
-      a[0] = p.need_m1 ? ld_stream_v4(p.m1 + r, pol_stream) : make_int4(0, 0, 0, 0);
-      b[0] = p.need_m2 ? ld_stream_v4(p.m2 + r, pol_stream) : make_int4(0, 0, 0, 0);
-      int32_t k[ND > 0 ? ND : 1];
-      OLAP_ROW(x) OLAP_ROW(y) OLAP_ROW(z) OLAP_ROW(w)
-    }
-#undef OLAP_ROW
   } else {
     scalar_rows(p.row_begin, p.row_end, gtid, gstride);
   }
@@ -248,36 +356,62 @@ __global__ void __launch_bounds__(512, U == 1 ? 2 : 1) starjoin_kernel(const Sta
 using StarKernel = void (*)(const StarParams);
 
 template <int ND, int ACC>
-static StarKernel pick_vec(bool vec, int unroll) {
-  if (!vec) return starjoin_kernel<ND, ACC, false, 1>;
-  return unroll >= 2 ? starjoin_kernel<ND, ACC, true, 2> : starjoin_kernel<ND, ACC, true, 1>;
-}
-
-template <int ND>
-static StarKernel pick_kernel(int acc, bool vec, int unroll) {
-  switch (acc) {
-    case ACC_NONE: return pick_vec<ND, ACC_NONE>(vec, unroll);
-    case ACC_SMEM: return pick_vec<ND, ACC_SMEM>(vec, unroll);
-    default: return pick_vec<ND, ACC_GLOBAL>(vec, unroll);
+static StarKernel pick_mode(bool vec, int mode) {
+  if (!vec) return starjoin_kernel<ND, ACC, false, MODE_SCALAR>;
+  switch (mode) {
+    case MODE_PIPE_512: return starjoin_kernel<ND, ACC, true, MODE_PIPE_512>;
+    case MODE_PIPE_256: return starjoin_kernel<ND, ACC, true, MODE_PIPE_256>;
+    default: return starjoin_kernel<ND, ACC, true, MODE_PLAIN>;
   }
 }
 
-static StarKernel select_kernel(int nd, int acc, bool vec, int unroll) {
+template <int ND>
+static StarKernel pick_kernel(int acc, bool vec, int mode) {
+  switch (acc) {
+    case ACC_NONE: return pick_mode<ND, ACC_NONE>(vec, mode);
+    case ACC_SMEM: return pick_mode<ND, ACC_SMEM>(vec, mode);
+    default: return pick_mode<ND, ACC_GLOBAL>(vec, mode);
+  }
+}
+
+static StarKernel select_kernel(int nd, int acc, bool vec, int mode) {
   switch (nd) {
-    case 0: return pick_kernel<0>(acc, vec, unroll);
-    case 1: return pick_kernel<1>(acc, vec, unroll);
-    case 2: return pick_kernel<2>(acc, vec, unroll);
-    case 3: return pick_kernel<3>(acc, vec, unroll);
-    default: return pick_kernel<4>(acc, vec, unroll);
+    case 0: return pick_kernel<0>(acc, vec, mode);
+    case 1: return pick_kernel<1>(acc, vec, mode);
+    case 2: return pick_kernel<2>(acc, vec, mode);
+    case 3: return pick_kernel<3>(acc, vec, mode);
+    default: return pick_kernel<4>(acc, vec, mode);
   }
 }
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
-// Validates a query and builds the launch parameters.  `accumulate` keeps the
-// existing contents of the outputs (used by the chunked host pipeline).
+// A planned launch: parameters, kernel choice and the bitmap builds it needs.
+struct StarPlan {
+  StarParams sp;
+  int nd = 0;
+  int acc = ACC_NONE;
+  bool vec = false;
+  int mode = MODE_PLAIN;
+  int block = 512;
+  size_t smem = 0;
+  int nbits = 0;                       // dims whose pass bitmap must be built
+  int bits_dim[OLAP_MAX_DIMS] = {};    // probe index of each
+  uint32_t* bits_buf[OLAP_MAX_DIMS] = {};
+  int32_t* code_nz = nullptr;          // [OLAP_MAX_DIMS] in the arena
+};
+
+static bool agg_needs(int ag, bool* m1, bool* m2) {
+  if (ag < OLAP_AGG_M1_PLUS_M2 || ag > OLAP_AGG_COUNT) return false;
+  *m1 |= (ag == OLAP_AGG_M1_PLUS_M2 || ag == OLAP_AGG_M1 || ag == OLAP_AGG_M1_TIMES_M2);
+  *m2 |= (ag == OLAP_AGG_M1_PLUS_M2 || ag == OLAP_AGG_M2 || ag == OLAP_AGG_M1_TIMES_M2);
+  return true;
+}
+
+// Validates a query and plans its launch.  Scratch (bitmaps, flags) comes
+// from `ar`, which the caller keeps alive until the launch has completed.
 int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_sums,
-                  int64_t* totals, StarParams* sp, int* acc_mode, size_t* smem_bytes) {
+                  int64_t* totals, Arena& ar, StarPlan* pl) {
   OLAP_REQUIRE(ctx, q != nullptr, "null query");
   OLAP_REQUIRE(ctx, q->dimvec_nums >= 0 && q->dimvec_nums <= OLAP_MAX_DIMS,
                "dimvec_nums must be in [0, 4]");
@@ -286,53 +420,99 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
                "group_nums must be in [1, 2^31)");
   OLAP_REQUIRE(ctx, q->row_begin >= 0 && q->row_end >= q->row_begin, "bad fact row range");
   bool need_m1 = false, need_m2 = false;
-  for (int a = 0; a < q->n_aggs; ++a) {
-    const int ag = q->agg[a];
-    OLAP_REQUIRE(ctx, ag >= OLAP_AGG_M1_PLUS_M2 && ag <= OLAP_AGG_COUNT, "unknown aggregate");
-    need_m1 |= (ag == OLAP_AGG_M1_PLUS_M2 || ag == OLAP_AGG_M1 || ag == OLAP_AGG_M1_TIMES_M2);
-    need_m2 |= (ag == OLAP_AGG_M1_PLUS_M2 || ag == OLAP_AGG_M2 || ag == OLAP_AGG_M1_TIMES_M2);
-  }
+  for (int a = 0; a < q->n_aggs; ++a)
+    OLAP_REQUIRE(ctx, agg_needs(q->agg[a], &need_m1, &need_m2), "unknown aggregate");
   const bool empty = q->row_end == q->row_begin;
   OLAP_REQUIRE(ctx, empty || !need_m1 || q->m1, "M1 column required by the aggregate");
   OLAP_REQUIRE(ctx, empty || !need_m2 || q->m2, "M2 column required by the aggregate");
 
+  StarParams* sp = &pl->sp;
   std::memset(sp, 0, sizeof(*sp));
   const int nd = q->dimvec_nums;
-  // Probe order: dimensions staged in shared memory first (their probes are
-  // nearly free and filter rows before any L2 probe), then the caller's
-  // order.  Group ids do not depend on the order.
+  pl->nd = nd;
+  const int64_t smem_cap = ctx->smem_optin - 2048;
+  // Staging policy (all knobs from the context; the autotuner sets them):
+  //  * int8 vectors up to TUNE_SMEM_DIM_BYTES in total are copied to shared
+  //    memory whole (filter and group code in one shared-memory probe);
+  //  * pass bitmaps of the next dimensions, in the caller's order, are staged
+  //    up to TUNE_SMEM_BITS_BYTES (filter in shared memory, group code read
+  //    from L2 for surviving rows only);
+  //  * remaining dimensions use a global pass bitmap through L1
+  //    (TUNE_PROBE_BITS = 1) or direct int8 probes.
   const int64_t smem_dim_budget =
-      std::min<int64_t>(tune_or(ctx, TUNE_SMEM_DIM_BYTES, 48 * 1024), ctx->smem_optin - 2048);
+      std::min<int64_t>(tune_or(ctx, TUNE_SMEM_DIM_BYTES, 48 * 1024), smem_cap);
+  const int64_t smem_bits_budget = tune_or(ctx, TUNE_SMEM_BITS_BYTES, 0);
+  const int64_t bits_knob = tune_or(ctx, TUNE_PROBE_BITS, 2);
   int idx[OLAP_MAX_DIMS];
   for (int j = 0; j < nd; ++j) idx[j] = j;
   std::stable_sort(idx, idx + nd, [&](int a, int b) { return q->dimvec_len[a] < q->dimvec_len[b]; });
-  bool staged[OLAP_MAX_DIMS] = {false, false, false, false};
+  int kind[OLAP_MAX_DIMS] = {0, 0, 0, 0};  // 1 int8 staged, 2 bitmap staged, 3 global bitmap
   int64_t used = 0;
   for (int t = 0; t < nd; ++t) {
     const int j = idx[t];
     const int64_t bytes = (q->dimvec_len[j] + 15) & ~int64_t(15);
     if (used + bytes <= smem_dim_budget) {
-      staged[j] = true;
+      kind[j] = 1;
       used += bytes;
     }
   }
+  int64_t bits_used = 0;
+  for (int j = 0; j < nd; ++j) {
+    if (kind[j] || empty) continue;
+    const int64_t bbytes = ((q->dimvec_len[j] + 31) / 32 * 4 + 15) & ~int64_t(15);
+    if (bits_used + bbytes <= smem_bits_budget && used + bits_used + bbytes <= smem_cap) {
+      kind[j] = 2;
+      bits_used += bbytes;
+    } else if (bits_knob == 1) {
+      kind[j] = 3;
+    }
+  }
+  pl->nbits = 0;
+  pl->code_nz = nullptr;
   int out = 0;
   int64_t soff = 0;
-  for (int pass = 0; pass < 2; ++pass) {
+  // Probe order: shared-memory int8, then shared-memory bitmaps, then the rest.
+  for (int pass = 1; pass <= 3; ++pass) {
     for (int j = 0; j < nd; ++j) {
-      if (staged[j] != (pass == 0)) continue;
+      const int kj = kind[j] == 3 ? 0 : kind[j];
+      if (pass == 3 ? kj != 0 : kj != pass) continue;
       OLAP_REQUIRE(ctx, q->dimvec[j] && (empty || q->fk[j]), "null dimension vector or fk column");
       OLAP_REQUIRE(ctx, q->dimvec_len[j] >= 1 && q->dimvec_len[j] <= INT32_MAX,
                    "dimvec_len must be in [1, 2^31)");
-      Probe& pr = sp->dim[out++];
+      const int k = out++;
+      Probe& pr = sp->dim[k];
       pr.vec = q->dimvec[j];
       pr.fk = q->fk[j];
       pr.len = static_cast<uint32_t>(q->dimvec_len[j]);
       pr.factor = q->factor[j];
-      pr.soff = staged[j] ? static_cast<int32_t>(soff) : -1;
-      if (staged[j]) soff += (q->dimvec_len[j] + 15) & ~int64_t(15);
+      pr.soff = -1;
+      pr.boff = -1;
+      pr.bits = nullptr;
+      pr.code_flag = -1;
+      if (kind[j] == 1) {
+        pr.soff = static_cast<int32_t>(soff);
+        soff += (q->dimvec_len[j] + 15) & ~int64_t(15);
+      }
+      if (kind[j] == 2 || kind[j] == 3) {
+        if (!pl->code_nz) {
+          pl->code_nz = ar.take<int32_t>(OLAP_MAX_DIMS);
+          if (!pl->code_nz) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
+        }
+        uint32_t* b = ar.take<uint32_t>((q->dimvec_len[j] + 31) / 32);
+        if (!b) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for pass bitmaps");
+        pr.bits = b;
+        pr.code_flag = pl->nbits;
+        pl->bits_dim[pl->nbits] = k;
+        pl->bits_buf[pl->nbits] = b;
+        ++pl->nbits;
+        if (kind[j] == 2) {
+          pr.boff = static_cast<int32_t>(soff);
+          soff += ((q->dimvec_len[j] + 31) / 32 * 4 + 15) & ~int64_t(15);
+        }
+      }
     }
   }
+  sp->code_nonzero = pl->code_nz;
   sp->smem_dim_bytes = static_cast<int32_t>(soff);
   sp->m1 = q->m1;
   sp->m2 = q->m2;
@@ -353,56 +533,70 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   for (int j = 0; j < nd; ++j) vec &= aligned16(sp->dim[j].fk);
   if (need_m1) vec &= aligned16(q->m1);
   if (need_m2) vec &= aligned16(q->m2);
+  pl->vec = vec;
   if (vec) {
     int64_t vb = (q->row_begin + 3) & ~int64_t(3);
     if (vb > q->row_end) vb = q->row_end;
-    int64_t ve = vb + ((q->row_end - vb) & ~int64_t(3));
+    const int64_t ve = vb + ((q->row_end - vb) & ~int64_t(3));
     sp->vec_begin = vb;
     sp->vec_end = ve;
   }
+  pl->mode = static_cast<int>(tune_or(ctx, TUNE_UNROLL, 1)) - 1;  // knob 1..3 -> mode 0..2
+  if (pl->mode < MODE_PLAIN || pl->mode > MODE_PIPE_256) pl->mode = MODE_PLAIN;
+  const int max_block = pl->mode == MODE_PIPE_256 ? 256 : pl->mode == MODE_PIPE_512 ? 512 : 1024;
+  // One 1024-thread block per SM when large bitmaps are staged (the staging
+  // copy is paid once per SM), else 512-thread blocks.
+  const int dflt_block = std::min(max_block, bits_used > 64 * 1024 ? 1024 : 512);
+  pl->block = static_cast<int>(std::min<int64_t>(tune_or(ctx, TUNE_BLOCK, dflt_block), max_block));
+  OLAP_REQUIRE(ctx, pl->block >= 64 && pl->block % 32 == 0, "block size must be a multiple of 32, >= 64");
 
   const int64_t acc_bytes = q->group_nums * q->n_aggs * 8;
   const int64_t smem_acc_budget = tune_or(ctx, TUNE_SMEM_ACC_BYTES, 96 * 1024);
   int acc = ACC_GLOBAL;
   if (!group_sums) acc = ACC_NONE;
-  else if (acc_bytes <= smem_acc_budget && soff + acc_bytes <= ctx->smem_optin - 1024) acc = ACC_SMEM;
-  *acc_mode = acc | (vec ? 4 : 0);
-  *smem_bytes = static_cast<size_t>(soff + (acc == ACC_SMEM ? acc_bytes : 0));
+  else if (acc_bytes <= smem_acc_budget && soff + acc_bytes <= smem_cap) acc = ACC_SMEM;
+  pl->acc = acc;
+  pl->smem = static_cast<size_t>(soff + (acc == ACC_SMEM ? acc_bytes : 0));
   return OLAP_OK;
 }
 
-int launch_starjoin(olap_ctx* ctx, const StarParams& sp, int mode, size_t smem, int nd,
-                    cudaStream_t stream) {
-  const int acc = mode & 3;
-  const bool vec = (mode & 4) != 0;
-  const int unroll = static_cast<int>(tune_or(ctx, TUNE_UNROLL, 1));
-  StarKernel k = select_kernel(nd, acc, vec, unroll);
-  if (smem > 48 * 1024)
+int launch_starjoin(olap_ctx* ctx, StarPlan& pl, cudaStream_t stream) {
+  // Pass bitmaps (and their code flags) first, on the same stream.
+  if (pl.nbits) {
+    OLAP_CUDA_TRY(ctx, cudaMemsetAsync(pl.code_nz, 0, sizeof(int32_t) * OLAP_MAX_DIMS, stream));
+    for (int b = 0; b < pl.nbits; ++b) {
+      const Probe& d = pl.sp.dim[pl.bits_dim[b]];
+      const uint64_t threads = ((static_cast<uint64_t>(d.len) + 31) / 32) * 32;
+      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((threads + 255) / 256,
+                                                                     static_cast<uint64_t>(ctx->sm_count) * 8));
+      build_pass_bits<<<grid, 256, 0, stream>>>(d.vec, d.len, pl.bits_buf[b], pl.code_nz + b);
+      OLAP_CUDA_TRY(ctx, cudaGetLastError());
+    }
+  }
+  StarKernel k = select_kernel(pl.nd, pl.acc, pl.vec, pl.mode);
+  if (pl.smem > 48 * 1024)
     OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            static_cast<int>(smem)));
-  const int block = static_cast<int>(tune_or(ctx, TUNE_BLOCK, 512));
-  OLAP_REQUIRE(ctx, block >= 64 && block <= 512 && block % 32 == 0, "block size must be 64..512");
+                                            static_cast<int>(pl.smem)));
   int bps = static_cast<int>(tune_or(ctx, TUNE_BLOCKS_PER_SM, 0));
   if (bps == 0) {
-    OLAP_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, block, smem));
+    OLAP_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, pl.block, pl.smem));
     if (bps < 1) return set_error(ctx, OLAP_ERR_CAPACITY, "star-join kernel does not fit an SM");
   }
+  const StarParams& sp = pl.sp;
   const int64_t rows = sp.row_end - sp.row_begin;
-  const int64_t work_items = vec ? std::max<int64_t>((rows + 3) / 4, 1) : std::max<int64_t>(rows, 1);
+  const int64_t work_items = pl.vec ? std::max<int64_t>((rows + 3) / 4, 1) : std::max<int64_t>(rows, 1);
   int64_t grid = static_cast<int64_t>(ctx->sm_count) * bps;
-  grid = std::min<int64_t>(grid, (work_items + block - 1) / block);
+  grid = std::min<int64_t>(grid, (work_items + pl.block - 1) / pl.block);
   grid = std::max<int64_t>(grid, 1);
-  k<<<static_cast<unsigned>(grid), block, smem, stream>>>(sp);
+  k<<<static_cast<unsigned>(grid), pl.block, pl.smem, stream>>>(sp);
   OLAP_CUDA_TRY(ctx, cudaGetLastError());
   return OLAP_OK;
 }
 
 int starjoin_device(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_sums,
-                    int64_t* totals, bool accumulate, cudaStream_t stream) {
-  StarParams sp;
-  int mode = 0;
-  size_t smem = 0;
-  int st = plan_starjoin(ctx, q, group_sums, totals, &sp, &mode, &smem);
+                    int64_t* totals, bool accumulate, cudaStream_t stream, Arena& ar) {
+  StarPlan pl;
+  int st = plan_starjoin(ctx, q, group_sums, totals, ar, &pl);
   if (st != OLAP_OK) return st;
   if (!accumulate) {
     if (group_sums)
@@ -411,7 +605,7 @@ int starjoin_device(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_
     if (totals) OLAP_CUDA_TRY(ctx, cudaMemsetAsync(totals, 0, sizeof(int64_t) * q->n_aggs, stream));
   }
   if (q->row_end == q->row_begin) return OLAP_OK;
-  return launch_starjoin(ctx, sp, mode, smem, q->dimvec_nums, stream);
+  return launch_starjoin(ctx, pl, stream);
 }
 
 // Multi-threaded host maximum of an int32 column (used to size a dimension
@@ -560,7 +754,12 @@ int starjoin_host(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
     cq.m2 = i_m2 >= 0 ? dbuf[b][i_m2] : nullptr;
     cq.row_begin = 0;
     cq.row_end = n;
-    if (st == OLAP_OK) st = starjoin_device(ctx, &cq, dsum, dtot, true, ctx->stream);
+    if (st == OLAP_OK) {
+      // Per-chunk scratch (bitmaps) after the pipeline's buffers; chunks on
+      // one stream reuse it in order.
+      Arena car = ar;
+      st = starjoin_device(ctx, &cq, dsum, dtot, true, ctx->stream, car);
+    }
     cudaEventRecord(scanned[b], ctx->stream);
   }
   if (st == OLAP_OK && group_sums)
@@ -600,7 +799,8 @@ int olap_starjoin_groupsum(olap_ctx* ctx, const olap_starjoin_query* q, int64_t*
   if (!ctx) return OLAP_ERR_INVALID;
   std::lock_guard<std::mutex> lk(ctx->mu);
   OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
-  return olap::starjoin_device(ctx, q, group_sums, totals, false, ctx->stream);
+  olap::Arena ar(ctx);
+  return olap::starjoin_device(ctx, q, group_sums, totals, false, ctx->stream, ar);
 }
 
 int olap_starjoin_groupsum_host(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_sums,
@@ -643,7 +843,7 @@ int olap_OLAPcore(olap_ctx* ctx, int8_t* const* dimvec_array, const int64_t* dim
   olap::Arena ar(ctx);
   int64_t* dtot = ar.take<int64_t>(1);
   if (!dtot) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
-  int st = olap::starjoin_device(ctx, &q, group_vector, dtot, false, ctx->stream);
+  int st = olap::starjoin_device(ctx, &q, group_vector, dtot, false, ctx->stream, ar);
   if (st != OLAP_OK) return st;
   OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(count, dtot, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
   OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));

@@ -28,7 +28,7 @@ from ._lib import (AGG_COUNT, AGG_M1, AGG_M1_PLUS_M2, AGG_M1_TIMES_M2, AGG_M2, D
                    GROUP_NULL, MAX_DIMS, OlapError, StarjoinQuery, check, lib)
 
 __all__ = [
-    "Context", "default_context", "starjoin_groupsum", "plan_olapcore",
+    "Context", "default_context", "starjoin_groupsum", "autotune", "plan_olapcore",
     "OLAPcore_rowwise", "OLAPcore_vwm_dv", "OLAPcore_vwm_sv",
     "AGG_M1_PLUS_M2", "AGG_M1", "AGG_M2", "AGG_M1_TIMES_M2", "AGG_COUNT",
     "DIM_NULL", "GROUP_NULL", "OlapError",
@@ -217,6 +217,25 @@ def starjoin_groupsum(dimvecs: Sequence, fks: Sequence, factors: Sequence[int], 
     st = lib.olap_starjoin_groupsum_host(ctx.handle, C.byref(q), _ptr(gs), _ptr(tot))
     check(st, ctx.handle)
     return gs, tot
+
+
+def autotune(dimvecs: Sequence, fks: Sequence, factors: Sequence[int], m1, m2, group_nums: int,
+             aggs: Sequence[int] = (AGG_M1_PLUS_M2,), dimvec_lens=None, sample_rows: int = 0,
+             ctx: Context | None = None):
+    """Pick the launch plan of this query shape on a sample of its own data.
+
+    Leaves the chosen ``TUNE_*`` knobs set on ``ctx`` and returns
+    ``(knobs[8], best_ms_per_sample)``."""
+    ctx = ctx or default_context()
+    first = fks[0] if len(fks) else (m1 if m1 is not None else m2)
+    n_rows = _nelem(first) if first is not None else 0
+    q = _build_query(dimvecs, fks, factors, m1, m2, group_nums, aggs, 0, n_rows, dimvec_lens)
+    ctx.follow_torch_stream()
+    knobs = (C.c_int64 * 8)()
+    ms = C.c_double()
+    check(lib.olap_starjoin_autotune(ctx.handle, C.byref(q), int(sample_rows), knobs, C.byref(ms)),
+          ctx.handle)
+    return list(knobs), ms.value
 
 
 def plan_olapcore(sele: Sequence[float], bitmap: Sequence[int], groups: Sequence[int]):

@@ -155,7 +155,14 @@ def test_dimvec_len_pads_like_reference(ctx):
     {_lib.TUNE_SMEM_DIM_BYTES: 200 * 1024},              # everything small staged
     {_lib.TUNE_SMEM_ACC_BYTES: 1},                       # global accumulators
     {_lib.TUNE_UNROLL: 2},
+    {_lib.TUNE_UNROLL: 3},
     {_lib.TUNE_BLOCK_THREADS: 128, _lib.TUNE_BLOCKS_PER_SM: 3},
+    {_lib.TUNE_BLOCK_THREADS: 1024},
+    {_lib.TUNE_PROBE_BITS: 1},                            # global pass bitmaps (L1)
+    {_lib.TUNE_PROBE_BITS: 1, _lib.TUNE_SMEM_ACC_BYTES: 1},
+    {_lib.TUNE_SMEM_BITS_BYTES: 200 * 1024},              # bitmaps staged in smem
+    {_lib.TUNE_SMEM_BITS_BYTES: 8 * 1024, _lib.TUNE_PROBE_BITS: 1, _lib.TUNE_BLOCK_THREADS: 1024},
+    {_lib.TUNE_SMEM_BITS_BYTES: 200 * 1024, _lib.TUNE_SMEM_DIM_BYTES: 1, _lib.TUNE_UNROLL: 2},
 ])
 def test_tuning_knobs_do_not_change_results(ctx, knobs):
     sizes, groups, sele = [30000, 2000, 20000, 2556], [5, 25, 4, 7], [0.3, 0.5, 0.7, 0.9]
@@ -228,3 +235,43 @@ def test_invalid_queries_rejected(ctx):
         olapcore.starjoin_groupsum([d], [f], [1], None, f, 5, aggs=(AGG_M1,), ctx=ctx)  # M1 missing
     with pytest.raises(_lib.OlapError):
         olapcore.starjoin_groupsum([d], [f], [1], f, f, 5, aggs=(9,), ctx=ctx)
+
+
+def test_bitmap_plans_with_nonzero_codes_and_drops(ctx):
+    """Pass bitmaps (shared memory and global) must still fetch group codes
+    for surviving rows, honour negative codes and count range errors."""
+    rng = np.random.default_rng(12)
+    n = 400_003
+    sizes = [70_000, 9_000, 300_000]
+    dv = [rng.integers(-2, 9, s).astype(np.int8) for s in sizes]
+    for d in dv:
+        d[rng.random(len(d)) < 0.4] = 127
+    dv[1][:] = np.where(dv[1] == 127, 127, 0)  # a dimension whose live codes are all 0
+    fk = [rng.integers(-1, s + 1, n).astype(np.int32) for s in sizes]
+    m1 = rng.integers(1, 10000, n).astype(np.int32)
+    m2 = rng.integers(1, 10000, n).astype(np.int32)
+    for knobs in ({}, {_lib.TUNE_PROBE_BITS: 1}, {_lib.TUNE_SMEM_BITS_BYTES: 220 * 1024},
+                  {_lib.TUNE_SMEM_BITS_BYTES: 2 * 1024, _lib.TUNE_PROBE_BITS: 1}):
+        try:
+            for k, v in knobs.items():
+                ctx.set_tuning(k, v)
+            check_same(ctx, dv, fk, [100, 10, 1], m1, m2, 1000, (AGG_M1, AGG_M1_TIMES_M2))
+        finally:
+            for k in knobs:
+                ctx.set_tuning(k, 0)
+
+
+def test_autotuned_plan_gives_same_results(ctx):
+    sizes, groups, sele = [300_000, 20_000, 140_000, 2556], [8, 8, 8, 8], [0.5, 0.2, 0.1, 1.0]
+    orders, factor, nd, G = olapcore.plan_olapcore(sele, [1] * 4, groups)
+    dv, fk, m1, m2 = random_star(31, 3_000_001, sizes, sele, groups)
+    dvs, fks = [dv[t] for t in orders], [fk[t] for t in orders]
+    try:
+        knobs, ms = olapcore.autotune([dev(d) for d in dvs], [dev(f) for f in fks], factor, dev(m1),
+                                      dev(m2), G, aggs=(AGG_M1, AGG_M1_TIMES_M2),
+                                      sample_rows=1_000_000, ctx=ctx)
+        assert ms > 0 and len(knobs) == 8
+        check_same(ctx, dvs, fks, factor, m1, m2, G, (AGG_M1, AGG_M1_TIMES_M2))
+    finally:
+        for k in range(8):
+            ctx.set_tuning(k, 0)

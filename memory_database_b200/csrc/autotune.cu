@@ -45,6 +45,14 @@ std::vector<Candidate> candidates(const olap_ctx* ctx, const olap_starjoin_query
     add({{OLAP_TUNE_PROBE_BITS, 1}, {OLAP_TUNE_SMEM_BITS_BYTES, budget}, {OLAP_TUNE_SMEM_ACC_BYTES, 1},
          {OLAP_TUNE_BLOCK_THREADS, 1024}});
   }
+  // Every plan also with 8 rows per thread (512-thread blocks).
+  const size_t n4 = c.size();
+  for (size_t i = 0; i < n4; ++i) {
+    Candidate x = c[i];
+    x.knob[OLAP_TUNE_UNROLL] = 2;
+    x.knob[OLAP_TUNE_BLOCK_THREADS] = 512;
+    c.push_back(x);
+  }
   return c;
 }
 

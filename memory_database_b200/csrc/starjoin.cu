@@ -22,6 +22,7 @@
 //    L2-resident global atomics; totals are reduced in registers;
 //  * the grid is persistent: SM count x resident blocks per SM.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <type_traits>
@@ -60,10 +61,6 @@ struct StarParams {
 };
 
 enum { ACC_NONE = 0, ACC_SMEM = 1, ACC_GLOBAL = 2 };
-// Streaming modes of the 128-bit path: plain (64 registers, 2 x 512-thread
-// blocks per SM), or software-pipelined (the next 4-row group's loads are in
-// flight while the current group is probed) with 512 or 256-thread blocks.
-enum { MODE_PLAIN = 0, MODE_PIPE_512 = 1, MODE_PIPE_256 = 2, MODE_SCALAR = 3 };
 
 __device__ __forceinline__ int64_t agg_value(int a, int32_t x, int32_t y) {
   switch (a) {
@@ -94,29 +91,19 @@ __global__ void build_pass_bits(const int8_t* __restrict__ vec, uint32_t len,
   if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) atomicOr(nonzero, 1);
 }
 
-template <int ND>
-struct Group4 {
-  int4 f[ND > 0 ? ND : 1];
-  int4 a, b;
+// Aggregate sets fixed at compile time for the 128-bit path.
+enum {
+  AGGK_GENERIC = 0,   // n_aggs / agg0 / agg1 read at run time
+  AGGK_M1PM2 = 1,     // SUM(M1 + M2): the reference's aggregate
+  AGGK_M1_M1M2 = 2,   // SUM(M1), SUM(M1 * M2)
 };
 
-template <int ND, int ACC, bool VEC, int MODE>
-__global__ void __launch_bounds__(MODE == MODE_PIPE_256 ? 256 : MODE == MODE_PIPE_512 ? 512 : 1024,
-                                  MODE == MODE_PIPE_256 ? 3 : 1)
-starjoin_kernel(const StarParams p) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ long long red[32][2];
-  __shared__ unsigned int red_bad;
-  __shared__ int32_t s_code_nz[OLAP_MAX_DIMS];
-  unsigned char* sdim = smem;
-  unsigned long long* sacc = reinterpret_cast<unsigned long long*>(smem + p.smem_dim_bytes);
+// Block prologue shared by both kernels: stage int8 vectors and pass
+// bitmaps into shared memory, zero the shared accumulators.
+template <int ND, int ACC>
+__device__ __forceinline__ void stage_block(const StarParams& p, unsigned char* sdim,
+                                            unsigned long long* sacc, int64_t nacc) {
   const int tid = threadIdx.x;
-  const int64_t nacc = p.n_groups * p.n_aggs;
-
-  if (tid == 0) red_bad = 0;
-  if (tid < OLAP_MAX_DIMS)
-    s_code_nz[tid] = (tid < ND && p.dim[tid].code_flag >= 0) ? p.code_nonzero[p.dim[tid].code_flag] : 0;
-  // Stage small dimension vectors into shared memory.
 #pragma unroll
   for (int j = 0; j < ND; ++j) {
     if (p.dim[j].soff >= 0) {
@@ -146,189 +133,24 @@ starjoin_kernel(const StarParams p) {
   }
   if (ACC == ACC_SMEM)
     for (int64_t i = tid; i < nacc; i += blockDim.x) sacc[i] = 0ull;
-  __syncthreads();
-  bool need_code[OLAP_MAX_DIMS];
-#pragma unroll
-  for (int j = 0; j < OLAP_MAX_DIMS; ++j) need_code[j] = s_code_nz[j] != 0;
+}
 
-  const uint64_t pol_stream = policy_evict_first();
-  const uint64_t pol_keep = policy_evict_last();
-  const int n_aggs = p.n_aggs;
-  const int agg0 = p.agg0, agg1 = p.agg1;
-  int64_t tot0 = 0, tot1 = 0;
-  unsigned int bad = 0;
-
-  // Accumulate one surviving row.
-  auto emit = [&](int64_t g, int32_t x, int32_t y) {
-    if (static_cast<uint64_t>(g) >= static_cast<uint64_t>(p.n_groups)) {
-      ++bad;
-      return;
-    }
-    const int64_t v0 = agg_value(agg0, x, y);
-    tot0 += v0;
-    if (ACC == ACC_SMEM) smem_add_u64(&sacc[g], static_cast<uint64_t>(v0));
-    if (ACC == ACC_GLOBAL) atomicAdd(&p.out[g], static_cast<unsigned long long>(v0));
-    if (n_aggs > 1) {
-      const int64_t v1 = agg_value(agg1, x, y);
-      tot1 += v1;
-      if (ACC == ACC_SMEM) smem_add_u64(&sacc[p.n_groups + g], static_cast<uint64_t>(v1));
-      if (ACC == ACC_GLOBAL)
-        atomicAdd(&p.out[p.n_groups + g], static_cast<unsigned long long>(v1));
-    }
-  };
-
-  // Probe R rows breadth-first: for each dimension, the R independent probes
-  // are issued together before any of them is consumed.  Every key is
-  // range-checked first (registers only), so the range-error count does not
-  // depend on the probe order.
-  auto probe_rows = [&](auto& key, const int32_t* x, const int32_t* y, auto rows_tag) {
-    constexpr int R = decltype(rows_tag)::value;
-    unsigned alive = (1u << R) - 1u;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      bool inb = true;
-#pragma unroll
-      for (int j = 0; j < ND; ++j) inb &= static_cast<uint32_t>(key[r][j]) < p.dim[j].len;
-      if (!inb) {
-        alive &= ~(1u << r);
-        ++bad;
-      }
-    }
-    int64_t g[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) g[r] = 0;
-#pragma unroll
-    for (int j = 0; j < ND; ++j) {
-      if (alive == 0) break;
-      const Probe& d = p.dim[j];
-      if (d.soff >= 0) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          if (alive & (1u << r)) {
-            const int32_t c = static_cast<int8_t>(sdim[d.soff + static_cast<uint32_t>(key[r][j])]);
-            if (c == OLAP_DIM_NULL) alive &= ~(1u << r);
-            else g[r] += static_cast<int64_t>(c) * d.factor;
-          }
-        }
-      } else if (d.boff >= 0) {
-        const uint32_t* sw = reinterpret_cast<const uint32_t*>(sdim + d.boff);
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const uint32_t k = static_cast<uint32_t>(key[r][j]);
-          if ((alive & (1u << r)) && !((sw[k >> 5] >> (k & 31)) & 1u)) alive &= ~(1u << r);
-        }
-      } else if (d.bits) {
-        uint32_t w[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-          w[r] = (alive & (1u << r)) ? __ldg(d.bits + (static_cast<uint32_t>(key[r][j]) >> 5)) : 0u;
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-          if (!((w[r] >> (static_cast<uint32_t>(key[r][j]) & 31)) & 1u)) alive &= ~(1u << r);
-      } else {
-        int32_t c[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-          c[r] = (alive & (1u << r)) ? ld_probe_s8(d.vec + static_cast<uint32_t>(key[r][j]), pol_keep)
-                                     : OLAP_DIM_NULL;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          if (c[r] == OLAP_DIM_NULL) alive &= ~(1u << r);
-          else g[r] += static_cast<int64_t>(c[r]) * d.factor;
-        }
-      }
-    }
-    if (alive == 0) return;
-    // Group codes of bitmap-filtered dimensions, for surviving rows only.
-#pragma unroll
-    for (int j = 0; j < ND; ++j) {
-      const Probe& d = p.dim[j];
-      if (d.soff < 0 && d.bits && need_code[j]) {
-        int32_t c[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-          c[r] = (alive & (1u << r)) ? ld_probe_s8(d.vec + static_cast<uint32_t>(key[r][j]), pol_keep) : 0;
-#pragma unroll
-        for (int r = 0; r < R; ++r) g[r] += static_cast<int64_t>(c[r]) * d.factor;
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-      if (alive & (1u << r)) emit(g[r], x[r], y[r]);
-  };
-
-  auto scalar_rows = [&](int64_t b, int64_t e, int64_t first, int64_t step) {
-    for (int64_t r = b + first; r < e; r += step) {
-      int32_t key[1][ND > 0 ? ND : 1];
-#pragma unroll
-      for (int j = 0; j < ND; ++j) key[0][j] = ld_stream_s32(p.dim[j].fk + r, pol_stream);
-      const int32_t x = p.need_m1 ? ld_stream_s32(p.m1 + r, pol_stream) : 0;
-      const int32_t y = p.need_m2 ? ld_stream_s32(p.m2 + r, pol_stream) : 0;
-      probe_rows(key, &x, &y, std::integral_constant<int, 1>{});
-    }
-  };
-
-  auto load4 = [&](Group4<ND>& G, int64_t r) {
-#pragma unroll
-    for (int j = 0; j < ND; ++j) G.f[j] = ld_stream_v4(p.dim[j].fk + r, pol_stream);
-    G.a = p.need_m1 ? ld_stream_v4(p.m1 + r, pol_stream) : make_int4(0, 0, 0, 0);
-    G.b = p.need_m2 ? ld_stream_v4(p.m2 + r, pol_stream) : make_int4(0, 0, 0, 0);
-  };
-  auto process4 = [&](const Group4<ND>& G) {
-    int32_t key[4][ND > 0 ? ND : 1];
-#pragma unroll
-    for (int j = 0; j < ND; ++j) {
-      key[0][j] = G.f[j].x;
-      key[1][j] = G.f[j].y;
-      key[2][j] = G.f[j].z;
-      key[3][j] = G.f[j].w;
-    }
-    const int32_t x[4] = {G.a.x, G.a.y, G.a.z, G.a.w};
-    const int32_t y[4] = {G.b.x, G.b.y, G.b.z, G.b.w};
-    probe_rows(key, x, y, std::integral_constant<int, 4>{});
-  };
-
-  const int64_t gtid = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid;
-  const int64_t gstride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  if (VEC) {
-    // Head and tail rows outside the 16-byte aligned range.
-    if (blockIdx.x == 0) {
-      scalar_rows(p.row_begin, p.vec_begin, tid, blockDim.x);
-      scalar_rows(p.vec_end, p.row_end, tid, blockDim.x);
-    }
-    const int64_t nvec = (p.vec_end - p.vec_begin) >> 2;
-    const int64_t base = p.vec_begin;
-    int64_t i = gtid;
-    if (MODE == MODE_PIPE_512 || MODE == MODE_PIPE_256) {
-      Group4<ND> cur;
-      if (i < nvec) load4(cur, base + 4 * i);
-      for (; i < nvec; i += gstride) {
-        Group4<ND> nxt;
-        const int64_t in = i + gstride;
-        if (in < nvec) load4(nxt, base + 4 * in);
-        process4(cur);
-        cur = nxt;
-      }
-    } else {
-      for (; i < nvec; i += gstride) {
-        Group4<ND> cur;
-        load4(cur, base + 4 * i);
-        process4(cur);
-      }
-    }
-  } else {
-    scalar_rows(p.row_begin, p.row_end, gtid, gstride);
-  }
-
-  // Block reduction of totals and of the range-error count.
+// Block epilogue shared by both kernels: reduce totals and the range-error
+// count, flush shared accumulators to the global group vector.
+template <int ACC>
+__device__ __forceinline__ void finish_block(const StarParams& p, int64_t tot0, int64_t tot1,
+                                             unsigned int bad, unsigned long long* sacc,
+                                             int64_t nacc, long long (*red)[2],
+                                             unsigned int* red_bad) {
+  const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   tot0 = warp_sum_i64(tot0);
   tot1 = warp_sum_i64(tot1);
-  unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
+  const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
   if (lane == 0) {
     red[warp][0] = tot0;
     red[warp][1] = tot1;
-    if (wbad) atomicAdd(&red_bad, wbad);
+    if (wbad) atomicAdd(red_bad, wbad);
   }
   __syncthreads();
   if (warp == 0) {
@@ -340,9 +162,9 @@ starjoin_kernel(const StarParams p) {
     if (lane == 0) {
       if (p.totals) {
         if (s0) atomicAdd(&p.totals[0], static_cast<unsigned long long>(s0));
-        if (n_aggs > 1 && s1) atomicAdd(&p.totals[1], static_cast<unsigned long long>(s1));
+        if (p.n_aggs > 1 && s1) atomicAdd(&p.totals[1], static_cast<unsigned long long>(s1));
       }
-      if (red_bad) atomicAdd(p.range_err, static_cast<unsigned long long>(red_bad));
+      if (*red_bad) atomicAdd(p.range_err, static_cast<unsigned long long>(*red_bad));
     }
   }
   if (ACC == ACC_SMEM) {
@@ -353,34 +175,328 @@ starjoin_kernel(const StarParams p) {
   }
 }
 
+// 128-bit path.  Each thread takes V rows per iteration (V/4 int4 groups,
+// grid-strided so that every load instruction is fully coalesced), checks all
+// keys, probes the dimensions breadth-first across its V rows, fetches group
+// codes of bitmap-filtered dimensions for survivors, and accumulates.  Group
+// ids are int32: the host selects this kernel only when sum_j 128*|factor_j|
+// fits in int32, so every intermediate is exact.
+template <int ND, int ACC, int AGGK, int V>
+__global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(const StarParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ long long red[32][2];
+  __shared__ unsigned int red_bad;
+  __shared__ int32_t s_code_nz[OLAP_MAX_DIMS];
+  constexpr int NG = V / 4;
+  unsigned char* sdim = smem;
+  unsigned long long* sacc = reinterpret_cast<unsigned long long*>(smem + p.smem_dim_bytes);
+  const int tid = threadIdx.x;
+  const int64_t nacc = p.n_groups * p.n_aggs;
+  if (tid == 0) red_bad = 0;
+  if (tid < OLAP_MAX_DIMS)
+    s_code_nz[tid] = (tid < ND && p.dim[tid].code_flag >= 0) ? p.code_nonzero[p.dim[tid].code_flag] : 0;
+  stage_block<ND, ACC>(p, sdim, sacc, nacc);
+  __syncthreads();
+  bool need_code[OLAP_MAX_DIMS];
+#pragma unroll
+  for (int j = 0; j < OLAP_MAX_DIMS; ++j) need_code[j] = s_code_nz[j] != 0;
+
+  const uint64_t pol_stream = policy_evict_first();
+  const uint64_t pol_keep = policy_evict_last();
+  const uint32_t n_groups = static_cast<uint32_t>(p.n_groups);
+  int64_t tot0 = 0, tot1 = 0;
+  unsigned int bad = 0;
+
+  const int32_t* fkb[ND > 0 ? ND : 1];
+#pragma unroll
+  for (int j = 0; j < ND; ++j) fkb[j] = p.dim[j].fk + p.vec_begin;
+  const int32_t* m1b = p.m1 + p.vec_begin;
+  const int32_t* m2b = p.m2 + p.vec_begin;
+  const bool need_m1 = AGGK == AGGK_GENERIC ? p.need_m1 != 0 : true;
+  const bool need_m2 = AGGK == AGGK_GENERIC ? p.need_m2 != 0 : true;
+
+  const uint32_t nvec = static_cast<uint32_t>((p.vec_end - p.vec_begin) >> 2);
+  const uint32_t gstride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + tid; i < nvec; i += NG * gstride) {
+    int4 kf[NG][ND > 0 ? ND : 1];
+    int4 ka[NG], kb[NG];
+    uint32_t alive = 0;
+#pragma unroll
+    for (int u = 0; u < NG; ++u) {
+      const uint32_t gi = i + u * gstride;
+      if (u == 0 || gi < nvec) {
+        alive |= 0xFu << (4 * u);
+#pragma unroll
+        for (int j = 0; j < ND; ++j) kf[u][j] = ld_stream_v4(fkb[j] + 4ull * gi, pol_stream);
+        ka[u] = need_m1 ? ld_stream_v4(m1b + 4ull * gi, pol_stream) : make_int4(0, 0, 0, 0);
+        kb[u] = need_m2 ? ld_stream_v4(m2b + 4ull * gi, pol_stream) : make_int4(0, 0, 0, 0);
+      } else {
+#pragma unroll
+        for (int j = 0; j < ND; ++j) kf[u][j] = make_int4(0, 0, 0, 0);
+        ka[u] = kb[u] = make_int4(0, 0, 0, 0);
+      }
+    }
+    auto key = [&](int r, int j) -> uint32_t {
+      const int4& v = kf[r >> 2][j];
+      const int c = r & 3;
+      return static_cast<uint32_t>(c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w);
+    };
+    auto mx = [&](const int4* m, int r) -> int32_t {
+      const int4& v = m[r >> 2];
+      const int c = r & 3;
+      return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+    };
+    // Range check of every key (registers only).
+    uint32_t inb = alive;
+#pragma unroll
+    for (int r = 0; r < V; ++r) {
+      bool ok = true;
+#pragma unroll
+      for (int j = 0; j < ND; ++j) ok &= key(r, j) < p.dim[j].len;
+      if (!ok) inb &= ~(1u << r);
+    }
+    bad += __popc(alive & ~inb);
+    alive = inb;
+    int32_t g[V];
+#pragma unroll
+    for (int r = 0; r < V; ++r) g[r] = 0;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      if (alive == 0) break;
+      const Probe& d = p.dim[j];
+      if (d.soff >= 0) {
+        const int8_t* sv = reinterpret_cast<const int8_t*>(sdim + d.soff);
+#pragma unroll
+        for (int r = 0; r < V; ++r) {
+          if (alive & (1u << r)) {
+            const int32_t c = sv[key(r, j)];
+            if (c == OLAP_DIM_NULL) alive &= ~(1u << r);
+            g[r] += c * d.factor;
+          }
+        }
+      } else if (d.boff >= 0) {
+        const uint32_t* sw = reinterpret_cast<const uint32_t*>(sdim + d.boff);
+#pragma unroll
+        for (int r = 0; r < V; ++r) {
+          const uint32_t k = key(r, j);
+          if ((alive & (1u << r)) && !((sw[k >> 5] >> (k & 31)) & 1u)) alive &= ~(1u << r);
+        }
+      } else if (d.bits) {
+        uint32_t w[V];
+#pragma unroll
+        for (int r = 0; r < V; ++r) w[r] = (alive & (1u << r)) ? __ldg(d.bits + (key(r, j) >> 5)) : 0u;
+#pragma unroll
+        for (int r = 0; r < V; ++r)
+          if (!((w[r] >> (key(r, j) & 31)) & 1u)) alive &= ~(1u << r);
+      } else {
+        int32_t c[V];
+#pragma unroll
+        for (int r = 0; r < V; ++r)
+          c[r] = (alive & (1u << r)) ? ld_probe_s8(d.vec + key(r, j), pol_keep) : OLAP_DIM_NULL;
+#pragma unroll
+        for (int r = 0; r < V; ++r) {
+          if (c[r] == OLAP_DIM_NULL) alive &= ~(1u << r);
+          g[r] += c[r] * d.factor;
+        }
+      }
+    }
+    if (alive == 0) continue;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      const Probe& d = p.dim[j];
+      if (d.soff < 0 && d.bits && need_code[j]) {
+        int32_t c[V];
+#pragma unroll
+        for (int r = 0; r < V; ++r)
+          c[r] = (alive & (1u << r)) ? ld_probe_s8(d.vec + key(r, j), pol_keep) : 0;
+#pragma unroll
+        for (int r = 0; r < V; ++r) g[r] += c[r] * d.factor;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < V; ++r) {
+      if (!(alive & (1u << r))) continue;
+      const uint32_t gg = static_cast<uint32_t>(g[r]);
+      if (gg >= n_groups) {
+        ++bad;
+        continue;
+      }
+      const int32_t x = mx(ka, r), y = mx(kb, r);
+      int64_t v0, v1 = 0;
+      if (AGGK == AGGK_M1PM2) {
+        v0 = static_cast<int64_t>(x) + y;
+      } else if (AGGK == AGGK_M1_M1M2) {
+        v0 = x;
+        v1 = static_cast<int64_t>(x) * y;
+      } else {
+        v0 = agg_value(p.agg0, x, y);
+        v1 = p.n_aggs > 1 ? agg_value(p.agg1, x, y) : 0;
+      }
+      tot0 += v0;
+      if (ACC == ACC_SMEM) smem_add_u64(&sacc[gg], static_cast<uint64_t>(v0));
+      if (ACC == ACC_GLOBAL) atomicAdd(&p.out[gg], static_cast<unsigned long long>(v0));
+      if (AGGK == AGGK_M1_M1M2 || (AGGK == AGGK_GENERIC && p.n_aggs > 1)) {
+        tot1 += v1;
+        if (ACC == ACC_SMEM) smem_add_u64(&sacc[n_groups + gg], static_cast<uint64_t>(v1));
+        if (ACC == ACC_GLOBAL) atomicAdd(&p.out[n_groups + gg], static_cast<unsigned long long>(v1));
+      }
+    }
+  }
+  // Head and tail rows outside the 16-byte aligned range (block 0).
+  if (blockIdx.x == 0) {
+    auto one = [&](int64_t r) {
+      uint32_t k[ND > 0 ? ND : 1];
+      bool ok = true;
+#pragma unroll
+      for (int j = 0; j < ND; ++j) {
+        k[j] = static_cast<uint32_t>(p.dim[j].fk[r]);
+        ok &= k[j] < p.dim[j].len;
+      }
+      if (!ok) {
+        ++bad;
+        return;
+      }
+      int64_t g = 0;
+#pragma unroll
+      for (int j = 0; j < ND; ++j) {
+        const int32_t c = p.dim[j].soff >= 0 ? static_cast<int8_t>(sdim[p.dim[j].soff + k[j]]) : p.dim[j].vec[k[j]];
+        if (c == OLAP_DIM_NULL) return;
+        g += static_cast<int64_t>(c) * p.dim[j].factor;
+      }
+      if (static_cast<uint64_t>(g) >= static_cast<uint64_t>(p.n_groups)) {
+        ++bad;
+        return;
+      }
+      const int32_t x = p.need_m1 ? p.m1[r] : 0, y = p.need_m2 ? p.m2[r] : 0;
+      const int64_t v0 = agg_value(p.agg0, x, y);
+      tot0 += v0;
+      if (ACC == ACC_SMEM) smem_add_u64(&sacc[g], static_cast<uint64_t>(v0));
+      if (ACC == ACC_GLOBAL) atomicAdd(&p.out[g], static_cast<unsigned long long>(v0));
+      if (p.n_aggs > 1) {
+        const int64_t v1 = agg_value(p.agg1, x, y);
+        tot1 += v1;
+        if (ACC == ACC_SMEM) smem_add_u64(&sacc[p.n_groups + g], static_cast<uint64_t>(v1));
+        if (ACC == ACC_GLOBAL) atomicAdd(&p.out[p.n_groups + g], static_cast<unsigned long long>(v1));
+      }
+    };
+    for (int64_t r = p.row_begin + tid; r < p.vec_begin; r += blockDim.x) one(r);
+    for (int64_t r = p.vec_end + tid; r < p.row_end; r += blockDim.x) one(r);
+  }
+  finish_block<ACC>(p, tot0, tot1, bad, sacc, nacc, red, &red_bad);
+}
+
+// Generic path: one row per thread step, 32-bit loads, int64 group ids.  Used
+// for columns that are not 16-byte aligned and for plans whose group-id
+// arithmetic could leave int32.
+template <int ND, int ACC>
+__global__ void __launch_bounds__(1024, 1) starjoin_scalar_kernel(const StarParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ long long red[32][2];
+  __shared__ unsigned int red_bad;
+  __shared__ int32_t s_code_nz[OLAP_MAX_DIMS];
+  unsigned char* sdim = smem;
+  unsigned long long* sacc = reinterpret_cast<unsigned long long*>(smem + p.smem_dim_bytes);
+  const int tid = threadIdx.x;
+  const int64_t nacc = p.n_groups * p.n_aggs;
+  if (tid == 0) red_bad = 0;
+  if (tid < OLAP_MAX_DIMS)
+    s_code_nz[tid] = (tid < ND && p.dim[tid].code_flag >= 0) ? p.code_nonzero[p.dim[tid].code_flag] : 0;
+  stage_block<ND, ACC>(p, sdim, sacc, nacc);
+  __syncthreads();
+  const uint64_t pol_stream = policy_evict_first();
+  const uint64_t pol_keep = policy_evict_last();
+  int64_t tot0 = 0, tot1 = 0;
+  unsigned int bad = 0;
+  const int64_t gstride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t r = p.row_begin + static_cast<int64_t>(blockIdx.x) * blockDim.x + tid; r < p.row_end;
+       r += gstride) {
+    uint32_t k[ND > 0 ? ND : 1];
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      k[j] = static_cast<uint32_t>(ld_stream_s32(p.dim[j].fk + r, pol_stream));
+      ok &= k[j] < p.dim[j].len;
+    }
+    const int32_t x = p.need_m1 ? ld_stream_s32(p.m1 + r, pol_stream) : 0;
+    const int32_t y = p.need_m2 ? ld_stream_s32(p.m2 + r, pol_stream) : 0;
+    if (!ok) {
+      ++bad;
+      continue;
+    }
+    int64_t g = 0;
+    bool live = true;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      if (!live) break;
+      const Probe& d = p.dim[j];
+      int32_t c;
+      if (d.soff >= 0) {
+        c = static_cast<int8_t>(sdim[d.soff + k[j]]);
+      } else {
+        if (d.boff >= 0) {
+          const uint32_t* sw = reinterpret_cast<const uint32_t*>(sdim + d.boff);
+          if (!((sw[k[j] >> 5] >> (k[j] & 31)) & 1u)) { live = false; break; }
+        } else if (d.bits) {
+          if (!((__ldg(d.bits + (k[j] >> 5)) >> (k[j] & 31)) & 1u)) { live = false; break; }
+        }
+        c = ld_probe_s8(d.vec + k[j], pol_keep);
+      }
+      if (c == OLAP_DIM_NULL) live = false;
+      else g += static_cast<int64_t>(c) * d.factor;
+    }
+    if (!live) continue;
+    if (static_cast<uint64_t>(g) >= static_cast<uint64_t>(p.n_groups)) {
+      ++bad;
+      continue;
+    }
+    const int64_t v0 = agg_value(p.agg0, x, y);
+    tot0 += v0;
+    if (ACC == ACC_SMEM) smem_add_u64(&sacc[g], static_cast<uint64_t>(v0));
+    if (ACC == ACC_GLOBAL) atomicAdd(&p.out[g], static_cast<unsigned long long>(v0));
+    if (p.n_aggs > 1) {
+      const int64_t v1 = agg_value(p.agg1, x, y);
+      tot1 += v1;
+      if (ACC == ACC_SMEM) smem_add_u64(&sacc[p.n_groups + g], static_cast<uint64_t>(v1));
+      if (ACC == ACC_GLOBAL) atomicAdd(&p.out[p.n_groups + g], static_cast<unsigned long long>(v1));
+    }
+  }
+  finish_block<ACC>(p, tot0, tot1, bad, sacc, nacc, red, &red_bad);
+}
+
 using StarKernel = void (*)(const StarParams);
 
 template <int ND, int ACC>
-static StarKernel pick_mode(bool vec, int mode) {
-  if (!vec) return starjoin_kernel<ND, ACC, false, MODE_SCALAR>;
-  switch (mode) {
-    case MODE_PIPE_512: return starjoin_kernel<ND, ACC, true, MODE_PIPE_512>;
-    case MODE_PIPE_256: return starjoin_kernel<ND, ACC, true, MODE_PIPE_256>;
-    default: return starjoin_kernel<ND, ACC, true, MODE_PLAIN>;
+static StarKernel pick_vec(int aggk, int v) {
+  if (v >= 8) {
+    switch (aggk) {
+      case AGGK_M1PM2: return starjoin_vec_kernel<ND, ACC, AGGK_M1PM2, 8>;
+      case AGGK_M1_M1M2: return starjoin_vec_kernel<ND, ACC, AGGK_M1_M1M2, 8>;
+      default: return starjoin_vec_kernel<ND, ACC, AGGK_GENERIC, 8>;
+    }
+  }
+  switch (aggk) {
+    case AGGK_M1PM2: return starjoin_vec_kernel<ND, ACC, AGGK_M1PM2, 4>;
+    case AGGK_M1_M1M2: return starjoin_vec_kernel<ND, ACC, AGGK_M1_M1M2, 4>;
+    default: return starjoin_vec_kernel<ND, ACC, AGGK_GENERIC, 4>;
   }
 }
 
 template <int ND>
-static StarKernel pick_kernel(int acc, bool vec, int mode) {
+static StarKernel pick_kernel(int acc, bool vec, int aggk, int v) {
   switch (acc) {
-    case ACC_NONE: return pick_mode<ND, ACC_NONE>(vec, mode);
-    case ACC_SMEM: return pick_mode<ND, ACC_SMEM>(vec, mode);
-    default: return pick_mode<ND, ACC_GLOBAL>(vec, mode);
+    case ACC_NONE: return vec ? pick_vec<ND, ACC_NONE>(aggk, v) : starjoin_scalar_kernel<ND, ACC_NONE>;
+    case ACC_SMEM: return vec ? pick_vec<ND, ACC_SMEM>(aggk, v) : starjoin_scalar_kernel<ND, ACC_SMEM>;
+    default: return vec ? pick_vec<ND, ACC_GLOBAL>(aggk, v) : starjoin_scalar_kernel<ND, ACC_GLOBAL>;
   }
 }
 
-static StarKernel select_kernel(int nd, int acc, bool vec, int mode) {
+static StarKernel select_kernel(int nd, int acc, bool vec, int aggk, int v) {
   switch (nd) {
-    case 0: return pick_kernel<0>(acc, vec, mode);
-    case 1: return pick_kernel<1>(acc, vec, mode);
-    case 2: return pick_kernel<2>(acc, vec, mode);
-    case 3: return pick_kernel<3>(acc, vec, mode);
-    default: return pick_kernel<4>(acc, vec, mode);
+    case 0: return pick_kernel<0>(acc, vec, aggk, v);
+    case 1: return pick_kernel<1>(acc, vec, aggk, v);
+    case 2: return pick_kernel<2>(acc, vec, aggk, v);
+    case 3: return pick_kernel<3>(acc, vec, aggk, v);
+    default: return pick_kernel<4>(acc, vec, aggk, v);
   }
 }
 
@@ -392,7 +508,8 @@ struct StarPlan {
   int nd = 0;
   int acc = ACC_NONE;
   bool vec = false;
-  int mode = MODE_PLAIN;
+  int aggk = 0;    // AGGK_* of the 128-bit path
+  int rows_v = 4;  // rows per thread per iteration (4 or 8)
   int block = 512;
   size_t smem = 0;
   int nbits = 0;                       // dims whose pass bitmap must be built
@@ -533,7 +650,6 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   for (int j = 0; j < nd; ++j) vec &= aligned16(sp->dim[j].fk);
   if (need_m1) vec &= aligned16(q->m1);
   if (need_m2) vec &= aligned16(q->m2);
-  pl->vec = vec;
   if (vec) {
     int64_t vb = (q->row_begin + 3) & ~int64_t(3);
     if (vb > q->row_end) vb = q->row_end;
@@ -541,12 +657,20 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
     sp->vec_begin = vb;
     sp->vec_end = ve;
   }
-  pl->mode = static_cast<int>(tune_or(ctx, TUNE_UNROLL, 1)) - 1;  // knob 1..3 -> mode 0..2
-  if (pl->mode < MODE_PLAIN || pl->mode > MODE_PIPE_256) pl->mode = MODE_PLAIN;
-  const int max_block = pl->mode == MODE_PIPE_256 ? 256 : pl->mode == MODE_PIPE_512 ? 512 : 1024;
+  // int32 group ids are exact when every partial sum of code*factor fits.
+  int64_t gbound = 0;
+  for (int j = 0; j < nd; ++j) gbound += 128 * std::llabs(static_cast<long long>(q->factor[j]));
+  if (gbound > INT32_MAX) vec = false;
+  if (vec && ((q->row_end - q->row_begin) >> 33) != 0) vec = false;
+  pl->vec = vec;
+  pl->aggk = AGGK_GENERIC;
+  if (q->n_aggs == 1 && q->agg[0] == OLAP_AGG_M1_PLUS_M2) pl->aggk = AGGK_M1PM2;
+  if (q->n_aggs == 2 && q->agg[0] == OLAP_AGG_M1 && q->agg[1] == OLAP_AGG_M1_TIMES_M2) pl->aggk = AGGK_M1_M1M2;
+  pl->rows_v = tune_or(ctx, TUNE_UNROLL, 1) >= 2 ? 8 : 4;
   // One 1024-thread block per SM when large bitmaps are staged (the staging
   // copy is paid once per SM), else 512-thread blocks.
-  const int dflt_block = std::min(max_block, bits_used > 64 * 1024 ? 1024 : 512);
+  const int dflt_block = bits_used > 64 * 1024 ? 1024 : 512;
+  const int max_block = (vec && pl->rows_v == 8) ? 512 : 1024;
   pl->block = static_cast<int>(std::min<int64_t>(tune_or(ctx, TUNE_BLOCK, dflt_block), max_block));
   OLAP_REQUIRE(ctx, pl->block >= 64 && pl->block % 32 == 0, "block size must be a multiple of 32, >= 64");
 
@@ -573,7 +697,7 @@ int launch_starjoin(olap_ctx* ctx, StarPlan& pl, cudaStream_t stream) {
       OLAP_CUDA_TRY(ctx, cudaGetLastError());
     }
   }
-  StarKernel k = select_kernel(pl.nd, pl.acc, pl.vec, pl.mode);
+  StarKernel k = select_kernel(pl.nd, pl.acc, pl.vec, pl.aggk, pl.rows_v);
   if (pl.smem > 48 * 1024)
     OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             static_cast<int>(pl.smem)));

@@ -214,6 +214,20 @@ def main() -> None:
     gs = torch.empty((2, G), dtype=torch.int64, device="cuda")
     tot = torch.empty((2,), dtype=torch.int64, device="cuda")
 
+    # Plan choice for this query shape: the library's autotuner times its
+    # candidate plans on a 64Mi-row sample of this rank's table (untimed).
+    if a.tune:
+        knobs = [0] * 8
+        for kv in filter(None, a.tune.split(",")):
+            k, v = kv.split("=")
+            knobs[int(k)] = int(v)
+    else:
+        knobs, _ = olapcore.autotune(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,
+                                     dimvec_lens=s.probe_lens, ctx=ctx)
+    plan = {name: knobs[k] for k, name in enumerate(
+        ["block_threads", "blocks_per_sm", "smem_dim_bytes", "smem_acc_bytes", "host_chunk_rows",
+         "rows_per_thread_mode", "probe_bits", "smem_bits_bytes"]) if knobs[k]}
+
     def step():
         olapcore.starjoin_groupsum(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,
                                    dimvec_lens=s.probe_lens, ctx=ctx, out=gs, totals_out=tot)
@@ -275,6 +289,7 @@ def main() -> None:
         "config": {"workload": WORKLOAD, "rows_per_gpu": a.rows, "dim_sizes": list(DIM_SIZES),
                    "sele": a.sele, "groups": a.groups, "fk_dist": a.fk_dist,
                    "group_nums": G, "l2": "inputs 14.4 GB/GPU > 126 MB L2; no flush",
+                   "plan": plan or "automatic",
                    "parallelism": f"row shards x{world}" + (", NCCL all-reduce of group vector" if world > 1 else "")},
         "hbm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -289,7 +304,7 @@ def main() -> None:
     # fact table in pinned host memory; H2D copies and the D2H of the group
     # sums are inside the timed region.
     if not a.no_e2e:
-        line["e2e"] = e2e_host(a, s, ctx, aggs, world)
+        line["e2e"] = e2e_host(a, s, ctx, aggs, world, knobs)
         line["gpu_launches"] = a.steps + line["e2e"].pop("_launches")
     if rank == 0 and world == 1 and not a.no_cpu:
         try:
@@ -305,7 +320,7 @@ def main() -> None:
     ctx.close()
 
 
-def e2e_host(a, s, ctx, aggs, world) -> dict:
+def e2e_host(a, s, ctx, aggs, world, knobs) -> dict:
     import ctypes as C
     import numpy as np
     import torch
@@ -321,6 +336,9 @@ def e2e_host(a, s, ctx, aggs, world) -> dict:
     dims_host = [d.cpu().numpy() for d in s.dimvec]
     G = s.group_nums
     hctx = olapcore.Context(ctx.device, scratch_bytes=1 << 30)
+    for k, v in enumerate(knobs):
+        if v and k != _lib.TUNE_HOST_CHUNK_ROWS:
+            hctx.set_tuning(k, v)
 
     def run():
         # the public call with host (pinned) buffers: olap_starjoin_groupsum_host

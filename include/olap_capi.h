@@ -148,6 +148,33 @@ OLAP_API int olap_starjoin_groupsum_host(olap_ctx* ctx, const olap_starjoin_quer
 OLAP_API int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q,
                                     int64_t sample_rows, int64_t* knobs_out, double* best_ms);
 
+/* ---- star-join without any allocation --------------------------------------
+ * No counterpart in the reference (whose CPU functions allocate per-thread
+ * group vectors with new/malloc on every call).  For callers that may not
+ * allocate device memory at all (a fixed device-memory budget owned by
+ * someone else, a framework whose allocator must see every byte, a request
+ * path where an allocation may not block or fail late): no olap_ctx is
+ * needed, and no cudaMalloc, cudaFree or other device or pinned allocation is
+ * made.  Scratch is a static device array of OLAP_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until the process exits.
+ *  - Same query, outputs and results as olap_starjoin_groupsum; device
+ *    pointers; asynchronous on cuda_stream (NULL: the legacy default stream)
+ *    on the current device.  range_errors (device int64, may be NULL)
+ *    receives the number of rows this call dropped.
+ *  - Dimension vectors totalling more than OLAP_NOALLOC_MAX_DIM_ENTRIES
+ *    entries are rejected with OLAP_ERR_CAPACITY (their pass bitmaps would
+ *    not fit the scratch).
+ *  - All calls share the scratch, which keeps the last call's contents; each
+ *    call clears what must start at zero.  Calls that overlap on the GPU race
+ *    on it: order them on one stream.
+ *  - The first call on a device looks up the scratch's device address; make
+ *    it before any stream capture. */
+#define OLAP_NOALLOC_SCRATCH_BYTES (1 << 20)
+#define OLAP_NOALLOC_MAX_DIM_ENTRIES 8000000
+OLAP_API int olap_starjoin_groupsum_noalloc(const olap_starjoin_query* q, int64_t* group_sums,
+                                            int64_t* totals, int64_t* range_errors,
+                                            void* cuda_stream);
+
 /* Reference-layout entry point, device pointers, synchronous.
  * dimvec_array / fk_array are host arrays of 4 device pointers indexed by
  * table (0 customer, 1 supplier, 2 part, 3 date); orders[0..dimvec_nums)

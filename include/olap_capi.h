@@ -189,6 +189,52 @@ OLAP_API int olap_OLAPcore(olap_ctx* ctx, int8_t* const* dimvec_array, const int
                   const int32_t* M1, const int32_t* M2, int64_t* group_vector,
                   int64_t* count);
 
+/* ---- column-wise OLAP core (device pointers, reference argument layout) ----
+ * dimvec_array / fk_array / dimvec_len indexed by table as in olap_OLAPcore;
+ * group ids are int16 as in the reference, so group_nums <= 32766. */
+/* join_cwm_sv (cpp:908-958): groupID[r] = sum of code*factor over the
+ * dimensions in orders, or GROUP_NULL (all dimensions fused in one pass). */
+OLAP_API int olap_join_cwm_sv(olap_ctx* ctx, int8_t* const* dimvec_array, const int64_t* dimvec_len,
+                              int32_t* const* fk_array, const int* orders, int dimvec_nums,
+                              int16_t* groupID, const int* factor, int64_t size_lineorder);
+/* agg_cwm_sv (cpp:764-827): group_vector[groupID[r]] += M1[r] + M2[r] for
+ * groupID[r] != GROUP_NULL; *d_count = the total (the reference's return). */
+OLAP_API int olap_agg_cwm_sv(olap_ctx* ctx, const int16_t* groupID, int64_t size_lineorder,
+                             const int32_t* M1, const int32_t* M2, int64_t group_nums,
+                             int64_t* group_vector, int64_t* d_count);
+/* join_cwm_dv (cpp:840-894): the surviving rows as OID (int64 row) and
+ * groupID lists in row order (the reference's per-thread lists concatenated);
+ * *d_index = their number. */
+OLAP_API int olap_join_cwm_dv(olap_ctx* ctx, int8_t* const* dimvec_array, const int64_t* dimvec_len,
+                              int32_t* const* fk_array, const int* orders, int dimvec_nums,
+                              int64_t* OID, int16_t* groupID, const int* factor, int64_t* d_index,
+                              int64_t size_lineorder);
+/* agg_cwm_dv (cpp:685-752): group_vector[groupID[k]] += M1[OID[k]] +
+ * M2[OID[k]] for k < index (OID outside [0, size_lineorder) is a range
+ * error); *d_count = the total. */
+OLAP_API int olap_agg_cwm_dv(olap_ctx* ctx, const int64_t* OID, const int16_t* groupID, int64_t index,
+                             const int32_t* M1, const int32_t* M2, int64_t size_lineorder,
+                             int64_t group_nums, int64_t* group_vector, int64_t* d_count);
+
+/* ---- star-join operator (code/starjoin/test_starjoin_option.cpp) -----------
+ * dimvec / fk / dimvec_len for the four tables customer, supplier, part,
+ * date (dimvec_len as in olap_starjoin_query). */
+/* starjoinalgo_rowwise (:37-50): rows whose four probes are not DIM_NULL. */
+OLAP_API int olap_starjoin_count(olap_ctx* ctx, int64_t size_lineorder, int8_t* const* dimvec,
+                                 const int64_t* dimvec_len, int32_t* const* fk, int64_t* d_count);
+/* starjoinalgo_cwm_sv (:66-121): result[r] = c<<12 + s<<8 + p<<4 + d
+ * (GROUP_BITS_TABLE = 4, metadata.h:76) or GROUP_NULL; *d_count = entries
+ * that are not GROUP_NULL (the reference's count, which also skips a packed
+ * id equal to 32767). */
+OLAP_API int olap_starjoin_cwm_sv(olap_ctx* ctx, int64_t size_lineorder, int8_t* const* dimvec,
+                                  const int64_t* dimvec_len, int32_t* const* fk, int32_t* result,
+                                  int64_t* d_count);
+/* starjoinalgo_cwm_dv (:137-189): (position, packed group) of the surviving
+ * rows in row order; *d_count = their number. */
+OLAP_API int olap_starjoin_cwm_dv(olap_ctx* ctx, int64_t size_lineorder, int8_t* const* dimvec,
+                                  const int64_t* dimvec_len, int32_t* const* fk, int32_t* out_pos,
+                                  int32_t* out_group, int64_t* d_count);
+
 /* Plan of the reference's main (cpp:1937-1987): dimensions with groups > 0
  * participate; orders is sorted by sort_by_rate (cpp:223-233, including its
  * comparison of sele[i] with sele[j] by position); group_nums = prod groups;
@@ -196,6 +242,102 @@ OLAP_API int olap_OLAPcore(olap_ctx* ctx, int8_t* const* dimvec_array, const int
  * Host-only, no device needed. */
 OLAP_API int olap_plan_olapcore(const double sele[4], const int bitmap[4], const int groups[4],
                        int orders[4], int factor[4], int* dimvec_nums, int64_t* group_nums);
+
+/* ---- select, project, gather (code/select, code/project) -------------------
+ * Selection vectors are int32 row ids in ascending order; bitmaps hold bit i
+ * of row i at byte i/8, bit i%8 (little-endian 32-bit words), the storage
+ * order of a std::vector<bool> on little-endian machines.  Counts are written
+ * to device int64s (asynchronous); read them after synchronising. */
+#define OLAP_CMP_LE 0 /* col <= val: every sel_lt_T_* primitive of the reference */
+#define OLAP_CMP_LT 1 /* col <  val */
+
+/* Row ids r of col (r in [0, col_len)) with cmp(col[r], val), or, when
+ * in_rowids is given, the entries r = in_rowids[i] (i < n_in) that pass:
+ * sel_lt_T_fsel_independent_val_{branching,non_branching}
+ * (select/test_select_option.cpp:172-205, 391-423; if_sv is in_rowids).
+ * out_rowids holds up to (in_rowids ? n_in : col_len) entries; *d_count
+ * receives the count.  in_rowids entries outside [0, col_len) are dropped and
+ * counted as range errors. */
+OLAP_API int olap_select_rowids(olap_ctx* ctx, const int32_t* col, int64_t col_len, int32_t val,
+                                int cmp, const int32_t* in_rowids, int64_t n_in,
+                                int32_t* out_rowids, int64_t* d_count);
+/* Bitmap of cmp(col[r], val): sel_lt_T_bmp_independent_val_{branching,
+ * non_branching} (select:206-228, 424-440); (n + 31) / 32 words written. */
+OLAP_API int olap_select_bitmap(olap_ctx* ctx, const int32_t* col, int64_t n, int32_t val, int cmp,
+                                uint32_t* bitmap);
+/* selalgo_rowwise (select:450-467): SUM(Rd) (*d_sum) and the row count
+ * (*d_count, may be NULL) over rows with Ra, Rb and Rc all <= condition.  The
+ * column-wise and vector-wise drivers (select:479-901) return the same sum. */
+OLAP_API int olap_selalgo(olap_ctx* ctx, int32_t condition, int64_t n, const int32_t* Ra,
+                          const int32_t* Rb, const int32_t* Rc, const int32_t* Rd, int64_t* d_sum,
+                          int64_t* d_count);
+/* Projection of the pairs (Ra[r], Rc[r]) of the rows with Ra[r] <= condition
+ * and Rc[r] <= condition, in row order: proalgo_rowwise / proalgo_cwm_em /
+ * proalgo_cwm_lm_* (project/test_project_option.cpp:34-864). */
+OLAP_API int olap_project_pairs(olap_ctx* ctx, int32_t condition, int64_t n, const int32_t* Ra,
+                                const int32_t* Rc, int32_t* out_a, int32_t* out_c, int64_t* d_count);
+/* Late materialisation: outs[c][i] = cols[c][rowids[i]] for 1..8 int32
+ * columns of col_len rows (a row id outside [0, col_len) gives 0 and is
+ * counted as a range error). */
+OLAP_API int olap_gather_i32(olap_ctx* ctx, const int32_t* rowids, int64_t k, int ncols,
+                             const int32_t* const* cols, int64_t col_len, int32_t* const* outs);
+
+/* ---- joins (code/join) -------------------------------------------------------
+ * Hash table: capacity 64-bit slots (a power of two > n; use
+ * olap_hashtable_capacity(n), which keeps the load <= 1/2), 16-byte aligned,
+ * caller-allocated.  A duplicate build key keeps the payload of its last
+ * row, as the reference's sequential build does.  Key INT32_MIN marks empty
+ * slots and cannot be built (counted as a range error). */
+OLAP_API int64_t olap_hashtable_capacity(int64_t n_build);
+/* build(relation_t*, std::unordered_map&) (join/test_join_option.cpp:44-50);
+ * synchronous; OLAP_ERR_CAPACITY if the table fills. */
+OLAP_API int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* payload,
+                                 int64_t n, uint64_t* table, int64_t capacity);
+/* probe(relation_t*, std::unordered_map&) (join:90-96): *d_sum = SUM of the
+ * matched payloads (a missing key adds 0, as operator[] inserts 0) and
+ * *d_matches the match count (may be NULL).  With out_rows/out_payload the
+ * matches (probe row, payload) are also written in probe-row order (then
+ * *d_matches, or the count of a NULL d_sum call, is their number). */
+OLAP_API int olap_hashjoin_probe(olap_ctx* ctx, const uint64_t* table, int64_t capacity,
+                                 const int32_t* keys, int64_t n, int64_t* d_sum, int64_t* d_matches,
+                                 int32_t* out_rows, int32_t* out_payload);
+/* build(relation_t*, int* vector) (join:30-36): vector[key] = payload (last
+ * row wins); keys outside [0, vector_len) are counted as range errors.
+ * Entries not built are left as they are. */
+OLAP_API int olap_vecjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* payload, int64_t n,
+                                int32_t* vector, int64_t vector_len);
+/* probe(relation_t*, int* vector) (join:58-64): *d_sum = SUM vector[key]. */
+OLAP_API int olap_vecjoin_probe(olap_ctx* ctx, const int32_t* keys, int64_t n, const int32_t* vector,
+                                int64_t vector_len, int64_t* d_sum);
+
+/* ---- group-by and aggregation (code/group, code/aggregation) ---------------- */
+/* vector_group (group/test_group_option.cpp:44-60): group_vector[vecInx[i]-1]
+ * += m1[i] + m2[i] over group_num groups (1-based ids; others are range
+ * errors); optional per-group counts; *d_total = the sum of all groups (the
+ * reference's return value). */
+OLAP_API int olap_group_vector(olap_ctx* ctx, int64_t n, const int32_t* vecInx, const int32_t* m1,
+                               const int32_t* m2, int64_t group_num, int64_t* group_vector,
+                               int64_t* counts, int64_t* d_total);
+OLAP_API int64_t olap_group_hash_capacity(int64_t max_groups);
+/* hashtable_group (group:71-88) for any int32 keys: groups of key[i] +
+ * key_offset with SUM(vals[i] + vals2[i]) (vals2 may be NULL) and COUNT,
+ * written unordered to out_keys/out_sums/out_counts (out_counts may be NULL),
+ * *d_groups their number.  capacity (a power of two, see
+ * olap_group_hash_capacity) bounds the number of distinct keys; the table is
+ * taken from CUDA's stream-ordered pool.  Synchronous. */
+OLAP_API int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_offset,
+                             const int32_t* vals, const int32_t* vals2, int64_t capacity,
+                             int32_t* out_keys, int64_t* out_sums, int64_t* out_counts,
+                             int64_t* d_groups);
+/* aggalgo_* (aggregation/test_aggregation_option.cpp:28-107) in int64 fixed
+ * point: *d_sum = SUM price*qty*(100 + tax_pct), i.e. 100 x SUM(price*qty*tax
+ * + price*qty) with tax = tax_pct/100 (exact modulo 2^64). */
+OLAP_API int olap_agg_fixed(olap_ctx* ctx, int64_t n, const int32_t* price, const int32_t* qty,
+                            const int32_t* tax_pct, int64_t* d_sum);
+/* The same expression in double, reduced in a fixed order (deterministic;
+ * differs from a sequential CPU sum only by rounding). */
+OLAP_API int olap_agg_f64(olap_ctx* ctx, int64_t n, const double* tax, const double* qty,
+                          const double* price, double* d_sum);
 
 /* ---- seeded synthetic data (counter-based; identical on host and device) --
  * Value i of stream s under seed k is a pure function of (k, s, i), so any

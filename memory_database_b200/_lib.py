@@ -32,6 +32,9 @@ AGG_M2 = 2
 AGG_M1_TIMES_M2 = 3
 AGG_COUNT = 4
 
+CMP_LE = 0
+CMP_LT = 1
+
 TUNE_BLOCK_THREADS = 0
 TUNE_BLOCKS_PER_SM = 1
 TUNE_SMEM_DIM_BYTES = 2
@@ -93,6 +96,29 @@ def _load() -> C.CDLL:
         "olap_OLAPcore": (C.c_int, [vp, vp, vp, vp, vp, C.c_int, vp, i64, i64, vp, vp, vp,
                                     C.POINTER(i64)]),
         "olap_plan_olapcore": (C.c_int, [vp, vp, vp, vp, vp, C.POINTER(C.c_int), C.POINTER(i64)]),
+        "olap_starjoin_groupsum_noalloc": (C.c_int, [C.POINTER(StarjoinQuery), vp, vp, vp, vp]),
+        "olap_select_rowids": (C.c_int, [vp, vp, i64, i32, C.c_int, vp, i64, vp, vp]),
+        "olap_select_bitmap": (C.c_int, [vp, vp, i64, i32, C.c_int, vp]),
+        "olap_selalgo": (C.c_int, [vp, i32, i64, vp, vp, vp, vp, vp, vp]),
+        "olap_project_pairs": (C.c_int, [vp, i32, i64, vp, vp, vp, vp, vp]),
+        "olap_gather_i32": (C.c_int, [vp, vp, i64, C.c_int, vp, i64, vp]),
+        "olap_hashtable_capacity": (i64, [i64]),
+        "olap_hashjoin_build": (C.c_int, [vp, vp, vp, i64, vp, i64]),
+        "olap_hashjoin_probe": (C.c_int, [vp, vp, i64, vp, i64, vp, vp, vp, vp]),
+        "olap_vecjoin_build": (C.c_int, [vp, vp, vp, i64, vp, i64]),
+        "olap_vecjoin_probe": (C.c_int, [vp, vp, i64, vp, i64, vp]),
+        "olap_group_vector": (C.c_int, [vp, i64, vp, vp, vp, i64, vp, vp, vp]),
+        "olap_group_hash_capacity": (i64, [i64]),
+        "olap_group_hash": (C.c_int, [vp, i64, vp, i32, vp, vp, i64, vp, vp, vp, vp]),
+        "olap_agg_fixed": (C.c_int, [vp, i64, vp, vp, vp, vp]),
+        "olap_agg_f64": (C.c_int, [vp, i64, vp, vp, vp, vp]),
+        "olap_join_cwm_sv": (C.c_int, [vp, vp, vp, vp, vp, C.c_int, vp, vp, i64]),
+        "olap_agg_cwm_sv": (C.c_int, [vp, vp, i64, vp, vp, i64, vp, vp]),
+        "olap_join_cwm_dv": (C.c_int, [vp, vp, vp, vp, vp, C.c_int, vp, vp, vp, vp, i64]),
+        "olap_agg_cwm_dv": (C.c_int, [vp, vp, vp, i64, vp, vp, i64, i64, vp, vp]),
+        "olap_starjoin_count": (C.c_int, [vp, i64, vp, vp, vp, vp]),
+        "olap_starjoin_cwm_sv": (C.c_int, [vp, i64, vp, vp, vp, vp, vp]),
+        "olap_starjoin_cwm_dv": (C.c_int, [vp, i64, vp, vp, vp, vp, vp, vp]),
         "olap_gen_uniform_i32_dev": (C.c_int, [vp, vp, i64, u64, u64, i32, i32]),
         "olap_gen_uniform_i32": (C.c_int, [vp, i64, u64, u64, i32, i32, C.c_int]),
         "olap_gen_zipf_i32_dev": (C.c_int, [vp, vp, i64, u64, u64, i64, f64]),

@@ -1,0 +1,228 @@
+// Single-pass, order-preserving stream compaction for sm_100a.
+//
+// Selection vectors in the reference are row ids in ascending order
+// (select/test_select_option.cpp:391-423), and the column-wise OLAP core keeps
+// its OID lists in row order (OLAPcore/test_multi_compute_operator.cpp
+// :240-283).  The compaction here produces exactly that order in one pass
+// over the input: each block claims tiles in increasing order through an
+// atomic counter, ranks its selected items with a block-wide scan, and finds
+// the tile's output offset with a decoupled look-back over the status words
+// of the preceding tiles (a warp inspects 32 predecessors at a time).
+//
+// Every tile a block waits for was claimed earlier by a block that is already
+// running, so the waits end; they are bounded anyway: after kSpinLimit polls a
+// block records a timeout in the context's counters and stops, and the host
+// call reports OLAP_ERR_TIMEOUT.
+#pragma once
+
+#include "olap_internal.cuh"
+
+namespace olap {
+
+constexpr int kCompactThreads = 256;
+constexpr int kCompactGroups = 4;                                 // int4 loads per thread
+constexpr int kCompactTile = kCompactThreads * 4 * kCompactGroups;  // 4096 items
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// Status word of a tile: flag in bits 62-63 (0 none, 1 aggregate, 2
+// inclusive prefix), value in bits 0-61.
+constexpr uint64_t kFlagAgg = 1ull << 62;
+constexpr uint64_t kFlagInc = 2ull << 62;
+constexpr uint64_t kValMask = (1ull << 62) - 1;
+
+struct ScanTiles {
+  unsigned long long* status;   // [n_tiles], zeroed before the launch
+  unsigned int* next_tile;      // claim counter, zeroed before the launch
+  unsigned long long* timeouts; // context counter
+  unsigned long long* total;    // selected items in all tiles (written by the last tile)
+  int64_t n_tiles;
+};
+
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const unsigned long long* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Claims the next tile for this block (all threads get the same id).
+__device__ __forceinline__ int64_t claim_tile(const ScanTiles& st, unsigned int* s_tile) {
+  if (threadIdx.x == 0) *s_tile = atomicAdd(st.next_tile, 1u);
+  __syncthreads();
+  const int64_t t = *s_tile;
+  __syncthreads();
+  return t;
+}
+
+// Exclusive prefix of this tile's count over all earlier tiles; run by one
+// full warp (warp 0).  Returns -1 on timeout.
+__device__ __forceinline__ int64_t lookback(const ScanTiles& st, int64_t tile, uint64_t count) {
+  const int lane = threadIdx.x & 31;
+  if (tile == 0) {
+    if (lane == 0) st_relaxed_u64(&st.status[0], kFlagInc | count);
+    return 0;
+  }
+  if (lane == 0) st_relaxed_u64(&st.status[tile], kFlagAgg | count);
+  uint64_t excl = 0;
+  int64_t t = tile - 1;
+  uint32_t spins = 0;
+  while (true) {
+    const int64_t idx = t - lane;
+    uint64_t w = idx >= 0 ? ld_relaxed_u64(&st.status[idx]) : kFlagInc;
+    while (__any_sync(0xffffffffu, (w >> 62) == 0)) {
+      if (++spins > kSpinLimit) {
+        if (lane == 0) atomicAdd(st.timeouts, 1ull);
+        return -1;
+      }
+      __nanosleep(64);
+      if ((w >> 62) == 0) w = ld_relaxed_u64(&st.status[idx]);
+    }
+    const uint32_t inc = __ballot_sync(0xffffffffu, (w >> 62) == 2);
+    uint64_t v = w & kValMask;
+    if (inc) {
+      const int k = __ffs(inc) - 1;  // closest predecessor with an inclusive prefix
+      if (lane > k) v = 0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      excl += v;
+      break;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    excl += v;
+    t -= 32;
+  }
+  if (lane == 0) st_relaxed_u64(&st.status[tile], kFlagInc | (excl + count));
+  return static_cast<int64_t>(excl);
+}
+
+// Block-wide exclusive scan of four 16-bit counters packed in a uint64
+// (one counter per int4 group of the thread).  Returns the thread's exclusive
+// prefix; *block_total receives the packed totals.
+__device__ __forceinline__ uint64_t block_scan_packed(uint64_t v, uint64_t* s_warp, uint64_t* block_total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    uint64_t w = lane < nw ? s_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) s_warp[lane] = w;  // inclusive per warp
+  }
+  __syncthreads();
+  const uint64_t warp_excl = warp > 0 ? s_warp[warp - 1] : 0;
+  *block_total = s_warp[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return warp_excl + x - v;
+}
+
+__device__ __forceinline__ uint32_t field16(uint64_t packed, int u) {
+  return static_cast<uint32_t>((packed >> (16 * u)) & 0xffffu);
+}
+
+// Generic compaction kernel.  Items are numbered 0 .. n_items-1; each thread
+// handles kCompactGroups groups of 4 consecutive items per tile.  The Op is
+// called per group and per selected item:
+//   uint32_t op.flags(int u, int64_t first, int nv)  -> 4-bit mask of the
+//       selected items among first .. first+3 (only the first nv exist);
+//       the op may cache what it loaded for group u;
+//   void op.emit(int u, int k, int64_t item, int64_t pos)  -> write selected
+//       item `item` (= first + k of group u) at output position `pos`.
+template <class Op>
+__global__ void __launch_bounds__(kCompactThreads) compact_kernel(const Op op_in, int64_t n_items, ScanTiles st) {
+  Op op = op_in;  // per-thread copy: ops cache the loaded items between flags() and emit()
+  __shared__ unsigned int s_tile;
+  __shared__ uint64_t s_warp[kCompactThreads / 32];
+  __shared__ long long s_base;
+  for (;;) {
+    const int64_t tile = claim_tile(st, &s_tile);
+    if (tile >= st.n_tiles) return;
+    const int64_t tile_first = tile * kCompactTile;
+    uint32_t mask[kCompactGroups];
+    uint64_t packed = 0;
+#pragma unroll
+    for (int u = 0; u < kCompactGroups; ++u) {
+      const int64_t first = tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
+      const int64_t left = n_items - first;
+      const int nv = left >= 4 ? 4 : (left > 0 ? static_cast<int>(left) : 0);
+      mask[u] = nv > 0 ? op.flags(u, first, nv) : 0u;
+      packed |= static_cast<uint64_t>(__popc(mask[u])) << (16 * u);
+    }
+    uint64_t tot;
+    const uint64_t excl = block_scan_packed(packed, s_warp, &tot);
+    uint64_t tile_count = 0;
+#pragma unroll
+    for (int u = 0; u < kCompactGroups; ++u) tile_count += field16(tot, u);
+    if (threadIdx.x < 32) {
+      const int64_t b = lookback(st, tile, tile_count);
+      if (threadIdx.x == 0) {
+        s_base = b;
+        if (tile == st.n_tiles - 1 && b >= 0) *st.total = static_cast<unsigned long long>(b) + tile_count;
+      }
+    }
+    __syncthreads();
+    const long long base = s_base;
+    if (base < 0) return;  // timed out: the host reports it
+    uint64_t off = 0;
+#pragma unroll
+    for (int u = 0; u < kCompactGroups; ++u) {
+      const uint32_t m = mask[u];
+      int64_t pos = base + static_cast<int64_t>(off) + field16(excl, u);
+      const int64_t first = tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if ((m >> k) & 1u) op.emit(u, k, first + k, pos++);
+      off += field16(tot, u);
+    }
+  }
+}
+
+// Host helper: scan-tile state for n_items from the arena; zeroes it on the stream.
+inline int make_scan_tiles(olap_ctx* ctx, Arena& ar, int64_t n_items, unsigned long long* total,
+                           cudaStream_t stream, ScanTiles* st) {
+  st->n_tiles = (n_items + kCompactTile - 1) / kCompactTile;
+  if (st->n_tiles < 1) st->n_tiles = 1;
+  st->status = ar.take<unsigned long long>(static_cast<size_t>(st->n_tiles));
+  st->next_tile = ar.take<unsigned int>(1);
+  st->timeouts = &ctx->counters->wait_timeouts;
+  st->total = total;
+  if (!st->status || !st->next_tile)
+    return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for the compaction state");
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(st->status, 0, sizeof(unsigned long long) * st->n_tiles, stream));
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(st->next_tile, 0, sizeof(unsigned int), stream));
+  if (total) OLAP_CUDA_TRY(ctx, cudaMemsetAsync(total, 0, sizeof(unsigned long long), stream));
+  return OLAP_OK;
+}
+
+inline unsigned compact_grid(const olap_ctx* ctx, int64_t n_tiles) {
+  int64_t g = static_cast<int64_t>(ctx->sm_count) * 8;  // 8 x 256 threads per SM
+  if (g > n_tiles) g = n_tiles;
+  return static_cast<unsigned>(g < 1 ? 1 : g);
+}
+
+// Checks the wait-timeout counter after a synchronising call.
+inline int check_timeouts(olap_ctx* ctx, cudaStream_t stream) {
+  unsigned long long t = 0;
+  OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(&t, &ctx->counters->wait_timeouts, sizeof(t),
+                                     cudaMemcpyDeviceToHost, stream));
+  OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(stream));
+  if (t) {
+    OLAP_CUDA_TRY(ctx, cudaMemsetAsync(&ctx->counters->wait_timeouts, 0, sizeof(t), stream));
+    return set_error(ctx, OLAP_ERR_TIMEOUT, "a bounded device wait expired in a compaction");
+  }
+  return OLAP_OK;
+}
+
+}  // namespace olap

@@ -1,0 +1,374 @@
+// Equi-join build and probe for sm_100a.
+//
+// Reference: code/join/test_join_option.cpp.  build(R, int* vector) stores
+// vector[key] = payload (:30-36) and probe(S, vector) sums vector[key] over
+// the probe keys (:58-64); the hash variants do the same through
+// std::unordered_map (:44-50, :90-96), where operator[] makes a missing key
+// contribute 0.  With duplicate build keys the sequential build keeps the last
+// row's payload; both builds here keep exactly that row.
+//
+// Hash table (a format of this library): 2^k 64-bit slots, open addressing
+// with linear probing over 32-byte buckets of 4 slots (one DRAM sector per
+// probe step).  During the build a slot holds (key << 32 | row) so that a
+// duplicate key keeps the largest row with one 64-bit atomicMax; a finishing
+// pass replaces the row by that row's payload, so a probe reads key and
+// payload in one load.  The key INT32_MIN marks an empty slot and cannot be
+// built (such build rows are counted as range errors).
+#include <cstring>
+
+#include "compact.cuh"
+
+namespace olap {
+
+constexpr uint64_t kEmptySlot = 0x80000000FFFFFFFFull;  // key INT32_MIN, row 0xffffffff
+
+__host__ __device__ __forceinline__ uint32_t hash32(uint32_t x) {  // murmur3 finaliser
+  x ^= x >> 16;
+  x *= 0x85ebca6bu;
+  x ^= x >> 13;
+  x *= 0xc2b2ae35u;
+  x ^= x >> 16;
+  return x;
+}
+
+__global__ void fill_u64_kernel(uint64_t* p, int64_t n, uint64_t v) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
+}
+
+__global__ void hash_build_kernel(const int32_t* __restrict__ keys, int64_t n, uint64_t* __restrict__ slots,
+                                  uint64_t mask, unsigned long long* range_err, unsigned long long* overflow) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
+    const int32_t k = keys[r];
+    if (k == INT32_MIN) {
+      atomicAdd(range_err, 1ull);
+      continue;
+    }
+    const uint64_t mine = (static_cast<uint64_t>(static_cast<uint32_t>(k)) << 32) | static_cast<uint32_t>(r);
+    uint64_t h = hash32(static_cast<uint32_t>(k)) & mask;
+    bool done = false;
+    for (uint64_t step = 0; step <= mask && !done; ++step) {
+      unsigned long long* s = reinterpret_cast<unsigned long long*>(slots + h);
+      const unsigned long long prev = atomicCAS(s, kEmptySlot, mine);
+      if (prev == kEmptySlot) {
+        done = true;
+      } else if ((prev >> 32) == static_cast<uint32_t>(k)) {
+        atomicMax(s, mine);  // same key in the high word: keeps the largest row
+        done = true;
+      } else {
+        h = (h + 1) & mask;
+      }
+    }
+    if (!done) atomicAdd(overflow, 1ull);
+  }
+}
+
+__global__ void hash_finish_kernel(uint64_t* __restrict__ slots, int64_t cap, const int32_t* __restrict__ payload) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < cap; i += stride) {
+    const uint64_t v = slots[i];
+    if (v == kEmptySlot) continue;
+    const uint32_t row = static_cast<uint32_t>(v);
+    slots[i] = (v & 0xffffffff00000000ull) | static_cast<uint32_t>(payload[row]);
+  }
+}
+
+// Probe: SUM of matched payloads and the match count; optionally the matches
+// (probe row, payload) compacted in probe-row order by the caller's second
+// pass (see ProbeOp).
+__device__ __forceinline__ bool hash_lookup(const uint64_t* __restrict__ slots, uint64_t mask, int32_t k,
+                                            int32_t* payload) {
+  uint64_t h = hash32(static_cast<uint32_t>(k)) & mask;
+  const uint32_t uk = static_cast<uint32_t>(k);
+  for (uint64_t step = 0; step <= mask; step += 4) {
+    // the 4-slot bucket holding h (one 32-byte sector), starting at h
+    const uint64_t b = h & ~3ull;
+    const ulonglong2 lo = __ldg(reinterpret_cast<const ulonglong2*>(slots + b));
+    const ulonglong2 hi = __ldg(reinterpret_cast<const ulonglong2*>(slots + b + 2));
+    const uint64_t s[4] = {lo.x, lo.y, hi.x, hi.y};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (j < static_cast<int>(h & 3)) continue;  // linear probing starts at h
+      if (s[j] == kEmptySlot) return false;
+      if ((s[j] >> 32) == uk) {
+        *payload = static_cast<int32_t>(static_cast<uint32_t>(s[j]));
+        return true;
+      }
+    }
+    h = (b + 4) & mask;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(512) hash_probe_sum_kernel(const int32_t* __restrict__ keys, int64_t n,
+                                                             const uint64_t* __restrict__ slots, uint64_t mask,
+                                                             int vec, unsigned long long* sum,
+                                                             unsigned long long* matches) {
+  __shared__ long long s_red[16][2];
+  const uint64_t pol = policy_evict_first();
+  int64_t s = 0, c = 0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t n4 = vec ? n >> 2 : 0;
+  for (int64_t i = tid; i < n4; i += stride) {
+    const int4 k = ld_stream_v4(keys + 4 * i, pol);
+    int32_t p0 = 0, p1 = 0, p2 = 0, p3 = 0;
+    const bool f0 = hash_lookup(slots, mask, k.x, &p0), f1 = hash_lookup(slots, mask, k.y, &p1);
+    const bool f2 = hash_lookup(slots, mask, k.z, &p2), f3 = hash_lookup(slots, mask, k.w, &p3);
+    s += (f0 ? p0 : 0) + static_cast<int64_t>(f1 ? p1 : 0) + (f2 ? p2 : 0) + static_cast<int64_t>(f3 ? p3 : 0);
+    c += f0 + f1 + f2 + f3;
+  }
+  for (int64_t r = 4 * n4 + tid; r < n; r += stride) {
+    int32_t p = 0;
+    if (hash_lookup(slots, mask, keys[r], &p)) {
+      s += p;
+      ++c;
+    }
+  }
+  s = warp_sum_i64(s);
+  c = warp_sum_i64(c);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    s_red[warp][0] = s;
+    s_red[warp][1] = c;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    long long x = lane < static_cast<int>(blockDim.x >> 5) ? s_red[lane][0] : 0;
+    long long y = lane < static_cast<int>(blockDim.x >> 5) ? s_red[lane][1] : 0;
+    x = warp_sum_i64(x);
+    y = warp_sum_i64(y);
+    if (lane == 0) {
+      if (x) atomicAdd(sum, static_cast<unsigned long long>(x));
+      if (y) atomicAdd(matches, static_cast<unsigned long long>(y));
+    }
+  }
+}
+
+// Matches (probe row, payload) in probe-row order.
+struct ProbeOp {
+  const int32_t* keys;
+  const uint64_t* slots;
+  uint64_t mask;
+  int32_t* out_rows;
+  int32_t* out_payload;
+  int32_t vec;
+  int4 pay[kCompactGroups];
+
+  __device__ __forceinline__ uint32_t flags(int u, int64_t first, int nv) {
+    int32_t k[4] = {0, 0, 0, 0};
+    if (vec && nv == 4) {
+      const int4 v = ld_stream_v4(keys + first, policy_evict_first());
+      k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w;
+    } else {
+      for (int j = 0; j < nv; ++j) k[j] = keys[first + j];
+    }
+    int32_t p[4] = {0, 0, 0, 0};
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (j < nv && hash_lookup(slots, mask, k[j], &p[j])) m |= 1u << j;
+    pay[u] = make_int4(p[0], p[1], p[2], p[3]);
+    return m;
+  }
+  __device__ __forceinline__ void emit(int u, int k, int64_t item, int64_t pos) {
+    out_rows[pos] = static_cast<int32_t>(item);
+    out_payload[pos] = k == 0 ? pay[u].x : k == 1 ? pay[u].y : k == 2 ? pay[u].z : pay[u].w;
+  }
+};
+
+// Direct-address join: build keeps the largest row per key through a 64-bit
+// staging vector, then the int32 payload vector is written.
+__global__ void vec_build_stage_kernel(const int32_t* __restrict__ keys, int64_t n, unsigned long long* stage,
+                                       int64_t len, unsigned long long* range_err) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
+    const int32_t k = keys[r];
+    if (k < 0 || k >= len) {
+      atomicAdd(range_err, 1ull);
+      continue;
+    }
+    atomicMax(stage + k, static_cast<unsigned long long>(r) + 1);
+  }
+}
+
+__global__ void vec_build_write_kernel(const unsigned long long* __restrict__ stage, int64_t len,
+                                       const int32_t* __restrict__ payload, int32_t* __restrict__ vector) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < len; i += stride) {
+    const unsigned long long r = stage[i];
+    if (r) vector[i] = payload[r - 1];
+  }
+}
+
+__global__ void __launch_bounds__(512) vec_probe_kernel(const int32_t* __restrict__ keys, int64_t n,
+                                                        const int32_t* __restrict__ vector, int64_t len,
+                                                        int vec, unsigned long long* sum,
+                                                        unsigned long long* range_err) {
+  __shared__ long long s_red[16];
+  const uint64_t pol = policy_evict_first();
+  int64_t s = 0;
+  unsigned int bad = 0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t n4 = vec ? n >> 2 : 0;
+  auto one = [&](int32_t k) {
+    if (k < 0 || k >= len) {
+      ++bad;
+      return;
+    }
+    s += __ldg(vector + k);
+  };
+  for (int64_t i = tid; i < n4; i += stride) {
+    const int4 k = ld_stream_v4(keys + 4 * i, pol);
+    one(k.x);
+    one(k.y);
+    one(k.z);
+    one(k.w);
+  }
+  for (int64_t r = 4 * n4 + tid; r < n; r += stride) one(keys[r]);
+  s = warp_sum_i64(s);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) s_red[warp] = s;
+  if (bad) atomicAdd(range_err, static_cast<unsigned long long>(bad));
+  __syncthreads();
+  if (warp == 0) {
+    long long x = lane < static_cast<int>(blockDim.x >> 5) ? s_red[lane] : 0;
+    x = warp_sum_i64(x);
+    if (lane == 0 && x) atomicAdd(sum, static_cast<unsigned long long>(x));
+  }
+}
+
+static bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+static unsigned grid_for(const olap_ctx* ctx, int64_t items, int threads) {
+  int64_t g = (items + threads - 1) / threads;
+  const int64_t cap = static_cast<int64_t>(ctx->sm_count) * (2048 / threads);
+  if (g > cap) g = cap;
+  return static_cast<unsigned>(g < 1 ? 1 : g);
+}
+
+}  // namespace olap
+
+extern "C" {
+
+int64_t olap_hashtable_capacity(int64_t n_build) {
+  int64_t cap = 8;
+  while (cap < 2 * n_build) cap <<= 1;
+  return cap;
+}
+
+int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* payload, int64_t n,
+                        uint64_t* table, int64_t capacity) {
+  if (!ctx) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_REQUIRE(ctx, n >= 0 && n <= UINT32_MAX - 1, "n must be in [0, 2^32-1)");
+  OLAP_REQUIRE(ctx, capacity >= 8 && (capacity & (capacity - 1)) == 0 && capacity > n,
+               "capacity must be a power of two larger than n (see olap_hashtable_capacity)");
+  OLAP_REQUIRE(ctx, table && (olap::al16(table)), "table must be 16-byte aligned");
+  OLAP_REQUIRE(ctx, n == 0 || (keys && payload), "null keys or payload");
+  olap::Arena ar(ctx);
+  unsigned long long* overflow = ar.take<unsigned long long>(1);
+  if (!overflow) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(overflow, 0, sizeof(*overflow), ctx->stream));
+  olap::fill_u64_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, olap::kEmptySlot);
+  if (n) {
+    olap::hash_build_kernel<<<olap::grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(
+        keys, n, table, static_cast<uint64_t>(capacity - 1), &ctx->counters->range_errors, overflow);
+    olap::hash_finish_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, payload);
+  }
+  OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  unsigned long long ov = 0;
+  OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(&ov, overflow, sizeof(ov), cudaMemcpyDeviceToHost, ctx->stream));
+  OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ov) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "hash table full");
+  return OLAP_OK;
+}
+
+int olap_hashjoin_probe(olap_ctx* ctx, const uint64_t* table, int64_t capacity, const int32_t* keys,
+                        int64_t n, int64_t* d_sum, int64_t* d_matches, int32_t* out_rows,
+                        int32_t* out_payload) {
+  if (!ctx) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_REQUIRE(ctx, n >= 0 && n <= INT32_MAX, "n must be in [0, 2^31)");
+  OLAP_REQUIRE(ctx, capacity >= 8 && (capacity & (capacity - 1)) == 0 && table, "bad table");
+  OLAP_REQUIRE(ctx, n == 0 || keys, "null keys");
+  OLAP_REQUIRE(ctx, d_sum || (out_rows && out_payload), "nothing to compute");
+  olap::Arena ar(ctx);
+  const uint64_t mask = static_cast<uint64_t>(capacity - 1);
+  if (d_sum) {
+    unsigned long long* m = d_matches ? reinterpret_cast<unsigned long long*>(d_matches)
+                                      : ar.take<unsigned long long>(1);
+    if (!m) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
+    OLAP_CUDA_TRY(ctx, cudaMemsetAsync(d_sum, 0, sizeof(int64_t), ctx->stream));
+    OLAP_CUDA_TRY(ctx, cudaMemsetAsync(m, 0, sizeof(int64_t), ctx->stream));
+    if (n)
+      olap::hash_probe_sum_kernel<<<olap::grid_for(ctx, (n + 3) / 4, 512), 512, 0, ctx->stream>>>(
+          keys, n, table, mask, olap::al16(keys), reinterpret_cast<unsigned long long*>(d_sum), m);
+    OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  }
+  if (out_rows && out_payload) {
+    olap::ProbeOp op;
+    std::memset(&op, 0, sizeof(op));
+    op.keys = keys;
+    op.slots = table;
+    op.mask = mask;
+    op.out_rows = out_rows;
+    op.out_payload = out_payload;
+    op.vec = olap::al16(keys);
+    olap::ScanTiles st;
+    unsigned long long* total = (!d_sum && d_matches) ? reinterpret_cast<unsigned long long*>(d_matches)
+                                                      : ar.take<unsigned long long>(1);
+    if (!total) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
+    int rc = olap::make_scan_tiles(ctx, ar, n, total, ctx->stream, &st);
+    if (rc != OLAP_OK) return rc;
+    olap::compact_kernel<olap::ProbeOp><<<olap::compact_grid(ctx, st.n_tiles), olap::kCompactThreads, 0,
+                                         ctx->stream>>>(op, n, st);
+    OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  }
+  return OLAP_OK;
+}
+
+int olap_vecjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* payload, int64_t n,
+                       int32_t* vector, int64_t vector_len) {
+  if (!ctx) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_REQUIRE(ctx, n >= 0 && vector_len >= 1 && vector, "bad sizes or null vector");
+  OLAP_REQUIRE(ctx, n == 0 || (keys && payload), "null keys or payload");
+  if (n == 0) return OLAP_OK;
+  // 64-bit staging (row + 1 per key) from the stream-ordered pool.
+  unsigned long long* stage = nullptr;
+  OLAP_CUDA_TRY(ctx, cudaMallocAsync(reinterpret_cast<void**>(&stage), sizeof(unsigned long long) * vector_len,
+                                     ctx->stream));
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(stage, 0, sizeof(unsigned long long) * vector_len, ctx->stream));
+  olap::vec_build_stage_kernel<<<olap::grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(
+      keys, n, stage, vector_len, &ctx->counters->range_errors);
+  olap::vec_build_write_kernel<<<olap::grid_for(ctx, vector_len, 256), 256, 0, ctx->stream>>>(
+      stage, vector_len, payload, vector);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(stage, ctx->stream);
+  if (e != cudaSuccess) return olap::check_cuda(ctx, e, "vecjoin build");
+  return OLAP_OK;
+}
+
+int olap_vecjoin_probe(olap_ctx* ctx, const int32_t* keys, int64_t n, const int32_t* vector,
+                       int64_t vector_len, int64_t* d_sum) {
+  if (!ctx) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_REQUIRE(ctx, n >= 0 && vector_len >= 1 && vector && d_sum, "bad arguments");
+  OLAP_REQUIRE(ctx, n == 0 || keys, "null keys");
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(d_sum, 0, sizeof(int64_t), ctx->stream));
+  if (n == 0) return OLAP_OK;
+  olap::vec_probe_kernel<<<olap::grid_for(ctx, (n + 3) / 4, 512), 512, 0, ctx->stream>>>(
+      keys, n, vector, vector_len, olap::al16(keys), reinterpret_cast<unsigned long long*>(d_sum),
+      &ctx->counters->range_errors);
+  OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  return OLAP_OK;
+}
+
+}  // extern "C"

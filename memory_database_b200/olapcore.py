@@ -296,3 +296,70 @@ def OLAPcore_vwm_sv(dimvec_array, fk_array, orders, dimvec_nums, factor, size_li
     """``OLAPcore_vwm_sv`` (test_multi_compute_operator.cpp:1258) on the B200."""
     return _olapcore(dimvec_array, fk_array, orders, dimvec_nums, factor, size_lineorder,
                      group_nums, M1, M2, nthreads, **kw)
+
+
+# ---- column-wise model (device tensors, reference argument layout) -----------
+
+def _tables(dimvec_array, fk_array, dimvec_len):
+    dv = (C.c_void_p * 4)(*[_ptr(x) for x in list(dimvec_array) + [None] * (4 - len(dimvec_array))])
+    fk = (C.c_void_p * 4)(*[_ptr(x) for x in list(fk_array) + [None] * (4 - len(fk_array))])
+    lens = [(_nelem(d) if d is not None else 0) for d in dimvec_array] if dimvec_len is None else list(dimvec_len)
+    ln = (C.c_int64 * 4)(*(lens + [0] * (4 - len(lens))))
+    return dv, fk, ln
+
+
+def join_cwm_sv(dimvec_array, fk_array, orders, dimvec_nums, groupID, factor, size_lineorder,
+                nthreads=None, *, dimvec_len=None, ctx: Context | None = None) -> None:
+    """``join_cwm_sv`` (test_multi_compute_operator.cpp:908): fills the int16
+    static vector ``groupID`` (GROUP_NULL for dropped rows)."""
+    ctx = ctx or default_context()
+    ctx.follow_torch_stream()
+    dv, fk, ln = _tables(dimvec_array, fk_array, dimvec_len)
+    o = (C.c_int * 4)(*list(orders)[:4])
+    f = (C.c_int * 4)(*list(factor)[:4])
+    check(lib.olap_join_cwm_sv(ctx.handle, dv, ln, fk, o, int(dimvec_nums), _ptr(groupID), f, int(size_lineorder)),
+          ctx.handle)
+
+
+def agg_cwm_sv(groupID, size_lineorder, M1, M2, group_nums, nthreads=None, *, group_vector=None,
+               ctx: Context | None = None) -> int:
+    """``agg_cwm_sv`` (:764): SUM(M1+M2) by groupID; returns the total."""
+    torch = _torch()
+    ctx = ctx or default_context()
+    ctx.follow_torch_stream()
+    gv = group_vector if group_vector is not None else torch.empty(int(group_nums), dtype=torch.int64,
+                                                                   device=groupID.device)
+    cnt = torch.zeros(1, dtype=torch.int64, device=groupID.device)
+    check(lib.olap_agg_cwm_sv(ctx.handle, _ptr(groupID), int(size_lineorder), _ptr(M1), _ptr(M2), int(group_nums),
+                              _ptr(gv), _ptr(cnt)), ctx.handle)
+    return int(cnt.item())
+
+
+def join_cwm_dv(dimvec_array, fk_array, orders, dimvec_nums, OID, groupID, factor, size_lineorder,
+                nthreads=None, *, dimvec_len=None, ctx: Context | None = None) -> int:
+    """``join_cwm_dv`` (:840): surviving rows as (OID, groupID) in row order;
+    returns their number (the reference's ``index``)."""
+    torch = _torch()
+    ctx = ctx or default_context()
+    ctx.follow_torch_stream()
+    dv, fk, ln = _tables(dimvec_array, fk_array, dimvec_len)
+    o = (C.c_int * 4)(*list(orders)[:4])
+    f = (C.c_int * 4)(*list(factor)[:4])
+    idx = torch.zeros(1, dtype=torch.int64, device=OID.device)
+    check(lib.olap_join_cwm_dv(ctx.handle, dv, ln, fk, o, int(dimvec_nums), _ptr(OID), _ptr(groupID), f, _ptr(idx),
+                               int(size_lineorder)), ctx.handle)
+    return int(idx.item())
+
+
+def agg_cwm_dv(OID, groupID, index, M1, M2, size_lineorder, group_nums, nthreads=None, *, group_vector=None,
+               ctx: Context | None = None) -> int:
+    """``agg_cwm_dv`` (:685): SUM(M1[OID]+M2[OID]) by groupID; returns the total."""
+    torch = _torch()
+    ctx = ctx or default_context()
+    ctx.follow_torch_stream()
+    gv = group_vector if group_vector is not None else torch.empty(int(group_nums), dtype=torch.int64,
+                                                                   device=OID.device)
+    cnt = torch.zeros(1, dtype=torch.int64, device=OID.device)
+    check(lib.olap_agg_cwm_dv(ctx.handle, _ptr(OID), _ptr(groupID), int(index), _ptr(M1), _ptr(M2),
+                              int(size_lineorder), int(group_nums), _ptr(gv), _ptr(cnt)), ctx.handle)
+    return int(cnt.item())

@@ -42,6 +42,29 @@ def _load_oracle() -> C.CDLL:
     lib.oracle_size_of_table.argtypes = [C.c_int, C.c_double]
     lib.oracle_size_of_table.restype = C.c_int
     lib.oracle_gen_olapcore_compat.argtypes = [C.c_double, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    lib.oracle_select_rowids.argtypes = [_vp, _i64, _i32, C.c_int, _vp, _i64, _vp, C.POINTER(_i64)]
+    lib.oracle_select_rowids.restype = _i64
+    lib.oracle_select_bitmap.argtypes = [_vp, _i64, _i32, C.c_int, _vp]
+    lib.oracle_selalgo.argtypes = [_i32, _i64, _vp, _vp, _vp, _vp, C.POINTER(_i64)]
+    lib.oracle_selalgo.restype = _i64
+    lib.oracle_project_pairs.argtypes = [_i32, _i64, _vp, _vp, _vp, _vp]
+    lib.oracle_project_pairs.restype = _i64
+    lib.oracle_gather.argtypes = [_vp, _i64, C.c_int, _vp, _i64, _vp]
+    lib.oracle_gather.restype = _i64
+    lib.oracle_vecjoin.argtypes = [_vp, _vp, _i64, _vp, _i64, _vp, _i64, C.POINTER(_i64)]
+    lib.oracle_vecjoin.restype = _i64
+    lib.oracle_hashjoin.argtypes = [_vp, _vp, _i64, _vp, _i64, C.POINTER(_i64), _vp, _vp]
+    lib.oracle_hashjoin.restype = _i64
+    lib.oracle_vector_group.argtypes = [_i64, _vp, _vp, _vp, _i64, _vp, _vp, C.POINTER(_i64)]
+    lib.oracle_vector_group.restype = _i64
+    lib.oracle_agg_fixed.argtypes = [_i64, _vp, _vp, _vp]
+    lib.oracle_agg_fixed.restype = _i64
+    lib.oracle_agg_f64.argtypes = [_i64, _vp, _vp, _vp]
+    lib.oracle_agg_f64.restype = C.c_double
+    lib.oracle_join_cwm_sv.argtypes = [C.c_int, _vp, _vp, _vp, _vp, _i64, _vp]
+    lib.oracle_join_cwm_sv.restype = _i64
+    lib.oracle_starjoin_cwm_sv.argtypes = [_vp, _vp, _vp, _i64, _vp]
+    lib.oracle_starjoin_cwm_sv.restype = _i64
     return lib
 
 
@@ -154,3 +177,141 @@ def gen_olapcore_compat(sf, sele, bitmap, groups, use_reference=False):
         oracle_lib().oracle_gen_olapcore_compat(float(sf), _p(s), _p(b), _p(g), _ptr_array(dv),
                                                 _ptr_array(fk), _p(m1), _p(m2))
     return dv, fk, m1, m2
+
+
+# ---- operators -----------------------------------------------------------------
+
+def _c32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def select_rowids(col, val, cmp=0, in_rowids=None):
+    """(row ids, range_errors) of sel_lt_T_fsel_independent_val_branching."""
+    col = _c32(col)
+    n_in = 0 if in_rowids is None else len(in_rowids)
+    ir = None if in_rowids is None else _c32(in_rowids)
+    out = np.zeros(max(len(col) if ir is None else n_in, 1), np.int32)
+    err = _i64()
+    k = oracle_lib().oracle_select_rowids(_p(col), len(col), int(val), int(cmp), None if ir is None else _p(ir),
+                                          n_in, _p(out), C.byref(err))
+    return out[:k], err.value
+
+
+def select_bitmap(col, val, cmp=0):
+    col = _c32(col)
+    bits = np.zeros(max((len(col) + 31) // 32, 1), np.uint32)
+    oracle_lib().oracle_select_bitmap(_p(col), len(col), int(val), int(cmp), _p(bits))
+    return bits[: (len(col) + 31) // 32]
+
+
+def selalgo(cond, ra, rb, rc, rd):
+    a, b, c, d = map(_c32, (ra, rb, rc, rd))
+    cnt = _i64()
+    s = oracle_lib().oracle_selalgo(int(cond), len(a), _p(a), _p(b), _p(c), _p(d), C.byref(cnt))
+    return s, cnt.value
+
+
+def project_pairs(cond, ra, rc):
+    a, c = _c32(ra), _c32(rc)
+    oa = np.zeros(max(len(a), 1), np.int32)
+    oc = np.zeros(max(len(a), 1), np.int32)
+    k = oracle_lib().oracle_project_pairs(int(cond), len(a), _p(a), _p(c), _p(oa), _p(oc))
+    return oa[:k], oc[:k]
+
+
+def gather(rowids, cols):
+    r = _c32(rowids)
+    cs = [_c32(c) for c in cols]
+    outs = [np.zeros(max(len(r), 1), np.int32) for _ in cs]
+    errs = oracle_lib().oracle_gather(_p(r), len(r), len(cs), (C.c_void_p * len(cs))(*[_p(c) for c in cs]),
+                                      len(cs[0]), (C.c_void_p * len(cs))(*[_p(o) for o in outs]))
+    return [o[: len(r)] for o in outs], errs
+
+
+def vecjoin(rk, rp, sk, vector_len, initial=None):
+    rk, rp, sk = _c32(rk), _c32(rp), _c32(sk)
+    vec = np.zeros(vector_len, np.int32) if initial is None else _c32(initial).copy()
+    err = _i64()
+    s = oracle_lib().oracle_vecjoin(_p(rk), _p(rp), len(rk), _p(sk), len(sk), _p(vec), vector_len, C.byref(err))
+    return s, vec, err.value
+
+
+def hashjoin(rk, rp, sk, want_pairs=False):
+    rk, rp, sk = _c32(rk), _c32(rp), _c32(sk)
+    m = _i64()
+    rows = np.zeros(max(len(sk), 1), np.int32) if want_pairs else None
+    pay = np.zeros(max(len(sk), 1), np.int32) if want_pairs else None
+    s = oracle_lib().oracle_hashjoin(_p(rk), _p(rp), len(rk), _p(sk), len(sk), C.byref(m),
+                                     None if rows is None else _p(rows), None if pay is None else _p(pay))
+    if want_pairs:
+        return s, m.value, rows[: m.value], pay[: m.value]
+    return s, m.value
+
+
+def vector_group(idx, m1, m2, G, want_counts=True):
+    idx, m1, m2 = _c32(idx), _c32(m1), _c32(m2)
+    gv = np.zeros(G, np.int64)
+    cnt = np.zeros(G, np.int64) if want_counts else None
+    err = _i64()
+    tot = oracle_lib().oracle_vector_group(len(idx), _p(idx), _p(m1), _p(m2), G, _p(gv),
+                                           None if cnt is None else _p(cnt), C.byref(err))
+    return tot, gv, cnt, err.value
+
+
+def agg_fixed(price, qty, tax):
+    p, q, t = _c32(price), _c32(qty), _c32(tax)
+    return oracle_lib().oracle_agg_fixed(len(p), _p(p), _p(q), _p(t))
+
+
+def agg_f64(tax, qty, price):
+    t, q, p = (np.ascontiguousarray(x, dtype=np.float64) for x in (tax, qty, price))
+    return oracle_lib().oracle_agg_f64(len(t), _p(t), _p(q), _p(p))
+
+
+def join_cwm_sv(dimvecs, lens, fks, factors, n):
+    nd = len(dimvecs)
+    dv = [np.ascontiguousarray(d, dtype=np.int8) for d in dimvecs]
+    fk = [_c32(f) for f in fks]
+    ln = np.array(list(lens) + [0] * (4 - nd), np.int64)
+    fac = np.array(list(factors) + [0] * (4 - nd), np.int32)
+    gid = np.zeros(max(n, 1), np.int16)
+    errs = oracle_lib().oracle_join_cwm_sv(nd, _ptr_array(dv), _p(ln), _ptr_array(fk), _p(fac), n, _p(gid))
+    return gid[:n], errs
+
+
+def starjoin_cwm_sv(dimvecs, lens, fks, n):
+    dv = [np.ascontiguousarray(d, dtype=np.int8) for d in dimvecs]
+    fk = [_c32(f) for f in fks]
+    ln = np.array(list(lens), np.int64)
+    res = np.zeros(max(n, 1), np.int32)
+    c = oracle_lib().oracle_starjoin_cwm_sv(_ptr_array(dv), _p(ln), _ptr_array(fk), n, _p(res))
+    return c, res[:n]
+
+
+def ref_module(name: str) -> C.CDLL:
+    """The reference's own operator module (select, join, group, aggregation,
+    starjoin) compiled from its sources into oracle/_ref."""
+    path = HERE / "_ref" / f"libref_{name}.so"
+    if not path.exists():
+        raise FileNotFoundError(f"{path} not built (needs the reference tree)")
+    lib = C.CDLL(str(path))
+    if name == "select":
+        lib.ref_selalgo_rowwise.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp, _vp]
+        lib.ref_sel_fsel_branching.argtypes = [C.c_int, _vp, _vp, C.c_int, _vp]
+        lib.ref_sel_fsel_non_branching.argtypes = [C.c_int, _vp, _vp, C.c_int, _vp]
+        lib.ref_sel_bmp.argtypes = [C.c_int, _vp, _vp, C.c_int]
+    elif name == "join":
+        lib.ref_vecjoin.argtypes = [_vp, _vp, C.c_uint64, _vp, C.c_uint64, _vp]
+        lib.ref_hashjoin.argtypes = [_vp, _vp, C.c_uint64, _vp, C.c_uint64]
+    elif name == "group":
+        lib.ref_vector_group.argtypes = [C.c_uint64, _vp, _vp, _vp, _vp, C.c_int]
+        lib.ref_vector_group.restype = _i64
+        lib.ref_hashtable_group.argtypes = [C.c_uint64, _vp, _vp, _vp]
+        lib.ref_hashtable_group.restype = _i64
+    elif name == "aggregation":
+        lib.ref_aggalgo_rowwise.argtypes = [C.c_int, _vp, _vp, _vp]
+        lib.ref_aggalgo_rowwise.restype = C.c_double
+    elif name == "starjoin":
+        lib.ref_starjoin_rowwise.argtypes = [C.c_int] + [_vp] * 8
+        lib.ref_starjoin_cwm_sv.argtypes = [C.c_int] + [_vp] * 9
+    return lib

@@ -177,3 +177,218 @@ int oracle_gen_olapcore_compat(double sf, const double* sele, const int* bitmap,
   }
   return 0;
 }
+
+/* ---- operators (config 2) ----------------------------------------------- */
+
+enum { CMP_LE = 0, CMP_LT = 1 };
+static int cmp_pass(int32_t v, int32_t val, int cmp) { return cmp == CMP_LT ? v < val : v <= val; }
+
+/* sel_lt_T_fsel_independent_val_branching (select/test_select_option.cpp
+ * :391-423): row ids (or entries of the input selection vector) that pass,
+ * in order.  Input entries outside [0, col_len) are dropped and counted. */
+int64_t oracle_select_rowids(const int32_t* col, int64_t col_len, int32_t val, int cmp,
+                             const int32_t* in_rowids, int64_t n_in, int32_t* out,
+                             int64_t* range_errors) {
+  int64_t j = 0, errs = 0;
+  if (!in_rowids) {
+    for (int64_t i = 0; i < col_len; i++)
+      if (cmp_pass(col[i], val, cmp)) out[j++] = (int32_t)i;
+  } else {
+    for (int64_t i = 0; i < n_in; i++) {
+      const int32_t r = in_rowids[i];
+      if (r < 0 || r >= col_len) { errs++; continue; }
+      if (cmp_pass(col[r], val, cmp)) out[j++] = r;
+    }
+  }
+  if (range_errors) *range_errors = errs;
+  return j;
+}
+
+/* sel_lt_T_bmp_independent_val_branching (select:424-440), packed LSB first. */
+void oracle_select_bitmap(const int32_t* col, int64_t n, int32_t val, int cmp, uint32_t* bits) {
+  for (int64_t w = 0; w < (n + 31) / 32; w++) bits[w] = 0;
+  for (int64_t i = 0; i < n; i++)
+    if (cmp_pass(col[i], val, cmp)) bits[i >> 5] |= 1u << (i & 31);
+}
+
+/* selalgo_rowwise (select:450-467): SUM(Rd) over rows with Ra, Rb, Rc <= cond. */
+int64_t oracle_selalgo(int32_t cond, int64_t n, const int32_t* ra, const int32_t* rb,
+                       const int32_t* rc, const int32_t* rd, int64_t* count) {
+  int64_t s = 0, c = 0;
+  for (int64_t i = 0; i < n; i++)
+    if (ra[i] <= cond && rb[i] <= cond && rc[i] <= cond) {
+      s += rd[i];
+      c++;
+    }
+  if (count) *count = c;
+  return s;
+}
+
+/* proalgo_rowwise (project/test_project_option.cpp:34-49): pairs (Ra, Rc) of
+ * the rows with Ra <= cond and Rc <= cond, in row order. */
+int64_t oracle_project_pairs(int32_t cond, int64_t n, const int32_t* ra, const int32_t* rc,
+                             int32_t* out_a, int32_t* out_c) {
+  int64_t j = 0;
+  for (int64_t i = 0; i < n; i++)
+    if (ra[i] <= cond && rc[i] <= cond) {
+      out_a[j] = ra[i];
+      out_c[j] = rc[i];
+      j++;
+    }
+  return j;
+}
+
+/* Late materialisation: outs[c][i] = cols[c][rowids[i]] (0 when out of range). */
+int64_t oracle_gather(const int32_t* rowids, int64_t k, int ncols, const int32_t* const* cols,
+                      int64_t col_len, int32_t* const* outs) {
+  int64_t errs = 0;
+  for (int64_t i = 0; i < k; i++) {
+    const int32_t r = rowids[i];
+    const int ok = r >= 0 && r < col_len;
+    errs += !ok;
+    for (int c = 0; c < ncols; c++) outs[c][i] = ok ? cols[c][r] : 0;
+  }
+  return errs;
+}
+
+/* build + probe of join/test_join_option.cpp: vector[key] = payload in row
+ * order (:30-36, last row wins), then SUM vector[key] over the probe keys
+ * (:58-64).  Build keys outside [0, len) and probe keys outside [0, len) are
+ * counted in *range_errors and skipped.  vector must be zeroed (or hold the
+ * caller's initial values). */
+int64_t oracle_vecjoin(const int32_t* rk, const int32_t* rp, int64_t nr, const int32_t* sk, int64_t ns,
+                       int32_t* vector, int64_t len, int64_t* range_errors) {
+  int64_t errs = 0, s = 0;
+  for (int64_t i = 0; i < nr; i++) {
+    if (rk[i] < 0 || rk[i] >= len) { errs++; continue; }
+    vector[rk[i]] = rp[i];
+  }
+  for (int64_t i = 0; i < ns; i++) {
+    if (sk[i] < 0 || sk[i] >= len) { errs++; continue; }
+    s += vector[sk[i]];
+  }
+  if (range_errors) *range_errors = errs;
+  return s;
+}
+
+/* Hash join through a dictionary with the semantics of std::unordered_map
+ * (join:44-50, :90-96): last build row wins per key, a missing probe key adds
+ * 0.  Implemented with a private open-addressing table (keys INT32_MIN
+ * skipped as in the library); also returns the match count and, when
+ * out_rows is given, the matches (probe row, payload) in probe-row order. */
+int64_t oracle_hashjoin(const int32_t* rk, const int32_t* rp, int64_t nr, const int32_t* sk, int64_t ns,
+                        int64_t* matches, int32_t* out_rows, int32_t* out_payload) {
+  int64_t cap = 16;
+  while (cap < 2 * nr + 16) cap <<= 1;
+  int32_t* keys = (int32_t*)malloc(sizeof(int32_t) * cap);
+  int32_t* vals = (int32_t*)malloc(sizeof(int32_t) * cap);
+  for (int64_t i = 0; i < cap; i++) keys[i] = INT32_MIN;
+  for (int64_t i = 0; i < nr; i++) {
+    const int32_t k = rk[i];
+    if (k == INT32_MIN) continue;
+    uint64_t h = ((uint64_t)(uint32_t)k * 2654435761u) & (cap - 1);
+    while (keys[h] != INT32_MIN && keys[h] != k) h = (h + 1) & (cap - 1);
+    keys[h] = k;
+    vals[h] = rp[i];
+  }
+  int64_t s = 0, m = 0;
+  for (int64_t i = 0; i < ns; i++) {
+    const int32_t k = sk[i];
+    if (k == INT32_MIN) continue;
+    uint64_t h = ((uint64_t)(uint32_t)k * 2654435761u) & (cap - 1);
+    while (keys[h] != INT32_MIN && keys[h] != k) h = (h + 1) & (cap - 1);
+    if (keys[h] == k) {
+      s += vals[h];
+      if (out_rows) {
+        out_rows[m] = (int32_t)i;
+        out_payload[m] = vals[h];
+      }
+      m++;
+    }
+  }
+  free(keys);
+  free(vals);
+  if (matches) *matches = m;
+  return s;
+}
+
+/* vector_group (group/test_group_option.cpp:44-60) with int64 sums: 1-based
+ * group ids, returns the total; ids outside [1, G] counted and skipped. */
+int64_t oracle_vector_group(int64_t n, const int32_t* idx, const int32_t* m1, const int32_t* m2, int64_t G,
+                            int64_t* gv, int64_t* counts, int64_t* range_errors) {
+  int64_t tot = 0, errs = 0;
+  for (int64_t g = 0; g < G; g++) {
+    gv[g] = 0;
+    if (counts) counts[g] = 0;
+  }
+  for (int64_t i = 0; i < n; i++) {
+    const int64_t g = (int64_t)idx[i] - 1;
+    if (g < 0 || g >= G) { errs++; continue; }
+    const int64_t v = (int64_t)m1[i] + m2[i];
+    gv[g] += v;
+    if (counts) counts[g]++;
+    tot += v;
+  }
+  if (range_errors) *range_errors = errs;
+  return tot;
+}
+
+/* aggalgo in int64 fixed point: SUM price*qty*(100 + tax_pct) (mod 2^64). */
+int64_t oracle_agg_fixed(int64_t n, const int32_t* price, const int32_t* qty, const int32_t* tax) {
+  uint64_t s = 0;
+  for (int64_t i = 0; i < n; i++)
+    s += (uint64_t)((int64_t)price[i] * qty[i]) * (uint64_t)((int64_t)100 + tax[i]);
+  return (int64_t)s;
+}
+
+/* aggalgo_rowwise (aggregation/test_aggregation_option.cpp:28-37) in double. */
+double oracle_agg_f64(int64_t n, const double* tax, const double* qty, const double* price) {
+  double r = 0.0;
+  for (int64_t i = 0; i < n; i++) r += (price[i] * qty[i]) * tax[i] + price[i] * qty[i];
+  return r;
+}
+
+/* join_cwm_sv thread body (OLAPcore/test_multi_compute_operator.cpp:290-322)
+ * over all dimensions: int16 group id or GROUP_NULL; keys outside [0, len)
+ * give GROUP_NULL and are counted. */
+int64_t oracle_join_cwm_sv(int nd, const int8_t* const* dimvec, const int64_t* len, const int32_t* const* fk,
+                           const int32_t* factor, int64_t n, int16_t* gid) {
+  int64_t errs = 0;
+  for (int64_t r = 0; r < n; r++) {
+    int ok = 1;
+    for (int d = 0; d < nd; d++)
+      if (fk[d][r] < 0 || fk[d][r] >= len[d]) ok = 0;
+    if (!ok) { errs++; gid[r] = 32767; continue; }
+    int32_t g = 0;
+    for (int d = 0; d < nd && ok; d++) {
+      const int c = dimvec[d][fk[d][r]];
+      if (c == DIM_NULL) ok = 0;
+      else g += c * factor[d];
+    }
+    gid[r] = ok ? (int16_t)g : (int16_t)32767;
+  }
+  return errs;
+}
+
+/* starjoinalgo_cwm_sv (starjoin/test_starjoin_option.cpp:66-121) over the
+ * four tables in order customer, supplier, part, date; returns the count of
+ * entries that are not GROUP_NULL. */
+int64_t oracle_starjoin_cwm_sv(const int8_t* const* dimvec, const int64_t* len, const int32_t* const* fk,
+                               int64_t n, int32_t* result) {
+  static const int shift[4] = {12, 8, 4, 0};
+  int64_t c = 0;
+  for (int64_t r = 0; r < n; r++) {
+    int ok = 1;
+    for (int d = 0; d < 4; d++)
+      if (fk[d][r] < 0 || fk[d][r] >= len[d]) ok = 0;
+    int32_t g = 0;
+    for (int d = 0; d < 4 && ok; d++) {
+      const int v = dimvec[d][fk[d][r]];
+      if (v == DIM_NULL) ok = 0;
+      else g += v << shift[d];
+    }
+    result[r] = ok ? g : 32767;
+    c += result[r] != 32767;
+  }
+  return c;
+}

@@ -1,0 +1,262 @@
+"""GPU parity tests of the building-block operators (select, project, gather,
+hash and vector join, group-by, aggregation, the column-wise OLAP core and
+the star-join operator) against the CPU oracle: bit-exact for every integer
+result, 1e-12 relative for the double aggregation."""
+import numpy as np
+import pytest
+
+import oracle
+from memory_database_b200 import _lib, olapcore, operators as ops
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+@pytest.mark.parametrize("n", [0, 1, 3, 4, 5, 4095, 4096, 4097, 1_000_003])
+@pytest.mark.parametrize("cmp", [ops.CMP_LE, ops.CMP_LT])
+def test_select_rowids_and_bitmap(ctx, n, cmp):
+    rng = np.random.default_rng(n + cmp)
+    col = rng.integers(1, 1001, max(n, 1)).astype(np.int32)[:n]
+    for val in (0, 1, 10, 500, 1000):
+        ids = ops.select_rowids(dev(col), val, cmp, ctx=ctx)
+        exp, _ = oracle.select_rowids(col, val, cmp)
+        assert np.array_equal(host(ids), exp)
+        bm = ops.select_bitmap(dev(col), val, cmp, ctx=ctx)
+        assert np.array_equal(host(bm).view(np.uint32), oracle.select_bitmap(col, val, cmp))
+
+
+def test_select_chained_selection_vector(ctx):
+    rng = np.random.default_rng(7)
+    n = 777_777
+    a = rng.integers(1, 1001, n).astype(np.int32)
+    b = rng.integers(1, 1001, n).astype(np.int32)
+    ids = ops.select_rowids(dev(a), 300, ctx=ctx)
+    ids2 = ops.select_rowids(dev(b), 700, in_rowids=ids, ctx=ctx)
+    e1, _ = oracle.select_rowids(a, 300)
+    e2, _ = oracle.select_rowids(b, 700, in_rowids=e1)
+    assert np.array_equal(host(ids2), e2)
+    # the reference-named primitive with an input selection vector
+    res = torch.empty(len(e1), dtype=torch.int32, device="cuda")
+    k = ops.sel_lt_T_fsel_independent_val_branching(len(e1), res, dev(b), 700, if_sv=ids, ctx=ctx)
+    assert k == len(e2) and np.array_equal(host(res[:k]), e2)
+    # out-of-range entries of an input selection vector are dropped and counted
+    bad = dev(np.array([0, 5, -1, n, n + 7, 3], np.int32))
+    got = ops.select_rowids(dev(b), 1000, in_rowids=bad, ctx=ctx)
+    assert host(got).tolist() == [0, 5, 3] and ctx.take_range_errors() == 3
+
+
+@pytest.mark.parametrize("sel", [0.001, 0.01, 0.1, 0.5])
+def test_select_config2_selectivities(ctx, sel):
+    """col < t at the config's selectivities (values uniform in [0, 2^20))."""
+    n = 1 << 24
+    L = _lib.lib
+    col = torch.empty(n, dtype=torch.int32, device="cuda")
+    _lib.check(L.olap_gen_uniform_i32_dev(ctx.handle, col.data_ptr(), n, 42, 50, 0, (1 << 20) - 1), ctx.handle)
+    t = int(sel * (1 << 20))
+    ids = ops.select_rowids(col, t, ops.CMP_LT, ctx=ctx)
+    exp, _ = oracle.select_rowids(host(col), t, ops.CMP_LT)
+    assert np.array_equal(host(ids), exp)
+    # project gather of 4 columns by those row ids
+    cols = [torch.roll(col, k) for k in range(4)]
+    outs = ops.gather(ids, cols, ctx=ctx)
+    eo, _ = oracle.gather(exp, [host(c) for c in cols])
+    for o, e in zip(outs, eo):
+        assert np.array_equal(host(o), e)
+
+
+def test_selalgo_and_project(ctx):
+    rng = np.random.default_rng(8)
+    n = 2_000_003
+    cols = [rng.integers(1, 1001, n).astype(np.int32) for _ in range(4)]
+    d = [dev(c) for c in cols]
+    for cond in (1, 215, 464, 1000):
+        assert ops.selalgo_rowwise(cond, n, *d, ctx=ctx) == oracle.selalgo(cond, *cols)[0]
+        k, oa, oc = ops.proalgo_rowwise(cond, n, d[0], d[2], ctx=ctx)
+        ea, ec = oracle.project_pairs(cond, cols[0], cols[2])
+        assert k == len(ea) and np.array_equal(host(oa), ea) and np.array_equal(host(oc), ec)
+    # unaligned columns take the scalar paths
+    assert ops.selalgo_rowwise(500, n - 1, d[0][1:], d[1][1:], d[2][1:], d[3][1:], ctx=ctx) == \
+        oracle.selalgo(500, cols[0][1:], cols[1][1:], cols[2][1:], cols[3][1:])[0]
+    k, oa, oc = ops.proalgo_rowwise(500, n - 1, d[0][1:], d[2][1:], ctx=ctx)
+    ea, ec = oracle.project_pairs(500, cols[0][1:], cols[2][1:])
+    assert np.array_equal(host(oa), ea) and np.array_equal(host(oc), ec)
+
+
+def test_gather_out_of_range(ctx):
+    col = np.arange(100, dtype=np.int32) * 3
+    ids = np.array([0, 99, 100, -1, 50, 7, 7], np.int32)
+    out = ops.gather(dev(ids), [dev(col)], ctx=ctx)
+    assert host(out[0]).tolist() == [0, 297, 0, 0, 150, 21, 21]
+    assert ctx.take_range_errors() == 2
+
+
+@pytest.mark.parametrize("dist", ["uniform", "zipf"])
+def test_hash_join_config2_shape(ctx, dist):
+    """2^20-row build side of unique shuffled keys, 2^24 probe keys over the
+    build keys (uniform or Zipf(1.0)), half of them made non-matching."""
+    rng = np.random.default_rng(9)
+    R, S = 1 << 20, 1 << 24
+    rk = rng.permutation(np.arange(1, R + 1)).astype(np.int32)
+    rp = rng.integers(-1000, 1000, R).astype(np.int32)
+    L = _lib.lib
+    pos = torch.empty(S, dtype=torch.int32, device="cuda")
+    if dist == "zipf":
+        _lib.check(L.olap_gen_zipf_i32_dev(ctx.handle, pos.data_ptr(), S, 42, 60, R, 1.0), ctx.handle)
+    else:
+        _lib.check(L.olap_gen_uniform_i32_dev(ctx.handle, pos.data_ptr(), S, 42, 60, 0, R - 1), ctx.handle)
+    ctx.synchronize()
+    sk = rk[host(pos)]
+    sk = np.where(rng.random(S) < 0.5, sk, sk + 4 * R).astype(np.int32)
+    ht = ops.HashTable(R, ctx=ctx).build(dev(rk), dev(rp))
+    s, m = ht.probe(dev(sk))
+    es, em = oracle.hashjoin(rk, rp, sk)
+    assert (s, m) == (es, em)
+    rows, pay = ht.probe_pairs(dev(sk[:500_000]))
+    es2, em2, erows, epay = oracle.hashjoin(rk, rp, sk[:500_000], want_pairs=True)
+    assert np.array_equal(host(rows), erows) and np.array_equal(host(pay), epay)
+
+
+def test_hash_join_duplicates_and_edge_keys(ctx):
+    rng = np.random.default_rng(10)
+    rk = rng.integers(-5000, 5000, 100_000).astype(np.int32)  # many duplicates, negatives
+    rk[:3] = [np.iinfo(np.int32).min, np.iinfo(np.int32).max, 0]
+    rp = np.arange(len(rk), dtype=np.int32)  # payload = row: "last row wins" visible
+    sk = rng.integers(-6000, 6000, 300_001).astype(np.int32)
+    sk[:2] = [np.iinfo(np.int32).min, np.iinfo(np.int32).max]
+    ht = ops.HashTable(len(rk), ctx=ctx).build(dev(rk), dev(rp))
+    assert ctx.take_range_errors() == 1  # the INT32_MIN build key
+    assert ht.probe(dev(sk)) == oracle.hashjoin(rk, rp, sk)
+    empty = ops.HashTable(0, ctx=ctx).build(dev(rk[:0]), dev(rp[:0]))
+    assert empty.probe(dev(sk)) == (0, 0)
+
+
+def test_vector_join(ctx):
+    rng = np.random.default_rng(11)
+    R = 1 << 20
+    rk = rng.permutation(np.arange(1, R + 1)).astype(np.int32)
+    rk = np.concatenate([rk, rk[:1000], np.array([-1, R + 5], np.int32)])  # duplicates, out of range
+    rp = rng.integers(-100, 100, len(rk)).astype(np.int32)
+    sk = rng.integers(0, R + 3, 3_000_000).astype(np.int32)
+    vec = torch.zeros(R + 1, dtype=torch.int32, device="cuda")
+    ops.vecjoin_build(dev(rk), dev(rp), vec, ctx=ctx)
+    s = ops.vecjoin_probe(dev(sk), vec, ctx=ctx)
+    es, evec, eerr = oracle.vecjoin(rk, rp, sk, R + 1)
+    assert np.array_equal(host(vec), evec) and s == es and ctx.take_range_errors() == eerr
+
+
+@pytest.mark.parametrize("G", [16, 1 << 12, 1 << 20, 1 << 22])
+def test_group_by_config2_cardinalities(ctx, G):
+    n = 1 << 24
+    L = _lib.lib
+    idx = torch.empty(n, dtype=torch.int32, device="cuda")
+    m1 = torch.empty(n, dtype=torch.int32, device="cuda")
+    m2 = torch.empty(n, dtype=torch.int32, device="cuda")
+    _lib.check(L.olap_gen_uniform_i32_dev(ctx.handle, idx.data_ptr(), n, 42, 70, 1, G), ctx.handle)
+    _lib.check(L.olap_gen_uniform_i32_dev(ctx.handle, m1.data_ptr(), n, 42, 71, 1, 10000), ctx.handle)
+    _lib.check(L.olap_gen_uniform_i32_dev(ctx.handle, m2.data_ptr(), n, 42, 72, -5000, 5000), ctx.handle)
+    gv = torch.empty(G, dtype=torch.int64, device="cuda")
+    cnt = torch.empty(G, dtype=torch.int64, device="cuda")
+    tot = ops.vector_group(n, idx, m1, m2, gv, G, counts=cnt, ctx=ctx)
+    etot, egv, ecnt, _ = oracle.vector_group(host(idx), host(m1), host(m2), G)
+    assert tot == etot and np.array_equal(host(gv), egv) and np.array_equal(host(cnt), ecnt)
+    # hash group-by on the same keys (0-based as the reference's hashtable_group)
+    keys, sums, counts = ops.group_hash(idx, m1, m2, key_offset=-1, max_groups=G, ctx=ctx)
+    order = np.argsort(host(keys))
+    k = host(keys)[order]
+    present = np.nonzero(ecnt)[0]
+    assert np.array_equal(k, present.astype(np.int32))
+    assert np.array_equal(host(sums)[order], egv[present]) and np.array_equal(host(counts)[order], ecnt[present])
+    assert ops.hashtable_group(n, idx, m1, m2, max_groups=G, ctx=ctx) == etot
+
+
+def test_group_edge_cases(ctx):
+    idx = np.array([1, 2, 0, 5, 3, 2, -7], np.int32)
+    m = np.array([10, 20, 30, 40, 50, 60, 70], np.int32)
+    gv = torch.empty(4, dtype=torch.int64, device="cuda")
+    tot = ops.vector_group(len(idx), dev(idx), dev(m), dev(m), gv, 4, ctx=ctx)
+    etot, egv, _, eerr = oracle.vector_group(idx, m, m, 4)
+    assert tot == etot and np.array_equal(host(gv), egv) and ctx.take_range_errors() == eerr == 3
+    keys, sums, counts = ops.group_hash(dev(idx), dev(m), ctx=ctx)
+    got = sorted(zip(host(keys).tolist(), host(sums).tolist(), host(counts).tolist()))
+    exp = {}
+    for k, v in zip(idx.tolist(), m.tolist()):
+        s, c = exp.get(k, (0, 0))
+        exp[k] = (s + v, c + 1)
+    assert got == sorted((k, s, c) for k, (s, c) in exp.items())
+
+
+def test_aggregation(ctx):
+    rng = np.random.default_rng(12)
+    n = (1 << 24) + 3
+    tax = rng.integers(1, 21, n).astype(np.int32)
+    qty = rng.integers(1, 11, n).astype(np.int32)
+    price = rng.integers(5, 21, n).astype(np.int32)
+    assert ops.aggalgo_fixed(dev(price), dev(qty), dev(tax), ctx=ctx) == oracle.agg_fixed(price, qty, tax)
+    td, qd, pd = tax.astype(np.float64) / 100, qty.astype(np.float64), price.astype(np.float64)
+    got = ops.aggalgo_f64(n, dev(td), dev(qd), dev(pd), ctx=ctx)
+    exp = oracle.agg_f64(td, qd, pd)
+    assert abs(got - exp) <= 1e-12 * abs(exp)
+    assert got == ops.aggalgo_f64(n, dev(td), dev(qd), dev(pd), ctx=ctx)  # deterministic
+
+
+def test_column_wise_olapcore(ctx, golden_queries):
+    """join_cwm_sv/agg_cwm_sv and join_cwm_dv/agg_cwm_dv on the reference's
+    queries whose groups fit int16: same static vector as the oracle, same
+    (OID, groupID) lists as the row order of the survivors, same totals."""
+    for q in golden_queries:
+        if q["group_nums"] > 32766:
+            continue
+        dv, fk, m1, m2 = oracle.gen_olapcore_compat(1.0, q["sele"], q["bitmap"], q["groups"])
+        n, G = len(m1), q["group_nums"]
+        ddv, dfk = [dev(d) for d in dv], [dev(f) for f in fk]
+        gid = torch.empty(n, dtype=torch.int16, device="cuda")
+        olapcore.join_cwm_sv(ddv, dfk, q["orders"], q["dimvec_nums"], gid, q["factor"], n, ctx=ctx)
+        egid, _ = oracle.join_cwm_sv([dv[t] for t in q["orders"]], [len(dv[t]) for t in q["orders"]],
+                                     [fk[t] for t in q["orders"]], q["factor"], n)
+        assert np.array_equal(host(gid), egid)
+        gv = torch.empty(G, dtype=torch.int64, device="cuda")
+        tot = olapcore.agg_cwm_sv(gid, n, dev(m1), dev(m2), G, group_vector=gv, ctx=ctx)
+        assert tot == q["total_sf1_reference"]
+        oid = torch.empty(n, dtype=torch.int64, device="cuda")
+        gid2 = torch.empty(n, dtype=torch.int16, device="cuda")
+        k = olapcore.join_cwm_dv(ddv, dfk, q["orders"], q["dimvec_nums"], oid, gid2, q["factor"], n, ctx=ctx)
+        live = np.nonzero(egid != 32767)[0]
+        assert k == len(live) and np.array_equal(host(oid[:k]), live)
+        assert np.array_equal(host(gid2[:k]), egid[live])
+        gv2 = torch.empty(G, dtype=torch.int64, device="cuda")
+        assert olapcore.agg_cwm_dv(oid, gid2, k, dev(m1), dev(m2), n, G, group_vector=gv2, ctx=ctx) == tot
+        assert torch.equal(gv, gv2)
+
+
+def test_starjoin_operator(ctx):
+    rng = np.random.default_rng(13)
+    sizes = [30000, 2000, 200000, 2555]
+    n = 3_000_001
+    dv = []
+    for s in sizes:
+        c = rng.integers(0, 16, s + 1).astype(np.int8)
+        c[rng.random(s + 1) < 0.4] = 127
+        c[s] = 0
+        dv.append(c)
+    fk = [rng.integers(0, s + 1, n).astype(np.int32) for s in sizes]
+    lens = [s + 1 for s in sizes]
+    ddv, dfk = [dev(d) for d in dv], [dev(f) for f in fk]
+    _, tot, _ = oracle.starjoin(dv, fk, [0, 0, 0, 0], None, None, 1, aggs=(4,))
+    assert ops.starjoinalgo_rowwise(n, *ddv, *dfk, ctx=ctx) == int(tot[0])
+    res = torch.empty(n, dtype=torch.int32, device="cuda")
+    c = ops.starjoinalgo_cwm_sv(n, *ddv, *dfk, res, ctx=ctx)
+    ec, eres = oracle.starjoin_cwm_sv(dv, lens, fk, n)
+    assert c == ec and np.array_equal(host(res), eres)
+    k, pos, grp = ops.starjoinalgo_cwm_dv(n, *ddv, *dfk, ctx=ctx)
+    assert k == int(tot[0])
+    live = np.nonzero(eres != 32767)[0]
+    assert np.array_equal(np.intersect1d(host(pos), live), live)
+    assert np.array_equal(host(grp)[np.isin(host(pos), live)], eres[live])

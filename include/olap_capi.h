@@ -339,6 +339,52 @@ OLAP_API int olap_agg_fixed(olap_ctx* ctx, int64_t n, const int32_t* price, cons
 OLAP_API int olap_agg_f64(olap_ctx* ctx, int64_t n, const double* tax, const double* qty,
                           const double* price, double* d_sum);
 
+/* ---- dimension-vector builder and batched multi-query star-join -------------
+ * Dimension tables as attributes: per dimension row an int32 filter attribute
+ * and an int32 group attribute.  A query's predicate on a table is the range
+ * [lo, hi) on the filter attribute; its group code is the group attribute
+ * (grouped tables) or 0.  This is how the reference's generator bakes a
+ * query's dimension vector (include/gendata_util.hpp:449-542). */
+/* One query's int8 dimension vector: dimvec[k] = (lo <= filter[k] < hi) ?
+ * (use_group ? group[k] : 0) : DIM_NULL (a group value outside [0, 127) is a
+ * range error and gives DIM_NULL). */
+OLAP_API int olap_build_dimvec(olap_ctx* ctx, const int32_t* filter_attr, const int32_t* group_attr,
+                               int64_t n, int32_t lo, int32_t hi, int use_group, int8_t* dimvec);
+
+typedef struct olap_batch olap_batch;
+/* One query of a batch (tables 0 customer, 1 supplier, 2 part, 3 date). */
+typedef struct olap_batch_query {
+  int64_t row_begin;               /* fact range [row_begin, row_end)          */
+  int64_t row_end;
+  int32_t lo[OLAP_MAX_DIMS];       /* filter range [lo, hi) per table          */
+  int32_t hi[OLAP_MAX_DIMS];
+  int32_t factor[OLAP_MAX_DIMS];   /* group weight per grouped table           */
+  int32_t uses;                    /* bit t: table t participates              */
+  int32_t grouped;                 /* bit t: table t contributes its group     */
+  int64_t group_nums;              /* groups of this query                     */
+} olap_batch_query;
+
+/* A batch engine for up to max_queries (<= 256) queries per launch; holds the
+ * packed attribute records of the dimensions and two staging slots (so one
+ * batch can be prepared while the previous one runs). */
+OLAP_API int olap_batch_create(olap_ctx* ctx, int max_queries, olap_batch** out);
+OLAP_API int olap_batch_destroy(olap_batch* b);
+/* Attributes of table `table` (n rows; group_attr may be NULL = all 0). */
+OLAP_API int olap_batch_set_dimension(olap_batch* b, int table, const int32_t* filter_attr,
+                                      const int32_t* group_attr, int64_t n);
+/* Runs n_queries star-joins in one persistent launch over the shared fact
+ * table (fk[4], m1, m2 of n_rows rows), aggregate `agg` (OLAP_AGG_*) per
+ * query.  Query q's groups land in out[off_q .. off_q + group_nums_q), off_q
+ * the sum of the earlier queries' group_nums; totals[q] its total.  Per query
+ * the result equals olap_starjoin_groupsum over the dimension vectors of
+ * olap_build_dimvec.  use_graph: record the launch as a CUDA graph and replay
+ * it while the parameters stay the same.  Asynchronous on the context
+ * stream. */
+OLAP_API int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries,
+                            const int32_t* const* fk, const int32_t* m1, const int32_t* m2,
+                            int64_t n_rows, int agg, int64_t* out, int64_t out_slots, int64_t* totals,
+                            int use_graph);
+
 /* ---- seeded synthetic data (counter-based; identical on host and device) --
  * Value i of stream s under seed k is a pure function of (k, s, i), so any
  * slice can be generated anywhere.  _dev variants write device memory on the

@@ -51,6 +51,21 @@ class OlapError(RuntimeError):
         self.status = status
 
 
+class BatchQuery(C.Structure):
+    """Mirror of ``olap_batch_query``."""
+
+    _fields_ = [
+        ("row_begin", C.c_int64),
+        ("row_end", C.c_int64),
+        ("lo", C.c_int32 * MAX_DIMS),
+        ("hi", C.c_int32 * MAX_DIMS),
+        ("factor", C.c_int32 * MAX_DIMS),
+        ("uses", C.c_int32),
+        ("grouped", C.c_int32),
+        ("group_nums", C.c_int64),
+    ]
+
+
 class StarjoinQuery(C.Structure):
     """Mirror of ``olap_starjoin_query``."""
 
@@ -119,6 +134,11 @@ def _load() -> C.CDLL:
         "olap_starjoin_count": (C.c_int, [vp, i64, vp, vp, vp, vp]),
         "olap_starjoin_cwm_sv": (C.c_int, [vp, i64, vp, vp, vp, vp, vp]),
         "olap_starjoin_cwm_dv": (C.c_int, [vp, i64, vp, vp, vp, vp, vp, vp]),
+        "olap_build_dimvec": (C.c_int, [vp, vp, vp, i64, i32, i32, C.c_int, vp]),
+        "olap_batch_create": (C.c_int, [vp, C.c_int, C.POINTER(vp)]),
+        "olap_batch_destroy": (C.c_int, [vp]),
+        "olap_batch_set_dimension": (C.c_int, [vp, C.c_int, vp, vp, i64]),
+        "olap_batch_run": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, i64, C.c_int, vp, i64, vp, C.c_int]),
         "olap_gen_uniform_i32_dev": (C.c_int, [vp, vp, i64, u64, u64, i32, i32]),
         "olap_gen_uniform_i32": (C.c_int, [vp, i64, u64, u64, i32, i32, C.c_int]),
         "olap_gen_zipf_i32_dev": (C.c_int, [vp, vp, i64, u64, u64, i64, f64]),

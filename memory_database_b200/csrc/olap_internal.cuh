@@ -150,6 +150,11 @@ __device__ __forceinline__ int32_t ld_probe_s8(const int8_t* p, uint64_t pol) {
   asm("ld.global.nc.L2::cache_hint.s8 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
   return v;
 }
+__device__ __forceinline__ int2 ld_probe_i2(const int2* p, uint64_t pol) {
+  int2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.s32 {%0,%1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
 __device__ __forceinline__ int32_t ld_probe_s32(const int32_t* p, uint64_t pol) {
   int32_t v;
   asm("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));

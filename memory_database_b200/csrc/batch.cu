@@ -11,16 +11,22 @@
 // olap_build_dimvec materialises one query's int8 dimension vector from those
 // attributes (the input of the plain star-join).
 //
-// The batched kernel runs Q such queries in one persistent launch over the
-// shared fact table.  Each fact row is read once and each dimension it
-// references is probed once (one 8-byte attribute record per key, kept hot in
-// L2): the per-query work is then register arithmetic — the range tests, the
-// group id and the fact-range test — followed by an int64 atomic into the
-// query's own group vector for the rows that pass.  Per query the result is
-// bit-identical to the plain star-join over the dimension vectors that
-// olap_build_dimvec builds for it.
+// The batched path runs up to 64 such queries in one persistent pass over
+// the shared fact table, in two kernels:
+//  * per dimension row, a 64-bit mask of the queries whose predicate the row
+//    passes (a query that does not use the table passes every row), next to
+//    the row's group attribute: a 16-byte record, 74 MB for the four
+//    headline tables, kept hot in L2;
+//  * over the fact rows: each row's record is probed once per table (only
+//    while some live query still uses the table), the masks are ANDed with
+//    the mask of the queries whose fact range covers the row, and only the
+//    queries left in the mask do per-query work (group id, one int64 atomic).
+// Per query the result is bit-identical to the plain star-join over the
+// dimension vectors that olap_build_dimvec builds for it.
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "olap_internal.cuh"
 
@@ -56,7 +62,7 @@ __global__ void build_dimvec_kernel(const int32_t* __restrict__ filt, const int3
 // Device-side query descriptor of the batched kernel (one per query).
 struct BatchQuery {
   int64_t row_begin, row_end;
-  int32_t lo[OLAP_MAX_DIMS];      // filter range [lo, hi) per table; lo > hi: table unused
+  int32_t lo[OLAP_MAX_DIMS];      // filter range [lo, hi) per table
   int32_t hi[OLAP_MAX_DIMS];
   int32_t factor[OLAP_MAX_DIMS];  // group weight per table (0: not a group dimension)
   int32_t uses;                   // bit t: table t participates
@@ -65,16 +71,36 @@ struct BatchQuery {
   int64_t out_offset;             // first slot of this query in the shared output
 };
 
+constexpr int kMaxBatchQueries = 64;            // one bit per query in a 64-bit mask
+constexpr int kMaxSegments = 2 * kMaxBatchQueries + 2;
+
+// Everything a batch uploads (one pinned staging copy per slot).
+struct BatchDesc {
+  BatchQuery q[kMaxBatchQueries];
+  int64_t seg_begin[kMaxSegments];             // sorted; segment s = [seg_begin[s], seg_begin[s+1])
+  unsigned long long seg_mask[kMaxSegments];   // queries whose fact range covers segment s
+  unsigned long long uses_mask[OLAP_MAX_DIMS]; // queries using table t
+  int32_t n_queries;
+  int32_t n_seg;
+};
+
+struct DimRecord {
+  unsigned long long mask;  // bit q: the row passes query q's predicate on this table
+  int32_t grp;              // group attribute
+  int32_t pad;
+};
+
 struct BatchParams {
   const int2* attrs[OLAP_MAX_DIMS];   // packed attribute records per table
+  DimRecord* rec[OLAP_MAX_DIMS];      // per-batch query masks per table
   uint32_t dim_len[OLAP_MAX_DIMS];
   const int32_t* fk[OLAP_MAX_DIMS];
   const int32_t* m1;
   const int32_t* m2;
   int64_t n_rows;
-  const BatchQuery* queries;
-  int32_t n_queries;
+  const BatchDesc* desc;
   int32_t tables_used;                // union of the queries' `uses`
+  int32_t probe_order;                // 4 x 2-bit table ids, smallest table first
   int32_t agg;                        // OLAP_AGG_* of every query (one aggregate)
   unsigned long long* out;            // concatenated group vectors
   unsigned long long* totals;         // [n_queries]
@@ -82,7 +108,6 @@ struct BatchParams {
 };
 
 constexpr int kBatchThreads = 512;
-constexpr int kMaxBatchQueries = 256;
 
 __device__ __forceinline__ int64_t batch_value(int agg, int32_t x, int32_t y) {
   switch (agg) {
@@ -94,18 +119,74 @@ __device__ __forceinline__ int64_t batch_value(int agg, int32_t x, int32_t y) {
   }
 }
 
-// Persistent: SMs x blocks, each thread 4 rows per step (128-bit loads), the
-// query descriptors in shared memory, queries evaluated in a uniform loop.
-__global__ void __launch_bounds__(kBatchThreads) batch_starjoin_kernel(const BatchParams p) {
+// Query masks of the rows of table t.
+__global__ void __launch_bounds__(256) batch_records_kernel(const BatchParams p, int t) {
+  __shared__ int32_t slo[kMaxBatchQueries], shi[kMaxBatchQueries];
+  __shared__ unsigned long long s_uses, s_grouped;
+  const BatchDesc& D = *p.desc;
+  const int nq = D.n_queries;
+  if (threadIdx.x == 0) {
+    unsigned long long u = 0, g = 0;
+    for (int q = 0; q < nq; ++q) {
+      if ((D.q[q].uses >> t) & 1) u |= 1ull << q;
+      if ((D.q[q].grouped >> t) & 1) g |= 1ull << q;
+    }
+    s_uses = u;
+    s_grouped = g;
+  }
+  for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+    slo[q] = D.q[q].lo[t];
+    shi[q] = D.q[q].hi[t];
+  }
+  __syncthreads();
+  const unsigned long long uses = s_uses, grouped = s_grouped;
+  const unsigned long long all = nq == 64 ? ~0ull : ((1ull << nq) - 1);
+  const int64_t n = p.dim_len[t];
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += stride) {
+    const int2 a = p.attrs[t][k];
+    // a group value that is not an int8 code is DIM_NULL in the dimension
+    // vector the plain path builds
+    const bool code_ok = static_cast<uint32_t>(a.y) < static_cast<uint32_t>(OLAP_DIM_NULL);
+    unsigned long long m = all & ~uses;
+    for (int q = 0; q < nq; ++q) {
+      const bool pass = a.x >= slo[q] && a.x < shi[q] && (code_ok || !((grouped >> q) & 1));
+      m |= static_cast<unsigned long long>(pass && ((uses >> q) & 1)) << q;
+    }
+    DimRecord r;
+    r.mask = m;
+    r.grp = a.y;
+    r.pad = 0;
+    reinterpret_cast<ulonglong2*>(p.rec[t])[k] = make_ulonglong2(r.mask, static_cast<uint32_t>(r.grp));
+  }
+}
+
+__device__ __forceinline__ ulonglong2 ld_record(const DimRecord* r, uint64_t pol) {
+  ulonglong2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.u64 {%0,%1}, [%2], %3;" : "=l"(v.x), "=l"(v.y) : "l"(r), "l"(pol));
+  return v;
+}
+
+// The fact pass: persistent, 4 rows per thread per step (128-bit loads).
+__global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const BatchParams p) {
   __shared__ BatchQuery sq[kMaxBatchQueries];
+  __shared__ int64_t sseg[kMaxSegments];
+  __shared__ unsigned long long smask[kMaxSegments];
+  __shared__ unsigned long long suses[OLAP_MAX_DIMS];
   __shared__ unsigned long long stot[kMaxBatchQueries];
   __shared__ unsigned int s_bad;
+  const BatchDesc& D = *p.desc;
   const int tid = threadIdx.x;
-  const int nq = p.n_queries;
+  const int nq = D.n_queries, nseg = D.n_seg;
   for (int i = tid; i < nq; i += blockDim.x) {
-    sq[i] = p.queries[i];
+    sq[i] = D.q[i];
     stot[i] = 0;
   }
+  for (int i = tid; i < nseg; i += blockDim.x) {
+    sseg[i] = D.seg_begin[i];
+    smask[i] = D.seg_mask[i];
+  }
+  if (tid < OLAP_MAX_DIMS) suses[tid] = D.uses_mask[tid];
   if (tid == 0) s_bad = 0;
   __syncthreads();
   const uint64_t pol_stream = policy_evict_first();
@@ -113,25 +194,45 @@ __global__ void __launch_bounds__(kBatchThreads) batch_starjoin_kernel(const Bat
   const int agg = p.agg;
   const bool need_m1 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M1 || agg == OLAP_AGG_M1_TIMES_M2;
   const bool need_m2 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M2 || agg == OLAP_AGG_M1_TIMES_M2;
+  // The used tables in probe order (smallest first).
+  int tab[OLAP_MAX_DIMS] = {0, 0, 0, 0};
+  uint32_t tlen[OLAP_MAX_DIMS] = {0, 0, 0, 0};
+  unsigned long long tuses[OLAP_MAX_DIMS] = {0, 0, 0, 0};
+  int ntab = 0;
+#pragma unroll
+  for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
+    const int t = (p.probe_order >> (2 * o)) & 3;
+    if ((p.tables_used >> t) & 1) {
+#pragma unroll
+      for (int w = 0; w < OLAP_MAX_DIMS; ++w)
+        if (w == ntab) {
+          tab[w] = t;
+          tlen[w] = p.dim_len[t];
+          tuses[w] = suses[t];
+        }
+      ++ntab;
+    }
+  }
   unsigned int bad = 0;
-  const int64_t n4 = p.n_rows >> 2;
+  const int64_t n4 = (p.n_rows + 3) >> 2;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  // Rows 4i..4i+3 (the tail of n_rows % 4 rows is taken by i == n4).
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid; i <= n4; i += stride) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid; i < n4; i += stride) {
     const int64_t r0 = 4 * i;
     const int nv = r0 + 4 <= p.n_rows ? 4 : static_cast<int>(p.n_rows - r0);
-    if (nv <= 0) continue;
+    const bool full = nv == 4;
+    // Arrays are indexed by probe position o (table t = tab[o]), so that
+    // every index is a compile-time constant.
     int32_t key[OLAP_MAX_DIMS][4];
     int32_t x[4] = {0, 0, 0, 0}, y[4] = {0, 0, 0, 0};
-    const bool full = nv == 4;
 #pragma unroll
-    for (int t = 0; t < OLAP_MAX_DIMS; ++t) {
-      if (!((p.tables_used >> t) & 1)) continue;
+    for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
+      if (o >= ntab) continue;
+      const int32_t* f = p.fk[tab[o]];
       if (full) {
-        const int4 v = ld_stream_v4(p.fk[t] + r0, pol_stream);
-        key[t][0] = v.x; key[t][1] = v.y; key[t][2] = v.z; key[t][3] = v.w;
+        const int4 v = ld_stream_v4(f + r0, pol_stream);
+        key[o][0] = v.x; key[o][1] = v.y; key[o][2] = v.z; key[o][3] = v.w;
       } else {
-        for (int k = 0; k < 4; ++k) key[t][k] = k < nv ? p.fk[t][r0 + k] : 0;
+        for (int k = 0; k < 4; ++k) key[o][k] = k < nv ? f[r0 + k] : 0;
       }
     }
     if (need_m1) {
@@ -150,64 +251,69 @@ __global__ void __launch_bounds__(kBatchThreads) batch_starjoin_kernel(const Bat
         for (int k = 0; k < nv; ++k) y[k] = p.m2[r0 + k];
       }
     }
-    // One attribute probe per (row, table), shared by every query.
-    int2 at[OLAP_MAX_DIMS][4];
-    uint32_t valid = nv == 4 ? 0xFu : ((1u << nv) - 1u);
-    uint32_t inb[OLAP_MAX_DIMS];
-#pragma unroll
-    for (int t = 0; t < OLAP_MAX_DIMS; ++t) {
-      inb[t] = 0;
-      if (!((p.tables_used >> t) & 1)) continue;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const bool ok = ((valid >> k) & 1) && static_cast<uint32_t>(key[t][k]) < p.dim_len[t];
-        inb[t] |= static_cast<uint32_t>(ok) << k;
-        at[t][k] = ok ? ld_probe_i2(p.attrs[t] + key[t][k], pol_keep) : make_int2(0, 0);
-      }
+    // Queries whose fact range covers each row: segment of r0 by binary
+    // search, later rows step forward.
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sseg[mid] <= r0) lo = mid; else hi = mid - 1;
     }
-    for (int q = 0; q < nq; ++q) {
-      const BatchQuery& Q = sq[q];
-      uint32_t live = valid;
-      // fact range
+    unsigned long long m[4];
+    int s = lo;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      while (s + 1 < nseg && sseg[s + 1] <= r0 + k) ++s;
+      m[k] = k < nv ? smask[s] : 0ull;
+    }
+    // Keys out of range drop the row for the queries that use the table
+    // (counted once per such query, as the plain path counts them).
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (!m[k]) continue;
+      unsigned long long oob = 0;
+#pragma unroll
+      for (int o = 0; o < OLAP_MAX_DIMS; ++o)
+        if (o < ntab && static_cast<uint32_t>(key[o][k]) >= tlen[o]) oob |= tuses[o];
+      bad += __popcll(m[k] & oob);
+      m[k] &= ~oob;
+    }
+    // Probe the tables, smallest first, breadth-first across the 4 rows; a
+    // table is probed for a row only while a live query of the row uses it.
+    int32_t gr[OLAP_MAX_DIMS][4];
+#pragma unroll
+    for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
+      if (o >= ntab) continue;
+      const unsigned long long ut = tuses[o];
+      const DimRecord* rt = p.rec[tab[o]];
+      ulonglong2 rec[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k)
-        if (r0 + k < Q.row_begin || r0 + k >= Q.row_end) live &= ~(1u << k);
-      if (!live) continue;
-      // Every key the query uses is range-checked first (as in the plain
-      // star-join), then the predicates and the group id.
-      uint32_t oob = 0;
-#pragma unroll
-      for (int t = 0; t < OLAP_MAX_DIMS; ++t)
-        if ((Q.uses >> t) & 1) oob |= live & ~inb[t];
-      bad += __popc(oob);
-      live &= ~oob;
-      if (!live) continue;
-      int32_t g[4] = {0, 0, 0, 0};
-#pragma unroll
-      for (int t = 0; t < OLAP_MAX_DIMS; ++t) {
-        if (!((Q.uses >> t) & 1)) continue;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          bool pass = at[t][k].x >= Q.lo[t] && at[t][k].x < Q.hi[t];
-          if ((Q.grouped >> t) & 1) {
-            // a group value that is not an int8 code is DIM_NULL in the
-            // dimension vector the plain path would build
-            pass &= static_cast<uint32_t>(at[t][k].y) < static_cast<uint32_t>(OLAP_DIM_NULL);
-            g[k] += at[t][k].y * Q.factor[t];
-          }
-          if (!pass) live &= ~(1u << k);
-        }
-      }
-      if (!live) continue;
+        rec[k] = (m[k] & ut) ? ld_record(rt + key[o][k], pol_keep) : make_ulonglong2(~0ull, 0ull);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        if (!((live >> k) & 1)) continue;
-        if (static_cast<uint64_t>(static_cast<int64_t>(g[k])) >= static_cast<uint64_t>(Q.group_nums)) {
+        m[k] &= rec[k].x;
+        gr[o][k] = static_cast<int32_t>(static_cast<uint32_t>(rec[k].y));
+      }
+    }
+    // Per-query work only for the queries left in each row's mask.
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      unsigned long long mk = m[k];
+      if (!mk) continue;
+      const int64_t v = batch_value(agg, x[k], y[k]);
+      while (mk) {
+        const int q = __ffsll(static_cast<long long>(mk)) - 1;
+        mk &= mk - 1;
+        const BatchQuery& Q = sq[q];
+        int32_t g = 0;
+#pragma unroll
+        for (int o = 0; o < OLAP_MAX_DIMS; ++o)
+          if (o < ntab && ((Q.grouped >> tab[o]) & 1)) g += gr[o][k] * Q.factor[tab[o]];
+        if (static_cast<uint64_t>(static_cast<int64_t>(g)) >= static_cast<uint64_t>(Q.group_nums)) {
           ++bad;
           continue;
         }
-        const int64_t v = batch_value(agg, x[k], y[k]);
-        atomicAdd(&p.out[Q.out_offset + g[k]], static_cast<unsigned long long>(v));
+        atomicAdd(&p.out[Q.out_offset + g], static_cast<unsigned long long>(v));
         atomicAdd(&stot[q], static_cast<unsigned long long>(v));
       }
     }
@@ -231,21 +337,23 @@ static unsigned grid_n(const olap_ctx* ctx, int64_t n, int threads) {
 
 // Batch handle: two staging slots (pinned host and device descriptors, one
 // recorded graph each) so that one batch can be prepared while the previous
-// one runs; packed attribute records per table.
+// one runs; packed attribute records and query-mask records per table.
 struct olap_batch {
   olap_ctx* ctx = nullptr;
   int max_queries = 0;
-  olap::BatchQuery* d_queries[2] = {};  // device
-  olap::BatchQuery* h_queries[2] = {};  // pinned host staging
+  olap::BatchDesc* d_desc[2] = {};      // device
+  olap::BatchDesc* h_desc[2] = {};      // pinned host staging
   cudaEvent_t done[2] = {};             // recorded after each slot's batch
   bool pending[2] = {false, false};
   cudaGraph_t graph[2] = {};
   cudaGraphExec_t exec[2] = {};
   olap::BatchParams params[2];
   int64_t out_slots[2] = {0, 0};
+  int32_t nq_rec[2] = {0, 0};
   bool have_params[2] = {false, false};
   int64_t runs = 0;
   int2* attrs[OLAP_MAX_DIMS] = {};
+  olap::DimRecord* rec[OLAP_MAX_DIMS] = {};
   int64_t attr_len[OLAP_MAX_DIMS] = {};
 };
 
@@ -275,15 +383,15 @@ int olap_batch_create(olap_ctx* ctx, int max_queries, olap_batch** out) {
   b->max_queries = max_queries;
   bool ok = true;
   for (int s = 0; s < 2 && ok; ++s) {
-    ok &= cudaMalloc(&b->d_queries[s], sizeof(olap::BatchQuery) * max_queries) == cudaSuccess;
-    ok &= cudaMallocHost(&b->h_queries[s], sizeof(olap::BatchQuery) * max_queries) == cudaSuccess;
+    ok &= cudaMalloc(&b->d_desc[s], sizeof(olap::BatchDesc)) == cudaSuccess;
+    ok &= cudaMallocHost(&b->h_desc[s], sizeof(olap::BatchDesc)) == cudaSuccess;
     ok &= cudaEventCreateWithFlags(&b->done[s], cudaEventDisableTiming) == cudaSuccess;
   }
   if (!ok) {
     cudaGetLastError();
     for (int s = 0; s < 2; ++s) {
-      if (b->d_queries[s]) cudaFree(b->d_queries[s]);
-      if (b->h_queries[s]) cudaFreeHost(b->h_queries[s]);
+      if (b->d_desc[s]) cudaFree(b->d_desc[s]);
+      if (b->h_desc[s]) cudaFreeHost(b->h_desc[s]);
       if (b->done[s]) cudaEventDestroy(b->done[s]);
     }
     delete b;
@@ -300,12 +408,14 @@ int olap_batch_destroy(olap_batch* b) {
     if (b->pending[s]) cudaEventSynchronize(b->done[s]);
     if (b->exec[s]) cudaGraphExecDestroy(b->exec[s]);
     if (b->graph[s]) cudaGraphDestroy(b->graph[s]);
-    cudaFree(b->d_queries[s]);
-    cudaFreeHost(b->h_queries[s]);
+    cudaFree(b->d_desc[s]);
+    cudaFreeHost(b->h_desc[s]);
     cudaEventDestroy(b->done[s]);
   }
-  for (int t = 0; t < OLAP_MAX_DIMS; ++t)
+  for (int t = 0; t < OLAP_MAX_DIMS; ++t) {
     if (b->attrs[t]) cudaFree(b->attrs[t]);
+    if (b->rec[t]) cudaFree(b->rec[t]);
+  }
   delete b;
   return OLAP_OK;
 }
@@ -318,20 +428,22 @@ int olap_batch_set_dimension(olap_batch* b, int table, const int32_t* filter_att
   std::lock_guard<std::mutex> lk(ctx->mu);
   OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   if (b->attr_len[table] != n) {
-    if (b->attrs[table]) {
-      for (int s = 0; s < 2; ++s)
-        if (b->pending[s]) cudaEventSynchronize(b->done[s]);
-      cudaStreamSynchronize(ctx->stream);
-      cudaFree(b->attrs[table]);
-      b->attrs[table] = nullptr;
-    }
+    for (int s = 0; s < 2; ++s)
+      if (b->pending[s]) cudaEventSynchronize(b->done[s]);
+    cudaStreamSynchronize(ctx->stream);
+    if (b->attrs[table]) cudaFree(b->attrs[table]);
+    if (b->rec[table]) cudaFree(b->rec[table]);
+    b->attrs[table] = nullptr;
+    b->rec[table] = nullptr;
+    b->attr_len[table] = 0;
     OLAP_CUDA_TRY(ctx, cudaMalloc(&b->attrs[table], sizeof(int2) * n));
+    OLAP_CUDA_TRY(ctx, cudaMalloc(&b->rec[table], sizeof(olap::DimRecord) * n));
     b->attr_len[table] = n;
   }
   olap::pack_dim_attrs_kernel<<<olap::grid_n(ctx, n, 256), 256, 0, ctx->stream>>>(filter_attr, group_attr, n,
                                                                                  b->attrs[table]);
   OLAP_CUDA_TRY(ctx, cudaGetLastError());
-  b->have_params[0] = b->have_params[1] = false;  // recorded graphs refer to the old records
+  b->have_params[0] = b->have_params[1] = false;  // recorded graphs refer to the old buffers
   return OLAP_OK;
 }
 
@@ -352,12 +464,14 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
     OLAP_CUDA_TRY(ctx, cudaEventSynchronize(b->done[slot]));
     b->pending[slot] = false;
   }
+  olap::BatchDesc& D = *b->h_desc[slot];
+  std::memset(&D, 0, sizeof(D));
   int tables = 0;
   int64_t off = 0;
+  std::vector<int64_t> cuts = {0, n_rows};
   for (int q = 0; q < n_queries; ++q) {
     const olap_batch_query& in = queries[q];
-    olap::BatchQuery& d = b->h_queries[slot][q];
-    std::memset(&d, 0, sizeof(d));
+    olap::BatchQuery& d = D.q[q];
     OLAP_REQUIRE(ctx, in.row_begin >= 0 && in.row_end >= in.row_begin && in.row_end <= n_rows,
                  "query fact range outside the table");
     OLAP_REQUIRE(ctx, in.group_nums >= 1 && in.group_nums <= INT32_MAX, "group_nums must be in [1, 2^31)");
@@ -373,6 +487,7 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
       if (in.uses & (1 << t)) {
         OLAP_REQUIRE(ctx, b->attrs[t] && fk[t], "query uses a table without attributes or fk column");
         d.uses |= 1 << t;
+        D.uses_mask[t] |= 1ull << q;
         if (in.grouped & (1 << t)) {
           d.grouped |= 1 << t;
           gbound += 128 * std::llabs(static_cast<long long>(in.factor[t]));
@@ -382,39 +497,71 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
     OLAP_REQUIRE(ctx, gbound <= INT32_MAX, "group factors too large");
     tables |= d.uses;
     off += in.group_nums;
+    cuts.push_back(in.row_begin);
+    cuts.push_back(in.row_end);
   }
   OLAP_REQUIRE(ctx, off <= out_slots, "out holds fewer slots than the queries' groups");
+  // Fact-range segments: between consecutive cut points the set of queries
+  // whose range covers a row is constant.
+  std::sort(cuts.begin(), cuts.end());
+  cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
+  int nseg = 0;
+  for (size_t c = 0; c + 1 < cuts.size(); ++c) {
+    unsigned long long m = 0;
+    for (int q = 0; q < n_queries; ++q)
+      if (D.q[q].row_begin <= cuts[c] && cuts[c + 1] <= D.q[q].row_end) m |= 1ull << q;
+    D.seg_begin[nseg] = cuts[c];
+    D.seg_mask[nseg] = m;
+    ++nseg;
+  }
+  if (nseg == 0) {  // empty table
+    D.seg_begin[0] = 0;
+    D.seg_mask[0] = 0;
+    nseg = 1;
+  }
+  D.n_queries = n_queries;
+  D.n_seg = nseg;
   olap::BatchParams p;
   std::memset(&p, 0, sizeof(p));
+  int order[OLAP_MAX_DIMS] = {0, 1, 2, 3};
+  std::stable_sort(order, order + OLAP_MAX_DIMS, [&](int x, int y) { return b->attr_len[x] < b->attr_len[y]; });
+  for (int o = 0; o < OLAP_MAX_DIMS; ++o) p.probe_order |= order[o] << (2 * o);
   for (int t = 0; t < OLAP_MAX_DIMS; ++t) {
     p.attrs[t] = b->attrs[t];
+    p.rec[t] = b->rec[t];
     p.dim_len[t] = static_cast<uint32_t>(b->attr_len[t]);
     p.fk[t] = fk[t];
   }
   p.m1 = m1;
   p.m2 = m2;
   p.n_rows = n_rows;
-  p.queries = b->d_queries[slot];
-  p.n_queries = n_queries;
+  p.desc = b->d_desc[slot];
   p.tables_used = tables;
   p.agg = agg;
   p.out = reinterpret_cast<unsigned long long*>(out);
   p.totals = reinterpret_cast<unsigned long long*>(totals);
   p.range_err = &ctx->counters->range_errors;
-  const bool need_m = agg != OLAP_AGG_COUNT;
-  OLAP_REQUIRE(ctx, !need_m || n_rows == 0 || (m1 || m2), "measure columns required");
+  const bool need_m1 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M1 || agg == OLAP_AGG_M1_TIMES_M2;
+  const bool need_m2 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M2 || agg == OLAP_AGG_M1_TIMES_M2;
+  OLAP_REQUIRE(ctx, n_rows == 0 || ((!need_m1 || m1) && (!need_m2 || m2)), "measure columns required");
   int bps = 1;
-  OLAP_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, olap::batch_starjoin_kernel,
+  OLAP_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, olap::batch_scan_kernel,
                                                                    olap::kBatchThreads, 0));
   const unsigned grid = static_cast<unsigned>(ctx->sm_count) * static_cast<unsigned>(bps < 1 ? 1 : bps);
-  // The work of one batch: descriptors H2D, zero outputs, one persistent launch.
-  auto enqueue = [&](cudaStream_t s) -> cudaError_t {
-    cudaError_t e = cudaMemcpyAsync(b->d_queries[slot], b->h_queries[slot],
-                                    sizeof(olap::BatchQuery) * n_queries, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(out, 0, sizeof(int64_t) * off, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(totals, 0, sizeof(int64_t) * n_queries, s);
+  // The work of one batch: descriptors H2D, zero outputs, query masks of the
+  // used tables, one persistent pass over the fact table.
+  auto enqueue = [&](cudaStream_t st) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(b->d_desc[slot], b->h_desc[slot], sizeof(olap::BatchDesc),
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(out, 0, sizeof(int64_t) * off, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(totals, 0, sizeof(int64_t) * n_queries, st);
+    for (int t = 0; t < OLAP_MAX_DIMS && e == cudaSuccess; ++t) {
+      if (!((tables >> t) & 1)) continue;
+      olap::batch_records_kernel<<<olap::grid_n(ctx, b->attr_len[t], 256), 256, 0, st>>>(p, t);
+      e = cudaGetLastError();
+    }
     if (e == cudaSuccess && n_rows > 0) {
-      olap::batch_starjoin_kernel<<<grid, olap::kBatchThreads, 0, s>>>(p);
+      olap::batch_scan_kernel<<<grid, olap::kBatchThreads, 0, st>>>(p);
       e = cudaGetLastError();
     }
     return e;
@@ -422,10 +569,11 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
   if (!use_graph) {
     OLAP_CUDA_TRY(ctx, enqueue(ctx->stream));
   } else {
-    // Graph of this slot: re-captured when the launch parameters change,
-    // replayed otherwise (its copy node reads the slot's pinned staging).
+    // Graph of this slot: re-captured when the launch shape changes, replayed
+    // otherwise (its copy node reads the slot's pinned staging).
     const bool same = b->have_params[slot] && b->exec[slot] &&
-                      std::memcmp(&b->params[slot], &p, sizeof(p)) == 0 && b->out_slots[slot] == off;
+                      std::memcmp(&b->params[slot], &p, sizeof(p)) == 0 && b->out_slots[slot] == off &&
+                      b->nq_rec[slot] == n_queries;
     if (!same) {
       if (b->exec[slot]) cudaGraphExecDestroy(b->exec[slot]);
       if (b->graph[slot]) cudaGraphDestroy(b->graph[slot]);
@@ -445,6 +593,7 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
       if (e != cudaSuccess) return olap::check_cuda(ctx, e, "batch graph capture");
       b->params[slot] = p;
       b->out_slots[slot] = off;
+      b->nq_rec[slot] = n_queries;
       b->have_params[slot] = true;
     }
     OLAP_CUDA_TRY(ctx, cudaGraphLaunch(b->exec[slot], ctx->stream));

@@ -69,9 +69,12 @@ struct BatchQuery {
   int32_t grouped;                // bit t: table t contributes its group attribute
   int64_t group_nums;
   int64_t out_offset;             // first slot of this query in the shared output
+  int32_t smem_off;               // first slot of its per-block accumulators, or -1
+  int32_t pad;
 };
 
-constexpr int kMaxBatchQueries = 64;            // one bit per query in a 64-bit mask
+constexpr int kMaxBatchQueries = 64;
+constexpr int kBatchSmemSlots = 4096;           // 32 KiB of per-block int64 accumulators            // one bit per query in a 64-bit mask
 constexpr int kMaxSegments = 2 * kMaxBatchQueries + 2;
 
 // Everything a batch uploads (one pinned staging copy per slot).
@@ -173,15 +176,13 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
   __shared__ int64_t sseg[kMaxSegments];
   __shared__ unsigned long long smask[kMaxSegments];
   __shared__ unsigned long long suses[OLAP_MAX_DIMS];
-  __shared__ unsigned long long stot[kMaxBatchQueries];
+  __shared__ unsigned long long sacc[kBatchSmemSlots];
   __shared__ unsigned int s_bad;
   const BatchDesc& D = *p.desc;
   const int tid = threadIdx.x;
   const int nq = D.n_queries, nseg = D.n_seg;
-  for (int i = tid; i < nq; i += blockDim.x) {
-    sq[i] = D.q[i];
-    stot[i] = 0;
-  }
+  for (int i = tid; i < nq; i += blockDim.x) sq[i] = D.q[i];
+  for (int i = tid; i < kBatchSmemSlots; i += blockDim.x) sacc[i] = 0ull;
   for (int i = tid; i < nseg; i += blockDim.x) {
     sseg[i] = D.seg_begin[i];
     smask[i] = D.seg_mask[i];
@@ -313,17 +314,39 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
           ++bad;
           continue;
         }
-        atomicAdd(&p.out[Q.out_offset + g], static_cast<unsigned long long>(v));
-        atomicAdd(&stot[q], static_cast<unsigned long long>(v));
+        if (Q.smem_off >= 0) smem_add_u64(&sacc[Q.smem_off + g], static_cast<uint64_t>(v));
+        else atomicAdd(&p.out[Q.out_offset + g], static_cast<unsigned long long>(v));
       }
     }
   }
   const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
   if ((tid & 31) == 0 && wbad) atomicAdd(&s_bad, wbad);
   __syncthreads();
-  for (int i = tid; i < nq; i += blockDim.x)
-    if (stot[i]) atomicAdd(&p.totals[i], stot[i]);
+  for (int q = 0; q < nq; ++q) {
+    const BatchQuery& Q = sq[q];
+    if (Q.smem_off < 0) continue;
+    for (int64_t g = tid; g < Q.group_nums; g += blockDim.x) {
+      const unsigned long long v = sacc[Q.smem_off + g];
+      if (v) atomicAdd(&p.out[Q.out_offset + g], v);
+    }
+  }
   if (tid == 0 && s_bad) atomicAdd(p.range_err, static_cast<unsigned long long>(s_bad));
+}
+
+// totals[q] = sum of query q's group vector (one block per query).
+__global__ void batch_totals_kernel(const BatchParams p) {
+  __shared__ long long red[32];
+  const BatchQuery& Q = p.desc->q[blockIdx.x];
+  int64_t s = 0;
+  for (int64_t g = threadIdx.x; g < Q.group_nums; g += blockDim.x) s += static_cast<int64_t>(p.out[Q.out_offset + g]);
+  s = warp_sum_i64(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    long long v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0;
+    v = warp_sum_i64(v);
+    if (threadIdx.x == 0) p.totals[blockIdx.x] = static_cast<unsigned long long>(v);
+  }
 }
 
 static unsigned grid_n(const olap_ctx* ctx, int64_t n, int threads) {
@@ -501,6 +524,21 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
     cuts.push_back(in.row_end);
   }
   OLAP_REQUIRE(ctx, off <= out_slots, "out holds fewer slots than the queries' groups");
+  // Per-block shared accumulators for the queries with the fewest groups
+  // (they see the most same-address atomics), as long as they fit.
+  {
+    std::vector<int> byg(n_queries);
+    for (int q = 0; q < n_queries; ++q) byg[q] = q;
+    std::stable_sort(byg.begin(), byg.end(), [&](int x, int y) { return D.q[x].group_nums < D.q[y].group_nums; });
+    int64_t used = 0;
+    for (int q : byg) {
+      D.q[q].smem_off = -1;
+      if (used + D.q[q].group_nums <= olap::kBatchSmemSlots) {
+        D.q[q].smem_off = static_cast<int32_t>(used);
+        used += D.q[q].group_nums;
+      }
+    }
+  }
   // Fact-range segments: between consecutive cut points the set of queries
   // whose range covers a row is constant.
   std::sort(cuts.begin(), cuts.end());
@@ -562,6 +600,10 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
     }
     if (e == cudaSuccess && n_rows > 0) {
       olap::batch_scan_kernel<<<grid, olap::kBatchThreads, 0, st>>>(p);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+      olap::batch_totals_kernel<<<n_queries, 256, 0, st>>>(p);
       e = cudaGetLastError();
     }
     return e;

@@ -385,6 +385,34 @@ OLAP_API int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int 
                             int64_t n_rows, int agg, int64_t* out, int64_t out_slots, int64_t* totals,
                             int use_graph);
 
+/* ---- TPC-H Q5-shaped join chain (code/TPCH_Q5/Q5.cpp) ---------------------
+ * Tables by column (device pointers).  Supplier and customer keys are 1-based
+ * row numbers; l_orderkey is the order's row (the reference's
+ * l_orderkey_new); n_regionkey[n] is the region row of nation n; nation keys
+ * are < 64. */
+typedef struct olap_q5_tables {
+  const int32_t* r_regionkey;  int64_t n_region;
+  const int32_t* n_regionkey;  int64_t n_nation;
+  const int32_t* s_nationkey;  int64_t n_supp;
+  const int32_t* c_nationkey;  int64_t n_cust;
+  const int32_t* o_custkey;
+  const int32_t* o_orderdate;  int64_t n_orders;
+  const int32_t* l_orderkey;
+  const int32_t* l_suppkey;
+  const int32_t* l_price;      /* extended price in cents     */
+  const int32_t* l_discount;   /* discount in percent [0,100] */
+  int64_t n_lines;
+} olap_q5_tables;
+/* set_bitmap + DimVec_S + DimVec_o + Tri_table_join (Q5.cpp:913-978):
+ * nation_sums[n] (device, n_nation entries) = SUM l_price * (100 -
+ * l_discount) over the lines whose supplier's nation is n, lies in a region
+ * with key `region`, and equals the nation of the line's order's customer,
+ * the order dated in [date1, date2).  int64 fixed point (the reference sums
+ * price * (1 - discount) in double).  Out-of-range customer, supplier or
+ * order references are dropped and counted as range errors. */
+OLAP_API int olap_q5_chain(olap_ctx* ctx, const olap_q5_tables* t, int32_t region, int32_t date1,
+                           int32_t date2, int64_t* nation_sums);
+
 /* ---- seeded synthetic data (counter-based; identical on host and device) --
  * Value i of stream s under seed k is a pure function of (k, s, i), so any
  * slice can be generated anywhere.  _dev variants write device memory on the

@@ -66,6 +66,20 @@ class BatchQuery(C.Structure):
     ]
 
 
+class Q5Tables(C.Structure):
+    """Mirror of ``olap_q5_tables``."""
+
+    _fields_ = [
+        ("r_regionkey", C.c_void_p), ("n_region", C.c_int64),
+        ("n_regionkey", C.c_void_p), ("n_nation", C.c_int64),
+        ("s_nationkey", C.c_void_p), ("n_supp", C.c_int64),
+        ("c_nationkey", C.c_void_p), ("n_cust", C.c_int64),
+        ("o_custkey", C.c_void_p), ("o_orderdate", C.c_void_p), ("n_orders", C.c_int64),
+        ("l_orderkey", C.c_void_p), ("l_suppkey", C.c_void_p), ("l_price", C.c_void_p),
+        ("l_discount", C.c_void_p), ("n_lines", C.c_int64),
+    ]
+
+
 class StarjoinQuery(C.Structure):
     """Mirror of ``olap_starjoin_query``."""
 
@@ -139,6 +153,7 @@ def _load() -> C.CDLL:
         "olap_batch_destroy": (C.c_int, [vp]),
         "olap_batch_set_dimension": (C.c_int, [vp, C.c_int, vp, vp, i64]),
         "olap_batch_run": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, i64, C.c_int, vp, i64, vp, C.c_int]),
+        "olap_q5_chain": (C.c_int, [vp, C.POINTER(Q5Tables), i32, i32, i32, vp]),
         "olap_gen_uniform_i32_dev": (C.c_int, [vp, vp, i64, u64, u64, i32, i32]),
         "olap_gen_uniform_i32": (C.c_int, [vp, i64, u64, u64, i32, i32, C.c_int]),
         "olap_gen_zipf_i32_dev": (C.c_int, [vp, vp, i64, u64, u64, i64, f64]),

@@ -1,0 +1,186 @@
+// The TPC-H Q5-shaped join chain for sm_100a.
+//
+// Reference: code/TPCH_Q5/Q5.cpp.  set_bitmap (:913-920) marks the regions
+// equal to REGION; DimVec_S (:921-931) maps each supplier to its nation when
+// the nation lies in a marked region (else -1); DimVec_o (:932-944) maps each
+// order to its customer's nation when that nation lies in a marked region and
+// DATE1 <= o_orderdate < DATE2 (else -1); Tri_table_join (:945-978) keeps the
+// line rows whose supplier nation is not -1 and equals their order's nation,
+// and adds l_extendedprice * (1 - l_discount) to that nation's sum (double).
+// Here the sum is int64 fixed point: SUM price_cents * (100 - discount_pct),
+// exactly 100 x 100 x the decimal revenue.
+//
+// Three passes: suppliers -> int8 nation vector (small: staged in shared
+// memory by the line pass), orders -> int8 nation vector (one byte per order,
+// L2-resident for the line pass), lines -> per-nation int64 sums in shared
+// memory, flushed once per block.  Customer and supplier keys are 1-based as
+// in the reference; orders are addressed by row (l_orderkey_new).
+#include <algorithm>
+#include <cstring>
+
+#include "olap_internal.cuh"
+
+namespace olap {
+
+constexpr int kQ5MaxNations = 64;
+
+// Nations whose region passes, as a bit mask (n_regionkey[n] == region).
+__device__ __forceinline__ bool nation_ok(uint64_t mask, int32_t n) {
+  return static_cast<uint32_t>(n) < kQ5MaxNations && ((mask >> n) & 1ull);
+}
+
+// set_bitmap + nation -> region: bit n set when nation n's region has key `region`.
+__global__ void q5_nation_mask_kernel(const int32_t* __restrict__ r_regionkey, int64_t n_region,
+                                      const int32_t* __restrict__ n_regionkey, int64_t n_nation, int32_t region,
+                                      unsigned long long* __restrict__ mask) {
+  const int n = threadIdx.x;
+  const bool ok = n < n_nation && n_regionkey[n] >= 0 && n_regionkey[n] < n_region &&
+                  r_regionkey[n_regionkey[n]] == region;
+  __shared__ unsigned long long s[2];
+  const unsigned int b = __ballot_sync(0xffffffffu, ok);
+  if ((n & 31) == 0) s[n >> 5] = b;
+  __syncthreads();
+  if (n == 0) *mask = s[0] | (s[1] << 32);
+}
+
+__global__ void q5_supplier_kernel(const int32_t* __restrict__ s_nationkey, int64_t n_supp,
+                                   const unsigned long long* __restrict__ d_mask, int8_t* __restrict__ dim_s) {
+  const uint64_t nmask = *d_mask;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_supp; i += stride) {
+    const int32_t n = s_nationkey[i];
+    dim_s[i] = nation_ok(nmask, n) ? static_cast<int8_t>(n) : static_cast<int8_t>(-1);
+  }
+}
+
+__global__ void q5_orders_kernel(const int32_t* __restrict__ o_custkey, const int32_t* __restrict__ o_orderdate,
+                                 int64_t n_orders, const int32_t* __restrict__ c_nationkey, int64_t n_cust,
+                                 const unsigned long long* __restrict__ d_mask, int32_t date1, int32_t date2,
+                                 int8_t* __restrict__ dim_o, unsigned long long* range_err) {
+  const uint64_t nmask = *d_mask;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const uint64_t pol = policy_evict_first();
+  unsigned int bad = 0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_orders; i += stride) {
+    const int32_t d = ld_stream_s32(o_orderdate + i, pol);
+    const int32_t c = ld_stream_s32(o_custkey + i, pol);
+    int8_t v = -1;
+    if (d >= date1 && d < date2) {
+      if (c < 1 || c > n_cust) {
+        ++bad;
+      } else {
+        const int32_t n = __ldg(c_nationkey + (c - 1));
+        if (nation_ok(nmask, n)) v = static_cast<int8_t>(n);
+      }
+    }
+    dim_o[i] = v;
+  }
+  if (bad) atomicAdd(range_err, static_cast<unsigned long long>(bad));
+}
+
+__global__ void __launch_bounds__(512) q5_lines_kernel(const int32_t* __restrict__ l_suppkey,
+                                                       const int32_t* __restrict__ l_order,
+                                                       const int32_t* __restrict__ price,
+                                                       const int32_t* __restrict__ disc, int64_t n_lines,
+                                                       const int8_t* __restrict__ dim_s, int64_t n_supp,
+                                                       const int8_t* __restrict__ dim_o, int64_t n_orders,
+                                                       unsigned long long* __restrict__ sums,
+                                                       unsigned long long* range_err, int stage_s) {
+  extern __shared__ int8_t s_dim[];  // staged supplier nations (stage_s)
+  __shared__ unsigned long long s_sum[kQ5MaxNations];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < kQ5MaxNations; i += blockDim.x) s_sum[i] = 0;
+  if (stage_s)
+    for (int64_t i = tid; i < n_supp; i += blockDim.x) s_dim[i] = dim_s[i];
+  __syncthreads();
+  const uint64_t pol = policy_evict_first();
+  const uint64_t keep = policy_evict_last();
+  unsigned int bad = 0;
+  auto one = [&](int32_t sk, int32_t ok, int32_t p, int32_t dc) {
+    if (sk < 1 || sk > n_supp || ok < 0 || ok >= n_orders) {
+      ++bad;
+      return;
+    }
+    const int32_t ns = stage_s ? s_dim[sk - 1] : dim_s[sk - 1];
+    if (ns < 0) return;
+    const int32_t no = static_cast<int8_t>(ld_probe_s8(dim_o + ok, keep));
+    if (no != ns) return;
+    smem_add_u64(&s_sum[ns], static_cast<uint64_t>(static_cast<int64_t>(p) * (100 - dc)));
+  };
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid;
+  const bool vec = ((reinterpret_cast<uintptr_t>(l_suppkey) | reinterpret_cast<uintptr_t>(l_order) |
+                     reinterpret_cast<uintptr_t>(price) | reinterpret_cast<uintptr_t>(disc)) & 15) == 0;
+  const int64_t n4 = vec ? n_lines >> 2 : 0;
+  for (int64_t i = t0; i < n4; i += stride) {
+    const int4 a = ld_stream_v4(l_suppkey + 4 * i, pol), b = ld_stream_v4(l_order + 4 * i, pol);
+    const int4 c = ld_stream_v4(price + 4 * i, pol), d = ld_stream_v4(disc + 4 * i, pol);
+    one(a.x, b.x, c.x, d.x);
+    one(a.y, b.y, c.y, d.y);
+    one(a.z, b.z, c.z, d.z);
+    one(a.w, b.w, c.w, d.w);
+  }
+  for (int64_t r = 4 * n4 + t0; r < n_lines; r += stride) one(l_suppkey[r], l_order[r], price[r], disc[r]);
+  const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
+  if ((tid & 31) == 0 && wbad) atomicAdd(range_err, static_cast<unsigned long long>(wbad));
+  __syncthreads();
+  for (int i = tid; i < kQ5MaxNations; i += blockDim.x)
+    if (s_sum[i]) atomicAdd(&sums[i], s_sum[i]);
+}
+
+static unsigned grid_q5(const olap_ctx* ctx, int64_t n, int threads) {
+  int64_t g = (n + threads - 1) / threads;
+  const int64_t cap = static_cast<int64_t>(ctx->sm_count) * (2048 / threads);
+  if (g > cap) g = cap;
+  return static_cast<unsigned>(g < 1 ? 1 : g);
+}
+
+}  // namespace olap
+
+extern "C" {
+
+int olap_q5_chain(olap_ctx* ctx, const olap_q5_tables* t, int32_t region, int32_t date1, int32_t date2,
+                  int64_t* nation_sums) {
+  if (!ctx || !t) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_REQUIRE(ctx, nation_sums, "null output");
+  OLAP_REQUIRE(ctx, t->n_region >= 1 && t->n_nation >= 1 && t->n_nation <= olap::kQ5MaxNations,
+               "1..64 nations");
+  OLAP_REQUIRE(ctx, t->n_supp >= 0 && t->n_cust >= 0 && t->n_orders >= 0 && t->n_lines >= 0, "bad sizes");
+  OLAP_REQUIRE(ctx, t->r_regionkey && t->n_regionkey, "null region or nation table");
+  olap::Arena ar(ctx);
+  int8_t* dim_s = ar.take<int8_t>(static_cast<size_t>(t->n_supp > 0 ? t->n_supp : 1));
+  int8_t* dim_o = ar.take<int8_t>(static_cast<size_t>(t->n_orders > 0 ? t->n_orders : 1));
+  unsigned long long* nmask = ar.take<unsigned long long>(1);
+  if (!dim_s || !dim_o || !nmask)
+    return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for Q5 vectors");
+  olap::q5_nation_mask_kernel<<<1, 64, 0, ctx->stream>>>(t->r_regionkey, t->n_region, t->n_regionkey, t->n_nation,
+                                                        region, nmask);
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(nation_sums, 0, sizeof(int64_t) * t->n_nation, ctx->stream));
+  if (t->n_supp)
+    olap::q5_supplier_kernel<<<olap::grid_q5(ctx, t->n_supp, 256), 256, 0, ctx->stream>>>(t->s_nationkey, t->n_supp,
+                                                                                         nmask, dim_s);
+  if (t->n_orders)
+    olap::q5_orders_kernel<<<olap::grid_q5(ctx, t->n_orders, 256), 256, 0, ctx->stream>>>(
+        t->o_custkey, t->o_orderdate, t->n_orders, t->c_nationkey, t->n_cust, nmask, date1, date2, dim_o,
+        &ctx->counters->range_errors);
+  if (t->n_lines) {
+    const bool stage = t->n_supp <= 160 * 1024;
+    const size_t smem = stage ? static_cast<size_t>((t->n_supp + 15) & ~int64_t(15)) : 0;
+    if (smem > 48 * 1024)
+      OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::q5_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(smem)));
+    int bps = 1;
+    OLAP_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, olap::q5_lines_kernel, 512, smem));
+    int64_t grid = static_cast<int64_t>(ctx->sm_count) * (bps < 1 ? 1 : bps);
+    grid = std::min<int64_t>(grid, (t->n_lines / 4 + 511) / 512 + 1);
+    olap::q5_lines_kernel<<<static_cast<unsigned>(grid), 512, smem, ctx->stream>>>(
+        t->l_suppkey, t->l_orderkey, t->l_price, t->l_discount, t->n_lines, dim_s, t->n_supp, dim_o, t->n_orders,
+        reinterpret_cast<unsigned long long*>(nation_sums), &ctx->counters->range_errors, stage ? 1 : 0);
+  }
+  OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  return OLAP_OK;
+}
+
+}  // extern "C"

@@ -65,6 +65,9 @@ def _load_oracle() -> C.CDLL:
     lib.oracle_join_cwm_sv.restype = _i64
     lib.oracle_starjoin_cwm_sv.argtypes = [_vp, _vp, _vp, _i64, _vp]
     lib.oracle_starjoin_cwm_sv.restype = _i64
+    lib.oracle_q5.argtypes = [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64,
+                              _i32, _i32, _i32, _vp]
+    lib.oracle_q5.restype = _i64
     return lib
 
 
@@ -315,3 +318,16 @@ def ref_module(name: str) -> C.CDLL:
         lib.ref_starjoin_rowwise.argtypes = [C.c_int] + [_vp] * 8
         lib.ref_starjoin_cwm_sv.argtypes = [C.c_int] + [_vp] * 9
     return lib
+
+
+def q5(tables: dict, region: int, date1: int, date2: int):
+    """(nation_sums, range_errors) of the Q5 chain; tables: name -> numpy array."""
+    t = {k: _c32(v) for k, v in tables.items()}
+    sums = np.zeros(len(t["n_regionkey"]), np.int64)
+    errs = oracle_lib().oracle_q5(_p(t["r_regionkey"]), len(t["r_regionkey"]), _p(t["n_regionkey"]),
+                                  len(t["n_regionkey"]), _p(t["s_nationkey"]), len(t["s_nationkey"]),
+                                  _p(t["c_nationkey"]), len(t["c_nationkey"]), _p(t["o_custkey"]),
+                                  _p(t["o_orderdate"]), len(t["o_custkey"]), _p(t["l_orderkey"]), _p(t["l_suppkey"]),
+                                  _p(t["l_price"]), _p(t["l_discount"]), len(t["l_orderkey"]), int(region),
+                                  int(date1), int(date2), _p(sums))
+    return sums, errs

@@ -392,3 +392,47 @@ int64_t oracle_starjoin_cwm_sv(const int8_t* const* dimvec, const int64_t* len, 
   }
   return c;
 }
+
+/* TPC-H Q5 chain (TPCH_Q5/Q5.cpp:913-978) in int64 fixed point:
+ * nation_sums[n] = SUM price * (100 - discount) over lines whose supplier
+ * nation (s_nationkey[suppkey-1]) is in a region with key `region` and equals
+ * the nation of the order's customer (c_nationkey[custkey-1]), the order dated
+ * in [date1, date2).  Invalid references are counted and skipped. */
+int64_t oracle_q5(const int32_t* r_regionkey, int64_t n_region, const int32_t* n_regionkey, int64_t n_nation,
+                  const int32_t* s_nationkey, int64_t n_supp, const int32_t* c_nationkey, int64_t n_cust,
+                  const int32_t* o_custkey, const int32_t* o_orderdate, int64_t n_orders, const int32_t* l_orderkey,
+                  const int32_t* l_suppkey, const int32_t* l_price, const int32_t* l_discount, int64_t n_lines,
+                  int32_t region, int32_t date1, int32_t date2, int64_t* nation_sums) {
+  int64_t errs = 0;
+  unsigned char ok_nation[64] = {0};
+  for (int64_t n = 0; n < n_nation && n < 64; n++) {
+    const int32_t r = n_regionkey[n];
+    ok_nation[n] = r >= 0 && r < n_region && r_regionkey[r] == region;
+  }
+  int8_t* ds = (int8_t*)malloc((size_t)(n_supp > 0 ? n_supp : 1));
+  int8_t* dor = (int8_t*)malloc((size_t)(n_orders > 0 ? n_orders : 1));
+  for (int64_t i = 0; i < n_supp; i++) {
+    const int32_t n = s_nationkey[i];
+    ds[i] = (n >= 0 && n < 64 && ok_nation[n]) ? (int8_t)n : -1;
+  }
+  for (int64_t i = 0; i < n_orders; i++) {
+    dor[i] = -1;
+    if (o_orderdate[i] >= date1 && o_orderdate[i] < date2) {
+      const int32_t c = o_custkey[i];
+      if (c < 1 || c > n_cust) { errs++; continue; }
+      const int32_t n = c_nationkey[c - 1];
+      if (n >= 0 && n < 64 && ok_nation[n]) dor[i] = (int8_t)n;
+    }
+  }
+  for (int64_t n = 0; n < n_nation; n++) nation_sums[n] = 0;
+  for (int64_t i = 0; i < n_lines; i++) {
+    const int32_t sk = l_suppkey[i], ok = l_orderkey[i];
+    if (sk < 1 || sk > n_supp || ok < 0 || ok >= n_orders) { errs++; continue; }
+    const int ns = ds[sk - 1];
+    if (ns < 0 || dor[ok] != ns) continue;
+    nation_sums[ns] += (int64_t)l_price[i] * (100 - l_discount[i]);
+  }
+  free(ds);
+  free(dor);
+  return errs;
+}

@@ -53,8 +53,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tune", type=str, default="", help="knob=value,... (olap_ctx_set_tuning)")
-    ap.add_argument("--suite", default="starjoin", choices=["starjoin", "batched"],
-                    help="starjoin: the headline line; batched: 64-query batches vs one launch per query")
+    ap.add_argument("--suite", default="starjoin", choices=["starjoin", "batched", "serving"],
+                    help="starjoin: the headline line; batched: 64-query batches vs one launch per query; "
+                         "serving: Poisson arrivals of the 70/30 star-join/Q5 mix, batched vs plain")
+    ap.add_argument("--rates", type=float, nargs="+", default=[50, 200, 500, 1000, 2000])
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--queries", type=int, default=64)
     return ap.parse_args()
 
@@ -246,6 +249,80 @@ def run_batched(a) -> None:
     ctx.close()
 
 
+def run_serving(a) -> None:
+    """Serving configuration: Poisson arrivals at each rate of --rates, 70%
+    star-joins of the batched configuration over the 600M-row table and 30%
+    Q5 chains over SF~10-sized tables, served with continuous batching and
+    with one launch per query; latency from arrival to the result on the
+    host."""
+    import numpy as np
+    import torch
+    from memory_database_b200 import batch, olapcore, q5 as Q5, serving as S, workloads
+    torch.cuda.set_device(0)
+    ctx = olapcore.Context(0)
+    groups = (25, 25, 40, 7)
+    s = workloads.make_star_schema(ctx, a.rows, DIM_SIZES, (1, 1, 1, 1), (1, 1, 1, 1), seed=42)
+    dims = batch.make_dim_tables(ctx, DIM_SIZES, groups, seed=7)
+    q5d = Q5.make_q5_data(ctx)
+    ctx.synchronize()
+    rng = np.random.default_rng(77)
+    star = batch.random_queries(rng, 2000, a.rows, groups)
+    q5q = Q5.random_q5_queries(rng, 500)
+    batched, plain = S.gpu_servers(dims, s.fk, s.m1, s.m2, q5d)
+    warm = S.poisson_requests(rng, 1000.0, 64, star, q5q)
+    batched.serve(S.reset(warm))
+    plain.serve(S.reset(warm))
+    # device time of one Q5 chain and of a 64-query Q5 batch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    qb = torch.empty((64, 25), dtype=torch.int64, device="cuda")
+    qo = torch.empty(25, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    e0.record()
+    for q in q5q[:64]:
+        Q5.q5(ctx, q5d, *q, out=qo)
+    e1.record()
+    torch.cuda.synchronize()
+    q5_plain_ms = e0.elapsed_time(e1) / 64
+    Q5.q5_batch(ctx, q5d, q5q[:64], out=qb)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(5):
+        Q5.q5_batch(ctx, q5d, q5q[:64], out=qb)
+    e1.record()
+    torch.cuda.synchronize()
+    q5_batch_ms = e0.elapsed_time(e1) / 5
+    per_rate = []
+    for rate in a.rates:
+        n = max(50, int(rate * a.serve_seconds))
+        reqs = S.poisson_requests(np.random.default_rng(int(rate)), rate, n, star, q5q)
+        with ClockSampler(0) as clk:
+            rb = batched.serve(S.reset(reqs))
+            nb = batched.batches
+            rp = plain.serve(S.reset(reqs))
+        sb, sp = S.summarize(rb, nb), S.summarize(rp)
+        per_rate.append({"offered_qps": rate, "requests": n,
+                         "batched": {"qps": sb.qps, "p50_ms": sb.p50_ms, "p99_ms": sb.p99_ms,
+                                     "mean_batch": sb.mean_batch, "by_kind": sb.by_kind},
+                         "plain": {"qps": sp.qps, "p50_ms": sp.p50_ms, "p99_ms": sp.p99_ms, "by_kind": sp.by_kind},
+                         "clocks": clk.summary()})
+        batched.batches = 0
+    top = per_rate[-1]
+    line = {"metric": "serving queries/sec with p50/p99 latency", "value": top["batched"]["qps"],
+            "unit": "queries/s", "n_gpus": 1, "higher_is_better": True,
+            "p50_ms": top["batched"]["p50_ms"], "p99_ms": top["batched"]["p99_ms"],
+            "plain_qps": top["plain"]["qps"], "plain_p50_ms": top["plain"]["p50_ms"],
+            "plain_p99_ms": top["plain"]["p99_ms"], "per_rate": per_rate,
+            "q5_chain_ms": q5_plain_ms, "q5_batch64_ms": q5_batch_ms,
+            "graph_captures": batched.engine.graph_captures(),
+            "config": {"workload": f"Poisson arrivals at {a.rates} queries/s, {a.serve_seconds:g} s each: 70% "
+                                   f"star-joins (batched configuration, {a.rows:,}-row table), 30% Q5 chains "
+                                   "(5/25/100,000/1,500,000/15,000,000/60,000,000 rows, one-year date filter); "
+                                   "continuous batching (<=64 per launch, 2 in flight per lane) vs one launch "
+                                   "per query; latency = arrival to result on the host"},
+            "data": "synthetic (seeded counter-based generator, generated in HBM)"}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     a = parse()
     if a.impl == "reference":
@@ -253,6 +330,9 @@ def main() -> None:
         return
     if a.suite == "batched":
         run_batched(a)
+        return
+    if a.suite == "serving":
+        run_serving(a)
         return
     import torch
     import torch.distributed as dist

@@ -364,7 +364,7 @@ typedef struct olap_batch_query {
   int64_t group_nums;              /* groups of this query                     */
 } olap_batch_query;
 
-/* A batch engine for up to max_queries (<= 256) queries per launch; holds the
+/* A batch engine for up to max_queries (<= 64) queries per launch; holds the
  * packed attribute records of the dimensions and two staging slots (so one
  * batch can be prepared while the previous one runs). */
 OLAP_API int olap_batch_create(olap_ctx* ctx, int max_queries, olap_batch** out);
@@ -378,12 +378,15 @@ OLAP_API int olap_batch_set_dimension(olap_batch* b, int table, const int32_t* f
  * the sum of the earlier queries' group_nums; totals[q] its total.  Per query
  * the result equals olap_starjoin_groupsum over the dimension vectors of
  * olap_build_dimvec.  use_graph: record the launch as a CUDA graph and replay
- * it while the parameters stay the same.  Asynchronous on the context
- * stream. */
+ * it while the tables, fact columns and aggregate stay the same (queries,
+ * their count and the output buffers may change between replays).
+ * Asynchronous on the context stream. */
 OLAP_API int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries,
                             const int32_t* const* fk, const int32_t* m1, const int32_t* m2,
                             int64_t n_rows, int agg, int64_t* out, int64_t out_slots, int64_t* totals,
                             int use_graph);
+/* Number of graphs recorded by olap_batch_run so far. */
+OLAP_API int olap_batch_graph_captures(olap_batch* b, int64_t* captures);
 
 /* ---- TPC-H Q5-shaped join chain (code/TPCH_Q5/Q5.cpp) ---------------------
  * Tables by column (device pointers).  Supplier and customer keys are 1-based
@@ -412,6 +415,20 @@ typedef struct olap_q5_tables {
  * order references are dropped and counted as range errors. */
 OLAP_API int olap_q5_chain(olap_ctx* ctx, const olap_q5_tables* t, int32_t region, int32_t date1,
                            int32_t date2, int64_t* nation_sums);
+
+/* Up to OLAP_Q5_MAX_BATCH Q5 queries, each with its own region and date
+ * range, in one pass over orders and one over lineitem (no counterpart in the
+ * reference, which runs one query per process).  nation_sums is device
+ * memory of n_queries x n_nation int64: row q equals, bit for bit, what
+ * olap_q5_chain gives for query q alone.  Each out-of-range reference is
+ * counted once per call (a customer reference only when the order's date
+ * lies in some query's range). */
+#define OLAP_Q5_MAX_BATCH 64
+typedef struct olap_q5_query {
+  int32_t region, date1, date2;
+} olap_q5_query;
+OLAP_API int olap_q5_batch(olap_ctx* ctx, const olap_q5_tables* t, const olap_q5_query* queries, int n_queries,
+                           int64_t* nation_sums);
 
 /* ---- seeded synthetic data (counter-based; identical on host and device) --
  * Value i of stream s under seed k is a pure function of (k, s, i), so any

@@ -80,6 +80,15 @@ class Q5Tables(C.Structure):
     ]
 
 
+class Q5Query(C.Structure):
+    """Mirror of ``olap_q5_query``."""
+
+    _fields_ = [("region", C.c_int32), ("date1", C.c_int32), ("date2", C.c_int32)]
+
+
+Q5_MAX_BATCH = 64
+
+
 class StarjoinQuery(C.Structure):
     """Mirror of ``olap_starjoin_query``."""
 
@@ -153,7 +162,9 @@ def _load() -> C.CDLL:
         "olap_batch_destroy": (C.c_int, [vp]),
         "olap_batch_set_dimension": (C.c_int, [vp, C.c_int, vp, vp, i64]),
         "olap_batch_run": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, i64, C.c_int, vp, i64, vp, C.c_int]),
+        "olap_batch_graph_captures": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "olap_q5_chain": (C.c_int, [vp, C.POINTER(Q5Tables), i32, i32, i32, vp]),
+        "olap_q5_batch": (C.c_int, [vp, C.POINTER(Q5Tables), C.POINTER(Q5Query), C.c_int, vp]),
         "olap_gen_uniform_i32_dev": (C.c_int, [vp, vp, i64, u64, u64, i32, i32]),
         "olap_gen_uniform_i32": (C.c_int, [vp, i64, u64, u64, i32, i32, C.c_int]),
         "olap_gen_zipf_i32_dev": (C.c_int, [vp, vp, i64, u64, u64, i64, f64]),

@@ -4,7 +4,7 @@ Dimension tables carry attributes (an int32 filter attribute and an int32
 group attribute per row).  A query filters each table it uses with a range
 [lo, hi) on the filter attribute, groups by the group attributes of 1-3
 tables and scans a contiguous fact range.  ``BatchEngine.run`` executes up to
-256 such queries in one persistent launch (optionally replayed as a CUDA
+64 such queries in one persistent launch (optionally replayed as a CUDA
 graph); ``run_plain`` executes one query the plain way — build its int8
 dimension vectors with ``olap_build_dimvec``, then one
 ``olap_starjoin_groupsum`` launch — and gives bit-identical results.
@@ -124,6 +124,11 @@ class BatchEngine:
             self.close()
         except Exception:
             pass
+
+    def graph_captures(self) -> int:
+        n = C.c_int64()
+        check(lib.olap_batch_graph_captures(self._h, C.byref(n)), self.ctx.handle)
+        return n.value
 
     def run(self, queries: list[Query], fk, m1, m2, agg: int = AGG_M1_PLUS_M2, use_graph: bool = True,
             out=None, totals=None):

@@ -83,6 +83,9 @@ struct BatchDesc {
   int64_t seg_begin[kMaxSegments];             // sorted; segment s = [seg_begin[s], seg_begin[s+1])
   unsigned long long seg_mask[kMaxSegments];   // queries whose fact range covers segment s
   unsigned long long uses_mask[OLAP_MAX_DIMS]; // queries using table t
+  unsigned long long* out;                     // concatenated group vectors
+  unsigned long long* totals;                  // [n_queries]
+  int64_t out_total;                           // slots of out in use
   int32_t n_queries;
   int32_t n_seg;
 };
@@ -105,8 +108,6 @@ struct BatchParams {
   int32_t tables_used;                // union of the queries' `uses`
   int32_t probe_order;                // 4 x 2-bit table ids, smallest table first
   int32_t agg;                        // OLAP_AGG_* of every query (one aggregate)
-  unsigned long long* out;            // concatenated group vectors
-  unsigned long long* totals;         // [n_queries]
   unsigned long long* range_err;
 };
 
@@ -179,6 +180,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
   __shared__ unsigned long long sacc[kBatchSmemSlots];
   __shared__ unsigned int s_bad;
   const BatchDesc& D = *p.desc;
+  unsigned long long* const out = D.out;
   const int tid = threadIdx.x;
   const int nq = D.n_queries, nseg = D.n_seg;
   for (int i = tid; i < nq; i += blockDim.x) sq[i] = D.q[i];
@@ -315,7 +317,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
           continue;
         }
         if (Q.smem_off >= 0) smem_add_u64(&sacc[Q.smem_off + g], static_cast<uint64_t>(v));
-        else atomicAdd(&p.out[Q.out_offset + g], static_cast<unsigned long long>(v));
+        else atomicAdd(&out[Q.out_offset + g], static_cast<unsigned long long>(v));
       }
     }
   }
@@ -327,25 +329,38 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
     if (Q.smem_off < 0) continue;
     for (int64_t g = tid; g < Q.group_nums; g += blockDim.x) {
       const unsigned long long v = sacc[Q.smem_off + g];
-      if (v) atomicAdd(&p.out[Q.out_offset + g], v);
+      if (v) atomicAdd(&out[Q.out_offset + g], v);
     }
   }
   if (tid == 0 && s_bad) atomicAdd(p.range_err, static_cast<unsigned long long>(s_bad));
 }
 
 // totals[q] = sum of query q's group vector (one block per query).
+// Zero the batch's outputs (their location and size come with the descriptor,
+// so a recorded graph serves any output buffer and query count).
+__global__ void batch_zero_kernel(const BatchParams p) {
+  const BatchDesc& D = *p.desc;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (int64_t i = t0; i < D.out_total; i += stride) D.out[i] = 0ull;
+  for (int64_t i = t0; i < D.n_queries; i += stride) D.totals[i] = 0ull;
+}
+
+// Launched with max_queries blocks; blocks past the batch's count return.
 __global__ void batch_totals_kernel(const BatchParams p) {
   __shared__ long long red[32];
-  const BatchQuery& Q = p.desc->q[blockIdx.x];
+  const BatchDesc& D = *p.desc;
+  if (static_cast<int>(blockIdx.x) >= D.n_queries) return;
+  const BatchQuery& Q = D.q[blockIdx.x];
   int64_t s = 0;
-  for (int64_t g = threadIdx.x; g < Q.group_nums; g += blockDim.x) s += static_cast<int64_t>(p.out[Q.out_offset + g]);
+  for (int64_t g = threadIdx.x; g < Q.group_nums; g += blockDim.x) s += static_cast<int64_t>(D.out[Q.out_offset + g]);
   s = warp_sum_i64(s);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
   __syncthreads();
   if (threadIdx.x < 32) {
     long long v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0;
     v = warp_sum_i64(v);
-    if (threadIdx.x == 0) p.totals[blockIdx.x] = static_cast<unsigned long long>(v);
+    if (threadIdx.x == 0) D.totals[blockIdx.x] = static_cast<unsigned long long>(v);
   }
 }
 
@@ -371,10 +386,9 @@ struct olap_batch {
   cudaGraph_t graph[2] = {};
   cudaGraphExec_t exec[2] = {};
   olap::BatchParams params[2];
-  int64_t out_slots[2] = {0, 0};
-  int32_t nq_rec[2] = {0, 0};
   bool have_params[2] = {false, false};
   int64_t runs = 0;
+  int64_t captures = 0;                 // graphs recorded so far
   int2* attrs[OLAP_MAX_DIMS] = {};
   olap::DimRecord* rec[OLAP_MAX_DIMS] = {};
   int64_t attr_len[OLAP_MAX_DIMS] = {};
@@ -470,6 +484,13 @@ int olap_batch_set_dimension(olap_batch* b, int table, const int32_t* filter_att
   return OLAP_OK;
 }
 
+int olap_batch_graph_captures(olap_batch* b, int64_t* captures) {
+  if (!b || !captures) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(b->ctx->mu);
+  *captures = b->captures;
+  return OLAP_OK;
+}
+
 int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries, const int32_t* const* fk,
                    const int32_t* m1, const int32_t* m2, int64_t n_rows, int agg, int64_t* out,
                    int64_t out_slots, int64_t* totals, int use_graph) {
@@ -559,6 +580,9 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
   }
   D.n_queries = n_queries;
   D.n_seg = nseg;
+  D.out = reinterpret_cast<unsigned long long*>(out);
+  D.totals = reinterpret_cast<unsigned long long*>(totals);
+  D.out_total = off;
   olap::BatchParams p;
   std::memset(&p, 0, sizeof(p));
   int order[OLAP_MAX_DIMS] = {0, 1, 2, 3};
@@ -576,8 +600,6 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
   p.desc = b->d_desc[slot];
   p.tables_used = tables;
   p.agg = agg;
-  p.out = reinterpret_cast<unsigned long long*>(out);
-  p.totals = reinterpret_cast<unsigned long long*>(totals);
   p.range_err = &ctx->counters->range_errors;
   const bool need_m1 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M1 || agg == OLAP_AGG_M1_TIMES_M2;
   const bool need_m2 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M2 || agg == OLAP_AGG_M1_TIMES_M2;
@@ -591,8 +613,10 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
   auto enqueue = [&](cudaStream_t st) -> cudaError_t {
     cudaError_t e = cudaMemcpyAsync(b->d_desc[slot], b->h_desc[slot], sizeof(olap::BatchDesc),
                                     cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(out, 0, sizeof(int64_t) * off, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(totals, 0, sizeof(int64_t) * n_queries, st);
+    if (e == cudaSuccess) {
+      olap::batch_zero_kernel<<<static_cast<unsigned>(ctx->sm_count) * 2, 512, 0, st>>>(p);
+      e = cudaGetLastError();
+    }
     for (int t = 0; t < OLAP_MAX_DIMS && e == cudaSuccess; ++t) {
       if (!((tables >> t) & 1)) continue;
       olap::batch_records_kernel<<<olap::grid_n(ctx, b->attr_len[t], 256), 256, 0, st>>>(p, t);
@@ -603,7 +627,7 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
-      olap::batch_totals_kernel<<<n_queries, 256, 0, st>>>(p);
+      olap::batch_totals_kernel<<<b->max_queries, 256, 0, st>>>(p);
       e = cudaGetLastError();
     }
     return e;
@@ -611,11 +635,11 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
   if (!use_graph) {
     OLAP_CUDA_TRY(ctx, enqueue(ctx->stream));
   } else {
-    // Graph of this slot: re-captured when the launch shape changes, replayed
-    // otherwise (its copy node reads the slot's pinned staging).
-    const bool same = b->have_params[slot] && b->exec[slot] &&
-                      std::memcmp(&b->params[slot], &p, sizeof(p)) == 0 && b->out_slots[slot] == off &&
-                      b->nq_rec[slot] == n_queries;
+    // Graph of this slot: re-captured when the launch parameters (tables,
+    // fact columns, aggregate) change, replayed otherwise.  Queries, output
+    // buffers and their sizes travel in the descriptor its copy node reads
+    // from the slot's pinned staging.
+    const bool same = b->have_params[slot] && b->exec[slot] && std::memcmp(&b->params[slot], &p, sizeof(p)) == 0;
     if (!same) {
       if (b->exec[slot]) cudaGraphExecDestroy(b->exec[slot]);
       if (b->graph[slot]) cudaGraphDestroy(b->graph[slot]);
@@ -634,9 +658,8 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
       cudaStreamDestroy(cs);
       if (e != cudaSuccess) return olap::check_cuda(ctx, e, "batch graph capture");
       b->params[slot] = p;
-      b->out_slots[slot] = off;
-      b->nq_rec[slot] = n_queries;
       b->have_params[slot] = true;
+      ++b->captures;
     }
     OLAP_CUDA_TRY(ctx, cudaGraphLaunch(b->exec[slot], ctx->stream));
   }

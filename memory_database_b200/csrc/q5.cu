@@ -128,6 +128,162 @@ __global__ void __launch_bounds__(512) q5_lines_kernel(const int32_t* __restrict
     if (s_sum[i]) atomicAdd(&sums[i], s_sum[i]);
 }
 
+// ---- batched: one pass over orders and lineitem for up to 64 queries ------
+//
+// A line counts for query q exactly when its supplier's nation equals its
+// order's customer nation n, n's region has key region_q, and the order date
+// lies in [date1_q, date2_q).  So the batch keeps, per nation, the mask of
+// queries whose region holds it (nat_q) and, per date of the queries' span,
+// the mask of queries whose range holds it (date_q).  The supplier vector
+// keeps nations some query wants, the order vector keeps the customer nation
+// of orders some query wants (nat_q & date_q != 0), and a line whose two
+// nations agree adds its value to sums[q][n] for every q in nat_q[n] &
+// date_q[date].  Each query's result is the single-query chain's bit for bit.
+
+constexpr int kQ5DateTable = 8192;  // dates per mask table (64 KB)
+
+struct Q5BatchDesc {
+  int32_t region[kQ5MaxNations], d1[kQ5MaxNations], d2[kQ5MaxNations];
+  int32_t n_q;
+  int32_t dlo, span;  // date table covers [dlo, dlo + span); span 0: no table
+};
+
+__device__ __forceinline__ uint64_t q5_date_mask(const Q5BatchDesc& D, const unsigned long long* tab, int32_t d) {
+  if (D.span > 0) {
+    const uint32_t k = static_cast<uint32_t>(d - D.dlo);
+    return k < static_cast<uint32_t>(D.span) ? tab[k] : 0ull;
+  }
+  uint64_t m = 0;
+  for (int q = 0; q < D.n_q; ++q) m |= static_cast<uint64_t>(d >= D.d1[q] && d < D.d2[q]) << q;
+  return m;
+}
+
+// nat_q[n] for every nation and the date table, in global scratch.
+__global__ void q5b_prep_kernel(const int32_t* __restrict__ r_regionkey, int64_t n_region,
+                                const int32_t* __restrict__ n_regionkey, int64_t n_nation, Q5BatchDesc D,
+                                unsigned long long* __restrict__ nat_q, unsigned long long* __restrict__ date_q) {
+  const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (tid < kQ5MaxNations) {
+    uint64_t m = 0;
+    const int n = static_cast<int>(tid);
+    if (n < n_nation && n_regionkey[n] >= 0 && n_regionkey[n] < n_region) {
+      const int32_t key = r_regionkey[n_regionkey[n]];
+      for (int q = 0; q < D.n_q; ++q) m |= static_cast<uint64_t>(key == D.region[q]) << q;
+    }
+    nat_q[n] = m;
+  }
+  for (int64_t k = tid; k < D.span; k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t d = D.dlo + static_cast<int32_t>(k);
+    uint64_t m = 0;
+    for (int q = 0; q < D.n_q; ++q) m |= static_cast<uint64_t>(d >= D.d1[q] && d < D.d2[q]) << q;
+    date_q[k] = m;
+  }
+}
+
+__global__ void q5b_supplier_kernel(const int32_t* __restrict__ s_nationkey, int64_t n_supp,
+                                    const unsigned long long* __restrict__ nat_q, int8_t* __restrict__ dim_s) {
+  __shared__ unsigned long long s_nat[kQ5MaxNations];
+  if (threadIdx.x < kQ5MaxNations) s_nat[threadIdx.x] = nat_q[threadIdx.x];
+  __syncthreads();
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_supp; i += stride) {
+    const int32_t n = s_nationkey[i];
+    const bool ok = static_cast<uint32_t>(n) < kQ5MaxNations && s_nat[n] != 0;
+    dim_s[i] = ok ? static_cast<int8_t>(n) : static_cast<int8_t>(-1);
+  }
+}
+
+__global__ void q5b_orders_kernel(const int32_t* __restrict__ o_custkey, const int32_t* __restrict__ o_orderdate,
+                                  int64_t n_orders, const int32_t* __restrict__ c_nationkey, int64_t n_cust,
+                                  const unsigned long long* __restrict__ nat_q,
+                                  const unsigned long long* __restrict__ date_q, Q5BatchDesc D,
+                                  int8_t* __restrict__ dim_o, unsigned long long* range_err) {
+  extern __shared__ unsigned long long s_date[];
+  __shared__ unsigned long long s_nat[kQ5MaxNations];
+  if (threadIdx.x < kQ5MaxNations) s_nat[threadIdx.x] = nat_q[threadIdx.x];
+  for (int k = threadIdx.x; k < D.span; k += blockDim.x) s_date[k] = date_q[k];
+  __syncthreads();
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const uint64_t pol = policy_evict_first();
+  unsigned int bad = 0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_orders; i += stride) {
+    const int32_t d = ld_stream_s32(o_orderdate + i, pol);
+    const int32_t c = ld_stream_s32(o_custkey + i, pol);
+    int8_t v = -1;
+    const uint64_t dm = q5_date_mask(D, s_date, d);
+    if (dm) {
+      if (c < 1 || c > n_cust) {
+        ++bad;
+      } else {
+        const int32_t n = __ldg(c_nationkey + (c - 1));
+        if (static_cast<uint32_t>(n) < kQ5MaxNations && (s_nat[n] & dm)) v = static_cast<int8_t>(n);
+      }
+    }
+    dim_o[i] = v;
+  }
+  if (bad) atomicAdd(range_err, static_cast<unsigned long long>(bad));
+}
+
+// Shared memory: [date table: span x 8][sums: n_q x n_nation x 8][supplier nations].
+__global__ void __launch_bounds__(1024, 1) q5b_lines_kernel(
+    const int32_t* __restrict__ l_suppkey, const int32_t* __restrict__ l_order, const int32_t* __restrict__ price,
+    const int32_t* __restrict__ disc, int64_t n_lines, const int8_t* __restrict__ dim_s, int64_t n_supp,
+    const int8_t* __restrict__ dim_o, const int32_t* __restrict__ o_orderdate, int64_t n_orders,
+    const unsigned long long* __restrict__ nat_q, const unsigned long long* __restrict__ date_q, Q5BatchDesc D,
+    int n_nation, unsigned long long* __restrict__ sums, unsigned long long* range_err, int stage_s) {
+  extern __shared__ __align__(16) unsigned char q5b_smem[];
+  unsigned long long* s_date = reinterpret_cast<unsigned long long*>(q5b_smem);
+  unsigned long long* s_sum = s_date + D.span;
+  int8_t* s_dim = reinterpret_cast<int8_t*>(s_sum + D.n_q * n_nation);
+  __shared__ unsigned long long s_nat[kQ5MaxNations];
+  const int tid = threadIdx.x;
+  if (tid < kQ5MaxNations) s_nat[tid] = nat_q[tid];
+  for (int k = tid; k < D.span; k += blockDim.x) s_date[k] = date_q[k];
+  for (int k = tid; k < D.n_q * n_nation; k += blockDim.x) s_sum[k] = 0;
+  if (stage_s)
+    for (int64_t i = tid; i < n_supp; i += blockDim.x) s_dim[i] = dim_s[i];
+  __syncthreads();
+  const uint64_t pol = policy_evict_first();
+  const uint64_t keep = policy_evict_last();
+  unsigned int bad = 0;
+  auto one = [&](int32_t sk, int32_t ok, int32_t p, int32_t dc) {
+    if (sk < 1 || sk > n_supp || ok < 0 || ok >= n_orders) {
+      ++bad;
+      return;
+    }
+    const int32_t ns = stage_s ? s_dim[sk - 1] : dim_s[sk - 1];
+    if (ns < 0) return;
+    const int32_t no = static_cast<int8_t>(ld_probe_s8(dim_o + ok, keep));
+    if (no != ns) return;
+    uint64_t m = s_nat[ns] & q5_date_mask(D, s_date, __ldg(o_orderdate + ok));
+    const uint64_t v = static_cast<uint64_t>(static_cast<int64_t>(p) * (100 - dc));
+    while (m) {
+      const int q = __ffsll(static_cast<long long>(m)) - 1;
+      m &= m - 1;
+      smem_add_u64(&s_sum[q * n_nation + ns], v);
+    }
+  };
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid;
+  const bool vec = ((reinterpret_cast<uintptr_t>(l_suppkey) | reinterpret_cast<uintptr_t>(l_order) |
+                     reinterpret_cast<uintptr_t>(price) | reinterpret_cast<uintptr_t>(disc)) & 15) == 0;
+  const int64_t n4 = vec ? n_lines >> 2 : 0;
+  for (int64_t i = t0; i < n4; i += stride) {
+    const int4 a = ld_stream_v4(l_suppkey + 4 * i, pol), b = ld_stream_v4(l_order + 4 * i, pol);
+    const int4 c = ld_stream_v4(price + 4 * i, pol), d = ld_stream_v4(disc + 4 * i, pol);
+    one(a.x, b.x, c.x, d.x);
+    one(a.y, b.y, c.y, d.y);
+    one(a.z, b.z, c.z, d.z);
+    one(a.w, b.w, c.w, d.w);
+  }
+  for (int64_t r = 4 * n4 + t0; r < n_lines; r += stride) one(l_suppkey[r], l_order[r], price[r], disc[r]);
+  const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
+  if ((tid & 31) == 0 && wbad) atomicAdd(range_err, static_cast<unsigned long long>(wbad));
+  __syncthreads();
+  for (int k = tid; k < D.n_q * n_nation; k += blockDim.x)
+    if (s_sum[k]) atomicAdd(&sums[k], s_sum[k]);
+}
+
 static unsigned grid_q5(const olap_ctx* ctx, int64_t n, int threads) {
   int64_t g = (n + threads - 1) / threads;
   const int64_t cap = static_cast<int64_t>(ctx->sm_count) * (2048 / threads);
@@ -149,6 +305,11 @@ int olap_q5_chain(olap_ctx* ctx, const olap_q5_tables* t, int32_t region, int32_
                "1..64 nations");
   OLAP_REQUIRE(ctx, t->n_supp >= 0 && t->n_cust >= 0 && t->n_orders >= 0 && t->n_lines >= 0, "bad sizes");
   OLAP_REQUIRE(ctx, t->r_regionkey && t->n_regionkey, "null region or nation table");
+  OLAP_REQUIRE(ctx, t->n_supp == 0 || t->s_nationkey, "null s_nationkey");
+  OLAP_REQUIRE(ctx, t->n_cust == 0 || t->c_nationkey, "null c_nationkey");
+  OLAP_REQUIRE(ctx, t->n_orders == 0 || (t->o_custkey && t->o_orderdate), "null orders column");
+  OLAP_REQUIRE(ctx, t->n_lines == 0 || (t->l_suppkey && t->l_orderkey && t->l_price && t->l_discount),
+               "null lineitem column");
   olap::Arena ar(ctx);
   int8_t* dim_s = ar.take<int8_t>(static_cast<size_t>(t->n_supp > 0 ? t->n_supp : 1));
   int8_t* dim_o = ar.take<int8_t>(static_cast<size_t>(t->n_orders > 0 ? t->n_orders : 1));
@@ -177,6 +338,84 @@ int olap_q5_chain(olap_ctx* ctx, const olap_q5_tables* t, int32_t region, int32_
     grid = std::min<int64_t>(grid, (t->n_lines / 4 + 511) / 512 + 1);
     olap::q5_lines_kernel<<<static_cast<unsigned>(grid), 512, smem, ctx->stream>>>(
         t->l_suppkey, t->l_orderkey, t->l_price, t->l_discount, t->n_lines, dim_s, t->n_supp, dim_o, t->n_orders,
+        reinterpret_cast<unsigned long long*>(nation_sums), &ctx->counters->range_errors, stage ? 1 : 0);
+  }
+  OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  return OLAP_OK;
+}
+
+int olap_q5_batch(olap_ctx* ctx, const olap_q5_tables* t, const olap_q5_query* queries, int n_queries,
+                  int64_t* nation_sums) {
+  if (!ctx || !t) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_REQUIRE(ctx, nation_sums && queries, "null output or query list");
+  OLAP_REQUIRE(ctx, n_queries >= 1 && n_queries <= OLAP_Q5_MAX_BATCH, "1..64 queries per batch");
+  OLAP_REQUIRE(ctx, t->n_region >= 1 && t->n_nation >= 1 && t->n_nation <= olap::kQ5MaxNations,
+               "1..64 nations");
+  OLAP_REQUIRE(ctx, t->n_supp >= 0 && t->n_cust >= 0 && t->n_orders >= 0 && t->n_lines >= 0, "bad sizes");
+  OLAP_REQUIRE(ctx, t->r_regionkey && t->n_regionkey, "null region or nation table");
+  OLAP_REQUIRE(ctx, t->n_supp == 0 || t->s_nationkey, "null s_nationkey");
+  OLAP_REQUIRE(ctx, t->n_cust == 0 || t->c_nationkey, "null c_nationkey");
+  OLAP_REQUIRE(ctx, t->n_orders == 0 || (t->o_custkey && t->o_orderdate), "null orders column");
+  OLAP_REQUIRE(ctx, t->n_lines == 0 || (t->l_suppkey && t->l_orderkey && t->l_price && t->l_discount),
+               "null lineitem column");
+  olap::Q5BatchDesc D;
+  std::memset(&D, 0, sizeof(D));
+  D.n_q = n_queries;
+  int64_t lo = INT64_MAX, hi = INT64_MIN;
+  for (int q = 0; q < n_queries; ++q) {
+    D.region[q] = queries[q].region;
+    D.d1[q] = queries[q].date1;
+    D.d2[q] = queries[q].date2;
+    if (queries[q].date1 < queries[q].date2) {
+      lo = std::min<int64_t>(lo, queries[q].date1);
+      hi = std::max<int64_t>(hi, queries[q].date2);
+    }
+  }
+  // every date range empty: span 1 at an arbitrary date, its mask 0
+  if (lo > hi) lo = hi = 0;
+  D.dlo = static_cast<int32_t>(lo);
+  D.span = hi - lo <= olap::kQ5DateTable ? static_cast<int32_t>(hi - lo > 0 ? hi - lo : 1) : 0;
+  olap::Arena ar(ctx);
+  int8_t* dim_s = ar.take<int8_t>(static_cast<size_t>(t->n_supp > 0 ? t->n_supp : 1));
+  int8_t* dim_o = ar.take<int8_t>(static_cast<size_t>(t->n_orders > 0 ? t->n_orders : 1));
+  unsigned long long* nat_q = ar.take<unsigned long long>(olap::kQ5MaxNations);
+  unsigned long long* date_q = ar.take<unsigned long long>(olap::kQ5DateTable);
+  if (!dim_s || !dim_o || !nat_q || !date_q)
+    return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for Q5 vectors");
+  const size_t out_bytes = sizeof(int64_t) * static_cast<size_t>(n_queries) * t->n_nation;
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(nation_sums, 0, out_bytes, ctx->stream));
+  olap::q5b_prep_kernel<<<8, 256, 0, ctx->stream>>>(t->r_regionkey, t->n_region, t->n_regionkey, t->n_nation, D,
+                                                    nat_q, date_q);
+  if (t->n_supp)
+    olap::q5b_supplier_kernel<<<olap::grid_q5(ctx, t->n_supp, 256), 256, 0, ctx->stream>>>(t->s_nationkey,
+                                                                                          t->n_supp, nat_q, dim_s);
+  const size_t date_bytes = sizeof(unsigned long long) * static_cast<size_t>(D.span);
+  if (t->n_orders) {
+    if (date_bytes > 48 * 1024)
+      OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::q5b_orders_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(date_bytes)));
+    olap::q5b_orders_kernel<<<olap::grid_q5(ctx, t->n_orders, 256), 256, date_bytes, ctx->stream>>>(
+        t->o_custkey, t->o_orderdate, t->n_orders, t->c_nationkey, t->n_cust, nat_q, date_q, D, dim_o,
+        &ctx->counters->range_errors);
+  }
+  if (t->n_lines) {
+    const size_t fixed = date_bytes + out_bytes;
+    const size_t stage_bytes = static_cast<size_t>((t->n_supp + 15) & ~int64_t(15));
+    const size_t budget = static_cast<size_t>(ctx->smem_optin) - 2048;  // static shared + headroom
+    const bool stage = fixed + stage_bytes <= budget;
+    const size_t smem = fixed + (stage ? stage_bytes : 0);
+    if (smem > 48 * 1024)
+      OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::q5b_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(smem)));
+    int bps = 1;
+    OLAP_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, olap::q5b_lines_kernel, 1024, smem));
+    int64_t grid = static_cast<int64_t>(ctx->sm_count) * (bps < 1 ? 1 : bps);
+    grid = std::min<int64_t>(grid, (t->n_lines / 4 + 1023) / 1024 + 1);
+    olap::q5b_lines_kernel<<<static_cast<unsigned>(grid), 1024, smem, ctx->stream>>>(
+        t->l_suppkey, t->l_orderkey, t->l_price, t->l_discount, t->n_lines, dim_s, t->n_supp, dim_o, t->o_orderdate,
+        t->n_orders, nat_q, date_q, D, static_cast<int>(t->n_nation),
         reinterpret_cast<unsigned long long*>(nation_sums), &ctx->counters->range_errors, stage ? 1 : 0);
   }
   OLAP_CUDA_TRY(ctx, cudaGetLastError());

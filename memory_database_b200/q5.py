@@ -12,7 +12,7 @@ from __future__ import annotations
 import ctypes as C
 from dataclasses import dataclass
 
-from ._lib import Q5Tables, check, lib
+from ._lib import Q5_MAX_BATCH, Q5Query, Q5Tables, check, lib
 from .olapcore import Context, _ptr
 
 DAYS = 7 * 365
@@ -70,3 +70,27 @@ def q5(ctx: Context, data: Q5Data, region: int, date1: int, date2: int, out=None
     t = data.c_struct()
     check(lib.olap_q5_chain(ctx.handle, C.byref(t), int(region), int(date1), int(date2), _ptr(sums)), ctx.handle)
     return sums
+
+
+def q5_batch(ctx: Context, data: Q5Data, queries, out=None):
+    """Up to 64 (region, date1, date2) queries in one pass; int64 [n, n_nation]."""
+    import torch
+    if not 1 <= len(queries) <= Q5_MAX_BATCH:
+        raise ValueError("1..64 queries per Q5 batch")
+    ctx.follow_torch_stream()
+    n_nation = data.cols["n_regionkey"].numel()
+    sums = out if out is not None else torch.empty((len(queries), n_nation), dtype=torch.int64, device="cuda")
+    qs = (Q5Query * len(queries))(*[Q5Query(int(r), int(a), int(b)) for r, a, b in queries])
+    t = data.c_struct()
+    check(lib.olap_q5_batch(ctx.handle, C.byref(t), qs, len(queries), _ptr(sums)), ctx.handle)
+    return sums
+
+
+def random_q5_queries(rng, n: int):
+    """(region, date1, date2): a uniform region and a one-year range starting
+    on a uniform day of the first six years (~1/7 of the orders)."""
+    out = []
+    for _ in range(n):
+        d1 = int(rng.integers(0, DAYS - 365))
+        out.append((int(rng.integers(0, 5)), d1, d1 + 365))
+    return out

@@ -79,9 +79,11 @@ def test_batch_equals_queries_alone(ctx, setup, agg):
 def test_batch_graph_replay_with_new_queries(ctx, setup):
     rng = np.random.default_rng(99)
     eng = None
-    for rep in range(4):  # same shape: recorded once per staging slot, then replayed
-        qs = batch.random_queries(rng, 64, setup[4], GROUPS)
+    for rep, nq in enumerate((64, 64, 17, 40, 1, 64)):
+        # recorded once per staging slot, then replayed for any query count
+        qs = batch.random_queries(rng, nq, setup[4], GROUPS)
         eng = _check_batch(ctx, setup, qs, olapcore.AGG_M1_PLUS_M2, use_graph=True, eng=eng)
+    assert eng.graph_captures() == 2
 
 
 def test_batch_plain_path_matches_oracle(ctx, setup):

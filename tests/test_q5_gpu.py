@@ -41,3 +41,39 @@ def test_q5_config_sizes_and_invalid_references(ctx):
     got = Q5.q5(ctx, data, 2, 365, 730).cpu().numpy()
     exp, errs = oracle.q5(h, 2, 365, 730)
     assert np.array_equal(got, exp) and ctx.take_range_errors() == errs > 0
+
+
+def test_q5_batch_equals_queries_alone(ctx):
+    data = Q5.make_q5_data(ctx, n_supp=20_000, n_cust=150_000, n_orders=2_000_000, n_lines=8_000_003)
+    rng = np.random.default_rng(4)
+    qs = Q5.random_q5_queries(rng, 64)
+    qs[0] = (1, 100, 100)            # empty date range
+    qs[1] = (7, 0, 365)              # no such region
+    qs[2] = (3, -5, Q5.DAYS + 5)     # every order
+    for n in (1, 2, 17, 64):
+        got = Q5.q5_batch(ctx, data, qs[:n]).cpu().numpy()
+        for q in range(n):
+            alone = Q5.q5(ctx, data, *qs[q]).cpu().numpy()
+            assert np.array_equal(got[q], alone), (n, q, qs[q])
+    h = _host(data)
+    exp, _ = oracle.q5(h, *qs[5])
+    assert np.array_equal(got[5], exp)
+    # a span wider than the date table: the per-query loop path
+    wide = [(r, 0, 20_000) for r in range(5)] + [(2, 365, 730)]
+    got = Q5.q5_batch(ctx, data, wide).cpu().numpy()
+    for q, w in enumerate(wide):
+        assert np.array_equal(got[q], Q5.q5(ctx, data, *w).cpu().numpy())
+    assert ctx.take_range_errors() == 0
+
+
+def test_q5_batch_counts_invalid_references_once(ctx):
+    data = Q5.make_q5_data(ctx, n_supp=5_000, n_cust=50_000, n_orders=500_000, n_lines=2_000_000)
+    data.cols["l_suppkey"][::997] = 5_001
+    data.cols["o_custkey"][::101] = 0
+    qs = [(r, 0, Q5.DAYS) for r in range(5)]
+    got = Q5.q5_batch(ctx, data, qs).cpu().numpy()
+    errs_batch = ctx.take_range_errors()
+    for q, w in enumerate(qs):
+        assert np.array_equal(got[q], Q5.q5(ctx, data, *w).cpu().numpy())
+        ctx.synchronize()
+        assert ctx.take_range_errors() == errs_batch  # every order in range: same count alone

@@ -53,9 +53,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tune", type=str, default="", help="knob=value,... (olap_ctx_set_tuning)")
-    ap.add_argument("--suite", default="starjoin", choices=["starjoin", "batched", "serving"],
+    ap.add_argument("--suite", default="starjoin", choices=["starjoin", "batched", "serving", "operators"],
                     help="starjoin: the headline line; batched: 64-query batches vs one launch per query; "
-                         "serving: Poisson arrivals of the 70/30 star-join/Q5 mix, batched vs plain")
+                         "serving: Poisson arrivals of the 70/30 star-join/Q5 mix, batched vs plain; "
+                         "operators: select/gather/hash join/hash group-by at 2^28 rows")
+    ap.add_argument("--op-rows", type=int, default=1 << 28)
     ap.add_argument("--rates", type=float, nargs="+", default=[50, 200, 500, 1000, 2000])
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--queries", type=int, default=64)
@@ -323,6 +325,146 @@ def run_serving(a) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_operators(a) -> None:
+    """Operator configuration at --op-rows int32 rows: select (col < t) to row
+    ids at four selectivities, gather of 4 columns by those ids, hash join
+    (2^24 unique build keys; probe keys uniform or Zipf(1.0) over them, half
+    replaced by keys that match nothing), hash group-by SUM/COUNT at four
+    cardinalities.  Device time per call (CUDA events, inputs resident, each
+    input larger than L2); every result is checked on the device against a
+    torch restatement."""
+    import ctypes as C
+    import torch
+    from memory_database_b200 import _lib, olapcore
+    from memory_database_b200.olapcore import _ptr
+    L = _lib.lib
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = olapcore.Context(0, stream=stream)
+    h = ctx.handle
+    n = a.op_rows
+    peak, peak_src = measured_peak_gbs()
+
+    def gen(m, st, lo, hi):
+        x = torch.empty(m, dtype=torch.int32, device="cuda")
+        _lib.check(L.olap_gen_uniform_i32_dev(h, _ptr(x), m, 99, st, lo, hi), h)
+        return x
+
+    def timed(fn, reps=5, warm=2):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def entry(name, ms, alg_bytes, ok, **kw):
+        gbs = alg_bytes / ms / 1e6
+        d = {"op": name, "ms": ms, "rows_per_s": n / (ms / 1e3), "alg_GBs": gbs, "frac_of_peak": gbs / peak,
+             "checked": bool(ok)}
+        d.update(kw)
+        return d
+
+    res = []
+    col = gen(n, 100, 0, (1 << 20) - 1)
+    cols4 = [gen(n, 101 + c, -1000, 1000) for c in range(4)]
+    ids = torch.empty(n, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    outs = [torch.empty(n, dtype=torch.int32, device="cuda") for _ in range(4)]
+    cp = (C.c_void_p * 4)(*[_ptr(x) for x in cols4])
+    op = (C.c_void_p * 4)(*[_ptr(x) for x in outs])
+    for sel in (0.001, 0.01, 0.1, 0.5):
+        t = int(sel * (1 << 20))
+
+        def sel_fn():
+            _lib.check(L.olap_select_rowids(h, _ptr(col), n, t, _lib.CMP_LT, None, 0, _ptr(ids), _ptr(cnt)), h)
+        ms = timed(sel_fn)
+        k = int(cnt.item())
+        got = ids[:k]
+        ok = k == int((col < t).sum()) and bool((col[got.long()] < t).all()) and bool((got[1:] > got[:-1]).all())
+        res.append(entry("select col<t -> row ids", ms, 4 * n + 4 * k, ok, selectivity=sel, matches=k))
+
+        def gat_fn():
+            _lib.check(L.olap_gather_i32(h, _ptr(ids), k, 4, cp, n, op), h)
+        ms = timed(gat_fn)
+        gl = got.long()
+        ok = all(torch.equal(outs[c][:k], cols4[c][gl]) for c in range(4))
+        res.append(entry("gather 4 int32 columns by row ids", ms, 36 * k, ok, selectivity=sel, k=k))
+    del outs, ids, cols4
+    torch.cuda.empty_cache()
+    # hash join: build keys = a bijection of [0, 2^24) onto [1, 2^24] (odd multiplier mod 2^24)
+    nb = 1 << 24
+    bkeys = ((torch.arange(nb, device="cuda", dtype=torch.int64) * 2654435761) % nb + 1).to(torch.int32)
+    bpay = gen(nb, 110, -1000, 1000)
+    cap = int(L.olap_hashtable_capacity(nb))
+    table = torch.empty(cap, dtype=torch.int64, device="cuda")
+
+    def build_fn():
+        _lib.check(L.olap_hashjoin_build(h, _ptr(bkeys), _ptr(bpay), nb, _ptr(table), cap), h)
+    ms = timed(build_fn, reps=3)
+    res.append(entry("hash join build (2^24 unique keys)", ms, 16 * nb, True, build_rows=nb, capacity=cap))
+    dense = torch.zeros(nb + 1, dtype=torch.int64, device="cuda")
+    dense[bkeys.long()] = bpay.long()
+    s_ = torch.zeros(1, dtype=torch.int64, device="cuda")
+    m_ = torch.zeros(1, dtype=torch.int64, device="cuda")
+    miss = gen(n, 112, 0, 1) == 0
+    for dist in ("uniform", "zipf1.0"):
+        idx = torch.empty(n, dtype=torch.int32, device="cuda")
+        if dist == "uniform":
+            _lib.check(L.olap_gen_uniform_i32_dev(h, _ptr(idx), n, 99, 111, 0, nb - 1), h)
+        else:
+            _lib.check(L.olap_gen_zipf_i32_dev(h, _ptr(idx), n, 99, 113, nb, 1.0), h)
+        pk = bkeys[idx.long()]
+        pk = torch.where(miss, pk + nb + 7, pk).contiguous()   # half match nothing
+        del idx
+
+        def probe_fn():
+            _lib.check(L.olap_hashjoin_probe(h, _ptr(table), cap, _ptr(pk), n, _ptr(s_), _ptr(m_), None, None), h)
+        ms = timed(probe_fn)
+        inr = pk <= nb
+        exp_s = int(dense[torch.where(inr, pk, 0).long()].sum())
+        ok = int(s_.item()) == exp_s and int(m_.item()) == int(inr.sum())
+        res.append(entry("hash join probe (SUM payload, 50% match)", ms, 12 * n, ok, keys=dist,
+                         matches=int(m_.item())))
+        del pk, inr
+    del table, dense, bkeys, bpay, miss
+    torch.cuda.empty_cache()
+    vals = gen(n, 120, 1, 10000)
+    for G in (16, 1 << 12, 1 << 20, 1 << 22):
+        keys = gen(n, 121, 0, G - 1)
+        gcap = int(L.olap_group_hash_capacity(G))
+        ok_, os_, oc_ = (torch.empty(gcap, dtype=t, device="cuda") for t in (torch.int32, torch.int64, torch.int64))
+        g_ = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+        def grp_fn():
+            _lib.check(L.olap_group_hash(h, n, _ptr(keys), 0, _ptr(vals), None, gcap, _ptr(ok_), _ptr(os_),
+                                         _ptr(oc_), _ptr(g_)), h)
+        ms = timed(grp_fn, reps=3)
+        k = int(g_.item())
+        es = torch.zeros(G, dtype=torch.int64, device="cuda").index_add_(0, keys.long(), vals.long())
+        ec = torch.bincount(keys.long(), minlength=G)
+        gs = torch.zeros(G, dtype=torch.int64, device="cuda")
+        gc = torch.zeros(G, dtype=torch.int64, device="cuda")
+        gs[ok_[:k].long()] = os_[:k]
+        gc[ok_[:k].long()] = oc_[:k]
+        ok = k == int((ec > 0).sum()) and torch.equal(gs, es) and torch.equal(gc, ec)
+        res.append(entry("hash group-by SUM/COUNT", ms, 8 * n, ok, groups=G))
+        del keys, ok_, os_, oc_
+    line = {"metric": "operator rows/sec and HBM GB/s vs peak", "value": min(r["frac_of_peak"] for r in res),
+            "unit": "min fraction of peak over the operators", "n_gpus": 1, "rows": n, "operators": res,
+            "peak_GBs": peak, "peak_source": peak_src, "all_checked": all(r["checked"] for r in res),
+            "config": {"workload": f"operator set at {n:,} int32 rows (select at 0.001/0.01/0.1/0.5, gather of 4 "
+                                   "columns, hash join 2^24 build / uniform and Zipf(1.0) probes at 50% match, "
+                                   "hash group-by at 16/4096/2^20/2^22 groups)"},
+            "data": "synthetic (seeded counter-based generator, generated in HBM)"}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     a = parse()
     if a.impl == "reference":
@@ -333,6 +475,9 @@ def main() -> None:
         return
     if a.suite == "serving":
         run_serving(a)
+        return
+    if a.suite == "operators":
+        run_operators(a)
         return
     import torch
     import torch.distributed as dist

@@ -5,7 +5,8 @@
 // its OID lists in row order (OLAPcore/test_multi_compute_operator.cpp
 // :240-283).  The compaction here produces exactly that order in one pass
 // over the input: each block claims tiles in increasing order through an
-// atomic counter, ranks its selected items with a block-wide scan, and finds
+// atomic counter, ranks its selected items with warp ballots and a scan of
+// the warp counts, and finds
 // the tile's output offset with a decoupled look-back over the status words
 // of the preceding tiles (a warp inspects 32 predecessors at a time).
 //
@@ -20,8 +21,7 @@
 namespace olap {
 
 constexpr int kCompactThreads = 256;
-constexpr int kCompactGroups = 4;                                 // int4 loads per thread
-constexpr int kCompactTile = kCompactThreads * 4 * kCompactGroups;  // 4096 items
+constexpr int kCompactGroups = 4;  // default int4 loads per thread and tile (ops set Op::kGroups)
 constexpr uint32_t kSpinLimit = 1u << 22;
 
 // Status word of a tile: flag in bits 62-63 (0 none, 1 aggregate, 2
@@ -98,76 +98,95 @@ __device__ __forceinline__ int64_t lookback(const ScanTiles& st, int64_t tile, u
   return static_cast<int64_t>(excl);
 }
 
-// Block-wide exclusive scan of four 16-bit counters packed in a uint64
-// (one counter per int4 group of the thread).  Returns the thread's exclusive
-// prefix; *block_total receives the packed totals.
-__device__ __forceinline__ uint64_t block_scan_packed(uint64_t v, uint64_t* s_warp, uint64_t* block_total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint64_t x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_warp[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    const int nw = blockDim.x >> 5;
-    uint64_t w = lane < nw ? s_warp[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
-    }
-    if (lane < nw) s_warp[lane] = w;  // inclusive per warp
-  }
-  __syncthreads();
-  const uint64_t warp_excl = warp > 0 ? s_warp[warp - 1] : 0;
-  *block_total = s_warp[(blockDim.x >> 5) - 1];
-  __syncthreads();
-  return warp_excl + x - v;
-}
-
-__device__ __forceinline__ uint32_t field16(uint64_t packed, int u) {
-  return static_cast<uint32_t>((packed >> (16 * u)) & 0xffffu);
-}
-
-// Generic compaction kernel.  Items are numbered 0 .. n_items-1; each thread
-// handles kCompactGroups groups of 4 consecutive items per tile.  The Op is
-// called per group and per selected item:
-//   uint32_t op.flags(int u, int64_t first, int nv)  -> 4-bit mask of the
-//       selected items among first .. first+3 (only the first nv exist);
-//       the op may cache what it loaded for group u;
+// Compaction kernel.  Items are numbered 0 .. n_items-1.  A tile holds
+// kCompactThreads x 4 x G items (G = Op::kGroups); in group u, lane l of
+// warp w owns the 4 consecutive items tile_first + u*1024 + w*128 + 4l + k,
+// so each group is one coalesced 16-byte load per thread and row order is
+// (u, w, l, k).  A thread ranks its selected items inside its warp with four
+// ballots, the block ranks the (u, w) warp counts with one warp scan, and the
+// tile's output base comes from the look-back.  The Op is called per group
+// and per selected item:
+//   template <bool kFull> uint32_t op.flags(int u, int64_t first, int nv)
+//       -> 4-bit mask of the selected items among first .. first+3 (only the
+//       first nv exist); kFull: nv == 4 and op.vec_ok() (16-byte loads are
+//       allowed), and op.prefetch(u, first) ran for every group first; the
+//       op may cache what it loaded for group u;
 //   void op.emit(int u, int k, int64_t item, int64_t pos)  -> write selected
 //       item `item` (= first + k of group u) at output position `pos`.
+// A larger G keeps more bytes in flight per block for ops that cache little.
+template <class Op>
+constexpr int64_t compact_tile_items() {
+  return static_cast<int64_t>(kCompactThreads) * 4 * Op::kGroups;
+}
+
 template <class Op>
 __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const Op op_in, int64_t n_items, ScanTiles st) {
+  constexpr int G = Op::kGroups;
+  constexpr int W = kCompactThreads / 32;
+  constexpr int E = G * W;  // warp counts per tile
+  static_assert(G <= 16 && E % 32 == 0, "groups per thread: a multiple of 4, at most 16");
+  constexpr int PER = E / 32;
   Op op = op_in;  // per-thread copy: ops cache the loaded items between flags() and emit()
   __shared__ unsigned int s_tile;
-  __shared__ uint64_t s_warp[kCompactThreads / 32];
+  __shared__ uint32_t s_cnt[E];  // warp counts of (u, w), then their exclusive prefixes in the tile
   __shared__ long long s_base;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
   for (;;) {
     const int64_t tile = claim_tile(st, &s_tile);
     if (tile >= st.n_tiles) return;
-    const int64_t tile_first = tile * kCompactTile;
-    uint32_t mask[kCompactGroups];
-    uint64_t packed = 0;
+    const int64_t tile_first = tile * compact_tile_items<Op>();
+    uint64_t masks = 0;  // 4 bits per group
+    if (op.vec_ok() && tile_first + compact_tile_items<Op>() <= n_items) {
+      // full tile, aligned columns: every group's loads are issued before
+      // the first is used, so G x 16 bytes per thread are in flight
 #pragma unroll
-    for (int u = 0; u < kCompactGroups; ++u) {
-      const int64_t first = tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
-      const int64_t left = n_items - first;
-      const int nv = left >= 4 ? 4 : (left > 0 ? static_cast<int>(left) : 0);
-      mask[u] = nv > 0 ? op.flags(u, first, nv) : 0u;
-      packed |= static_cast<uint64_t>(__popc(mask[u])) << (16 * u);
+      for (int u = 0; u < G; ++u)
+        op.prefetch(u, tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x);
+#pragma unroll
+      for (int u = 0; u < G; ++u) {
+        const int64_t first = tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
+        masks |= static_cast<uint64_t>(op.template flags<true>(u, first, 4)) << (4 * u);
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < G; ++u) {
+        const int64_t first = tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
+        const int64_t left = n_items - first;
+        const int nv = left >= 4 ? 4 : (left > 0 ? static_cast<int>(left) : 0);
+        const uint32_t m = nv > 0 ? op.template flags<false>(u, first, nv) : 0u;
+        masks |= static_cast<uint64_t>(m) << (4 * u);
+      }
     }
-    uint64_t tot;
-    const uint64_t excl = block_scan_packed(packed, s_warp, &tot);
-    uint64_t tile_count = 0;
 #pragma unroll
-    for (int u = 0; u < kCompactGroups; ++u) tile_count += field16(tot, u);
-    if (threadIdx.x < 32) {
+    for (int u = 0; u < G; ++u) {
+      const uint32_t c = __reduce_add_sync(0xffffffffu, __popc(static_cast<uint32_t>(masks >> (4 * u)) & 15u));
+      if (lane == 0) s_cnt[u * W + warp] = c;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t v[PER];
+      uint32_t sum = 0;
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        v[i] = s_cnt[lane * PER + i];
+        sum += v[i];
+      }
+      uint32_t inc = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+      }
+      uint32_t run = inc - sum;
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        s_cnt[lane * PER + i] = run;
+        run += v[i];
+      }
+      const uint64_t tile_count = __shfl_sync(0xffffffffu, inc, 31);
       const int64_t b = lookback(st, tile, tile_count);
-      if (threadIdx.x == 0) {
+      if (lane == 0) {
         s_base = b;
         if (tile == st.n_tiles - 1 && b >= 0) *st.total = static_cast<unsigned long long>(b) + tile_count;
       }
@@ -175,24 +194,27 @@ __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const Op op_in
     __syncthreads();
     const long long base = s_base;
     if (base < 0) return;  // timed out: the host reports it
-    uint64_t off = 0;
 #pragma unroll
-    for (int u = 0; u < kCompactGroups; ++u) {
-      const uint32_t m = mask[u];
-      int64_t pos = base + static_cast<int64_t>(off) + field16(excl, u);
+    for (int u = 0; u < G; ++u) {
+      const uint32_t m = static_cast<uint32_t>(masks >> (4 * u)) & 15u;
+      uint32_t before = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) before += __popc(__ballot_sync(0xffffffffu, (m >> k) & 1u) & lt);
+      if (!m) continue;
+      int64_t pos = base + s_cnt[u * W + warp] + before;
       const int64_t first = tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
 #pragma unroll
       for (int k = 0; k < 4; ++k)
         if ((m >> k) & 1u) op.emit(u, k, first + k, pos++);
-      off += field16(tot, u);
     }
   }
 }
 
-// Host helper: scan-tile state for n_items from the arena; zeroes it on the stream.
+// Host helper: scan-tile state for n_items in tiles of tile_items
+// (compact_tile_items<Op>()) from the arena; zeroes it on the stream.
 inline int make_scan_tiles(olap_ctx* ctx, Arena& ar, int64_t n_items, unsigned long long* total,
-                           cudaStream_t stream, ScanTiles* st) {
-  st->n_tiles = (n_items + kCompactTile - 1) / kCompactTile;
+                           cudaStream_t stream, ScanTiles* st, int64_t tile_items) {
+  st->n_tiles = (n_items + tile_items - 1) / tile_items;
   if (st->n_tiles < 1) st->n_tiles = 1;
   st->status = ar.take<unsigned long long>(static_cast<size_t>(st->n_tiles));
   st->next_tile = ar.take<unsigned int>(1);

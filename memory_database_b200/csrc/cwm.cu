@@ -107,6 +107,7 @@ __global__ void agg_cwm_kernel(const int16_t* __restrict__ gid, const int64_t* _
 
 // join_cwm_dv and starjoinalgo_cwm_dv: surviving rows in row order.
 struct SurvivorOp {
+  static constexpr int kGroups = kCompactGroups;
   DimSet d;
   int64_t* oid64;        // join_cwm_dv: OID (int64)
   int16_t* gid16;        //              groupID (int16)
@@ -115,6 +116,9 @@ struct SurvivorOp {
   unsigned long long* range_err;
   int4 g[kCompactGroups];
 
+  __device__ __forceinline__ bool vec_ok() const { return true; }
+  __device__ __forceinline__ void prefetch(int, int64_t) {}
+  template <bool kFull>
   __device__ __forceinline__ uint32_t flags(int u, int64_t first, int nv) {
     int32_t gg[4] = {0, 0, 0, 0};
     uint32_t m = 0;
@@ -247,7 +251,7 @@ int olap_join_cwm_dv(olap_ctx* ctx, int8_t* const* dimvec_array, const int64_t* 
   olap::Arena ar(ctx);
   olap::ScanTiles sc;
   st = olap::make_scan_tiles(ctx, ar, size_lineorder, reinterpret_cast<unsigned long long*>(d_index),
-                             ctx->stream, &sc);
+                             ctx->stream, &sc, olap::compact_tile_items<olap::SurvivorOp>());
   if (st != OLAP_OK) return st;
   olap::compact_kernel<olap::SurvivorOp><<<olap::compact_grid(ctx, sc.n_tiles), olap::kCompactThreads, 0,
                                           ctx->stream>>>(op, size_lineorder, sc);
@@ -343,7 +347,7 @@ int olap_starjoin_cwm_dv(olap_ctx* ctx, int64_t size_lineorder, int8_t* const* d
   olap::Arena ar(ctx);
   olap::ScanTiles sc;
   st = olap::make_scan_tiles(ctx, ar, size_lineorder, reinterpret_cast<unsigned long long*>(d_count),
-                             ctx->stream, &sc);
+                             ctx->stream, &sc, olap::compact_tile_items<olap::SurvivorOp>());
   if (st != OLAP_OK) return st;
   olap::compact_kernel<olap::SurvivorOp><<<olap::compact_grid(ctx, sc.n_tiles), olap::kCompactThreads, 0,
                                           ctx->stream>>>(op, size_lineorder, sc);

@@ -181,6 +181,7 @@ __global__ void __launch_bounds__(kGroupThreads) group_hash_kernel(int64_t n, co
 
 // Compaction of the occupied slots into (key, sum, count) arrays.
 struct SlotOp {
+  static constexpr int kGroups = kCompactGroups;
   const int32_t* keys;
   const unsigned long long* sums;
   const unsigned long long* counts;
@@ -189,6 +190,9 @@ struct SlotOp {
   int64_t* out_counts;
   int4 k4[kCompactGroups];
 
+  __device__ __forceinline__ bool vec_ok() const { return true; }
+  __device__ __forceinline__ void prefetch(int, int64_t) {}
+  template <bool kFull>
   __device__ __forceinline__ uint32_t flags(int u, int64_t first, int nv) {
     int32_t k[4] = {kEmptyKey, kEmptyKey, kEmptyKey, kEmptyKey};
     for (int j = 0; j < nv; ++j) k[j] = keys[first + j];
@@ -367,7 +371,8 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
     op.out_sums = out_sums;
     op.out_counts = out_counts;
     olap::ScanTiles sc;
-    st = olap::make_scan_tiles(ctx, ar, capacity, reinterpret_cast<unsigned long long*>(d_groups), ctx->stream, &sc);
+    st = olap::make_scan_tiles(ctx, ar, capacity, reinterpret_cast<unsigned long long*>(d_groups), ctx->stream,
+                               &sc, olap::compact_tile_items<olap::SlotOp>());
     if (st == OLAP_OK)
       olap::compact_kernel<olap::SlotOp><<<olap::compact_grid(ctx, sc.n_tiles), olap::kCompactThreads, 0,
                                           ctx->stream>>>(op, capacity, sc);

@@ -148,6 +148,7 @@ __global__ void __launch_bounds__(512) hash_probe_sum_kernel(const int32_t* __re
 
 // Matches (probe row, payload) in probe-row order.
 struct ProbeOp {
+  static constexpr int kGroups = kCompactGroups;
   const int32_t* keys;
   const uint64_t* slots;
   uint64_t mask;
@@ -156,9 +157,16 @@ struct ProbeOp {
   int32_t vec;
   int4 pay[kCompactGroups];
 
+  __device__ __forceinline__ bool vec_ok() const { return vec != 0; }
+  __device__ __forceinline__ void prefetch(int u, int64_t first) {
+    pay[u] = ld_stream_v4_ordered(keys + first, policy_evict_first());  // the keys, until flags() replaces them
+  }
+  template <bool kFull>
   __device__ __forceinline__ uint32_t flags(int u, int64_t first, int nv) {
     int32_t k[4] = {0, 0, 0, 0};
-    if (vec && nv == 4) {
+    if (kFull) {
+      k[0] = pay[u].x; k[1] = pay[u].y; k[2] = pay[u].z; k[3] = pay[u].w;
+    } else if (vec && nv == 4) {
       const int4 v = ld_stream_v4(keys + first, policy_evict_first());
       k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w;
     } else {
@@ -323,7 +331,7 @@ int olap_hashjoin_probe(olap_ctx* ctx, const uint64_t* table, int64_t capacity, 
     unsigned long long* total = (!d_sum && d_matches) ? reinterpret_cast<unsigned long long*>(d_matches)
                                                       : ar.take<unsigned long long>(1);
     if (!total) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
-    int rc = olap::make_scan_tiles(ctx, ar, n, total, ctx->stream, &st);
+    int rc = olap::make_scan_tiles(ctx, ar, n, total, ctx->stream, &st, olap::compact_tile_items<olap::ProbeOp>());
     if (rc != OLAP_OK) return rc;
     olap::compact_kernel<olap::ProbeOp><<<olap::compact_grid(ctx, st.n_tiles), olap::kCompactThreads, 0,
                                          ctx->stream>>>(op, n, st);

@@ -136,6 +136,15 @@ __device__ __forceinline__ int4 ld_stream_v4(const int32_t* p, uint64_t pol) {
       : "l"(p), "l"(pol));
   return v;
 }
+// The same load kept in program order with other issue-ordered loads, so a
+// batch of them is in flight before the first result is used.
+__device__ __forceinline__ int4 ld_stream_v4_ordered(const int32_t* p, uint64_t pol) {
+  int4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p), "l"(pol));
+  return v;
+}
 __device__ __forceinline__ int32_t ld_stream_s32(const int32_t* p, uint64_t pol) {
   int32_t v;
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"

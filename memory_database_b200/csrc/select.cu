@@ -21,8 +21,12 @@ __device__ __forceinline__ int32_t lane4(const int4& v, int k) {
   return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
 }
 
-// Items are rows (or positions of an input selection vector).
+// Items are rows (kRid false) or positions of an input selection vector.
+// The plain column case caches nothing between flags() and emit(), so it
+// takes 16 groups per thread (64 KB tiles); with row ids, 8.
+template <bool kRid>
 struct SelectOp {
+  static constexpr int kGroups = kRid ? 8 : 16;
   const int32_t* col;
   const int32_t* in_rowids;  // optional input selection vector
   int32_t* out;
@@ -31,13 +35,22 @@ struct SelectOp {
   int32_t val;
   int32_t cmp;
   int32_t vec;               // col (or in_rowids) 16-byte aligned
-  int4 rid[kCompactGroups];  // row ids of the group (in_rowids case)
+  int4 rid[kGroups];  // values (or row ids) of each group, loaded by prefetch()
 
+  __device__ __forceinline__ bool vec_ok() const { return vec != 0; }
+  __device__ __forceinline__ void prefetch(int u, int64_t first) {
+    rid[u] = ld_stream_v4_ordered((kRid ? in_rowids : col) + first, policy_evict_first());
+  }
+  template <bool kFull>
   __device__ __forceinline__ uint32_t flags(int u, int64_t first, int nv) {
     const uint64_t pol = policy_evict_first();
     uint32_t m = 0;
-    if (!in_rowids) {
-      if (vec && nv == 4) {
+    if constexpr (!kRid) {
+      if (kFull) {
+        const int4 v = rid[u];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) m |= static_cast<uint32_t>(cmp_pass(lane4(v, k), val, cmp)) << k;
+      } else if (vec && nv == 4) {
         const int4 v = ld_stream_v4(col + first, pol);
 #pragma unroll
         for (int k = 0; k < 4; ++k) m |= static_cast<uint32_t>(cmp_pass(lane4(v, k), val, cmp)) << k;
@@ -46,7 +59,9 @@ struct SelectOp {
       }
     } else {
       int4 r = make_int4(0, 0, 0, 0);
-      if (vec && nv == 4) {
+      if (kFull) {
+        r = rid[u];
+      } else if (vec && nv == 4) {
         r = ld_stream_v4(in_rowids + first, pol);
       } else {
         int32_t t[4] = {0, 0, 0, 0};
@@ -68,12 +83,14 @@ struct SelectOp {
     return m;
   }
   __device__ __forceinline__ void emit(int u, int k, int64_t item, int64_t pos) {
-    out[pos] = in_rowids ? lane4(rid[u], k) : static_cast<int32_t>(item);
+    if constexpr (kRid) out[pos] = lane4(rid[u], k);
+    else out[pos] = static_cast<int32_t>(item);
   }
 };
 
 // Rows where Ra <= c and Rc <= c; writes the pair (Ra, Rc).
 struct ProjectOp {
+  static constexpr int kGroups = kCompactGroups;
   const int32_t* ra;
   const int32_t* rc;
   int32_t* out_a;
@@ -82,9 +99,17 @@ struct ProjectOp {
   int32_t vec;
   int4 a[kCompactGroups], c[kCompactGroups];
 
+  __device__ __forceinline__ bool vec_ok() const { return vec != 0; }
+  __device__ __forceinline__ void prefetch(int u, int64_t first) {
+    a[u] = ld_stream_v4(ra + first, policy_evict_first());
+    c[u] = ld_stream_v4(rc + first, policy_evict_first());
+  }
+  template <bool kFull>
   __device__ __forceinline__ uint32_t flags(int u, int64_t first, int nv) {
     const uint64_t pol = policy_evict_first();
-    if (vec && nv == 4) {
+    if (kFull) {
+      // a[u], c[u] loaded by prefetch()
+    } else if (vec && nv == 4) {
       a[u] = ld_stream_v4(ra + first, pol);
       c[u] = ld_stream_v4(rc + first, pol);
     } else {
@@ -221,7 +246,7 @@ static int run_compaction(olap_ctx* ctx, const Op& op, int64_t n_items, int64_t*
   unsigned long long* total = d_count ? reinterpret_cast<unsigned long long*>(d_count)
                                       : ar.take<unsigned long long>(1);
   if (!total) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
-  int rc = make_scan_tiles(ctx, ar, n_items, total, ctx->stream, &st);
+  int rc = make_scan_tiles(ctx, ar, n_items, total, ctx->stream, &st, compact_tile_items<Op>());
   if (rc != OLAP_OK) return rc;
   compact_kernel<Op><<<compact_grid(ctx, st.n_tiles), kCompactThreads, 0, ctx->stream>>>(op, n_items, st);
   OLAP_CUDA_TRY(ctx, cudaGetLastError());
@@ -249,16 +274,24 @@ int olap_select_rowids(olap_ctx* ctx, const int32_t* col, int64_t col_len, int32
                "lengths must be in [0, 2^31)");
   OLAP_REQUIRE(ctx, cmp == OLAP_CMP_LE || cmp == OLAP_CMP_LT, "cmp must be OLAP_CMP_LE or OLAP_CMP_LT");
   OLAP_REQUIRE(ctx, n == 0 || (col && out_rowids), "null column or output");
-  olap::SelectOp op;
-  std::memset(&op, 0, sizeof(op));
-  op.col = col;
-  op.in_rowids = in_rowids;
-  op.out = out_rowids;
-  op.range_err = &ctx->counters->range_errors;
-  op.col_len = col_len;
-  op.val = val;
-  op.cmp = cmp;
-  op.vec = in_rowids ? olap::al16(in_rowids) : olap::al16(col);
+  auto fill = [&](auto& op) {
+    std::memset(&op, 0, sizeof(op));
+    op.col = col;
+    op.in_rowids = in_rowids;
+    op.out = out_rowids;
+    op.range_err = &ctx->counters->range_errors;
+    op.col_len = col_len;
+    op.val = val;
+    op.cmp = cmp;
+    op.vec = in_rowids ? olap::al16(in_rowids) : olap::al16(col);
+  };
+  if (in_rowids) {
+    olap::SelectOp<true> op;
+    fill(op);
+    return olap::run_compaction(ctx, op, n, d_count);
+  }
+  olap::SelectOp<false> op;
+  fill(op);
   return olap::run_compaction(ctx, op, n, d_count);
 }
 

@@ -70,6 +70,8 @@ extern "C" {
 #define OLAP_TUNE_UNROLL 5          /* scan mode: 1 plain, 2 pipelined x512, 3 pipelined x256 */
 #define OLAP_TUNE_PROBE_BITS 6      /* global pass bitmaps for unstaged dims: 1 on, 2 off (default) */
 #define OLAP_TUNE_SMEM_BITS_BYTES 7 /* bytes of pass bitmaps staged in smem (default 0)          */
+#define OLAP_TUNE_GROUP_COMBINE 8   /* hash group-by warp combining of equal keys: 1 on, 2 off (default) */
+#define OLAP_TUNE_GROUP_PLAN 9      /* hash group-by: 1 per-block tables (capacity <= 8192), 2 partitioned */
 
 typedef struct olap_ctx olap_ctx;
 
@@ -323,8 +325,11 @@ OLAP_API int64_t olap_group_hash_capacity(int64_t max_groups);
  * key_offset with SUM(vals[i] + vals2[i]) (vals2 may be NULL) and COUNT,
  * written unordered to out_keys/out_sums/out_counts (out_counts may be NULL),
  * *d_groups their number.  capacity (a power of two, see
- * olap_group_hash_capacity) bounds the number of distinct keys; the table is
- * taken from CUDA's stream-ordered pool.  Synchronous. */
+ * olap_group_hash_capacity; at most 2^27) bounds the number of distinct keys
+ * (more give OLAP_ERR_CAPACITY).  Up to capacity 8192 each block aggregates
+ * in a shared-memory table; above, the rows are first partitioned by key
+ * hash (the context keeps a grow-only device buffer of about 8-16 bytes per
+ * row for that).  Synchronous. */
 OLAP_API int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_offset,
                              const int32_t* vals, const int32_t* vals2, int64_t capacity,
                              int32_t* out_keys, int64_t* out_sums, int64_t* out_counts,

@@ -43,6 +43,8 @@ TUNE_HOST_CHUNK_ROWS = 4
 TUNE_UNROLL = 5
 TUNE_PROBE_BITS = 6
 TUNE_SMEM_BITS_BYTES = 7
+TUNE_GROUP_COMBINE = 8
+TUNE_GROUP_PLAN = 9
 
 
 class OlapError(RuntimeError):

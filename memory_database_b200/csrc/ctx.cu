@@ -97,6 +97,7 @@ int olap_ctx_destroy(olap_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->arena) cudaFree(ctx->arena);
+  if (ctx->big) cudaFree(ctx->big);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -12,9 +12,10 @@
 //
 // Dense group-by accumulates per block in shared memory when the group vector
 // fits (exact 64-bit sums from 32-bit shared atomics), else in L2 with 64-bit
-// atomics.  Hash group-by keeps a 4096-slot shared-memory table per block
-// (keys inserted with shared CAS) in front of a global open-addressing table;
-// rows that do not fit the block table go to the global table directly.
+// atomics.  Hash group-by aggregates in shared-memory tables: per block when
+// every distinct key fits one table, else per partition of the key hash
+// (see the plans below).
+#include <algorithm>
 #include <cstring>
 
 #include "compact.cuh"
@@ -121,62 +122,535 @@ __device__ __forceinline__ void global_add(const HashAgg& t, int32_t k, uint64_t
   atomicAdd(t.overflow, 1ull);
 }
 
-__global__ void __launch_bounds__(kGroupThreads) group_hash_kernel(int64_t n, const int32_t* __restrict__ keys,
-                                                                   int32_t key_offset,
-                                                                   const int32_t* __restrict__ vals,
-                                                                   const int32_t* __restrict__ vals2, HashAgg t,
-                                                                   unsigned long long* range_err) {
-  __shared__ int32_t skey[kSmemSlots];
-  __shared__ unsigned long long ssum[kSmemSlots];
-  __shared__ unsigned int scnt[kSmemSlots];
-  const int tid = threadIdx.x;
-  for (int i = tid; i < kSmemSlots; i += blockDim.x) {
-    skey[i] = kEmptyKey;
-    ssum[i] = 0;
-    scnt[i] = 0;
+// ---- hash group-by --------------------------------------------------------
+//
+// Two plans, chosen by the capacity (a power of two >= 2 x the distinct keys):
+//  * capacity <= kAggSlots: every block keeps a shared-memory table with
+//    `capacity` slots, so each distinct key stays in shared memory; blocks
+//    flush their tables into the global table once, and the occupied slots
+//    are compacted into the outputs.  One read of the columns.
+//  * larger: the rows are partitioned by high bits of the key hash into P
+//    partitions of at most capacity / (2P) <= kAggSlots / 2 distinct keys (a
+//    histogram pass, a scan of the partition offsets, a scatter pass), then
+//    one block per partition aggregates it in a kAggSlots-slot shared table
+//    and writes its groups straight to the outputs.
+// Optionally (OLAP_TUNE_GROUP_COMBINE) a warp first combines its rows that
+// share a key (match_any plus two 32-bit reductions of the split values), so
+// each distinct key of a warp costs one shared-table update.
+
+constexpr int kAggThreads = 1024;
+constexpr int kAggSlots = 8192;  // 16 B per slot: 128 KB of shared memory
+
+struct SmemAgg {
+  int32_t* key;
+  unsigned int* cnt;
+  unsigned long long* sum;
+  uint32_t slots;   // a power of two >= 4
+  uint32_t nb;      // buckets of 4 slots
+};
+
+__device__ __forceinline__ SmemAgg smem_agg(unsigned char* base, uint32_t slots) {
+  SmemAgg t;
+  t.sum = reinterpret_cast<unsigned long long*>(base);
+  t.key = reinterpret_cast<int32_t*>(t.sum + slots);
+  t.cnt = reinterpret_cast<unsigned int*>(t.key + slots);
+  t.slots = slots;
+  t.nb = slots >> 2;
+  return t;
+}
+
+__device__ __forceinline__ void smem_agg_clear(const SmemAgg& t) {
+  for (uint32_t i = threadIdx.x; i < t.slots; i += blockDim.x) {
+    t.key[i] = kEmptyKey;
+    t.cnt[i] = 0;
+    t.sum[i] = 0;
   }
+}
+
+__device__ __forceinline__ int4 lds_volatile_v4(const int32_t* p) {
+  int4 v;
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  asm volatile("ld.volatile.shared.v4.s32 {%0,%1,%2,%3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+  return v;
+}
+
+// Adds (s, c) to key k's slot; false when the table has no room for k.
+// Buckets of 4 slots, probed linearly: one 16-byte read finds k or the first
+// free slot of a bucket, which keeps the probe loops of a warp short at half
+// load.  Keys are never removed, so a key lives in the first bucket that had
+// a free slot when it was inserted, and a thread that loses a slot's CAS to
+// the same key uses that slot.
+__device__ __forceinline__ bool smem_agg_add(const SmemAgg& t, int32_t k, uint64_t s, uint32_t c) {
+  const uint32_t nb = t.nb;  // a power of two
+  // low hash bits: the partitions of plan 2 use the high ones
+  uint32_t b = mix32(static_cast<uint32_t>(k)) & (nb - 1);
+  for (uint32_t step = 0; step < nb; ++step) {
+    const int4 q = lds_volatile_v4(t.key + 4 * b);
+    int slot = q.x == k ? 0 : q.y == k ? 1 : q.z == k ? 2 : q.w == k ? 3 : -1;
+    if (slot < 0 && (q.x == kEmptyKey || q.y == kEmptyKey || q.z == kEmptyKey || q.w == kEmptyKey)) {
+      // k is new to this bucket and it has room: claim the first free slot
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int32_t cur = j == 0 ? q.x : j == 1 ? q.y : j == 2 ? q.z : q.w;
+        if (slot < 0 && cur == kEmptyKey) {
+          const int32_t prev = atomicCAS(t.key + 4 * b + j, kEmptyKey, k);
+          if (prev == kEmptyKey || prev == k) slot = j;
+        }
+      }
+    }
+    if (slot >= 0) {
+      smem_add_u64(t.sum + 4 * b + slot, s);
+      atomicAdd(t.cnt + 4 * b + slot, c);
+      return true;
+    }
+    b = (b + 1) & (nb - 1);
+  }
+  return false;
+}
+
+// Warp combine of the rows that share a key: returns true on the lane that
+// carries its key's (sum, count) for this warp step.  v lies in [-2^32, 2^32):
+// v + 2^32 splits into 24 low and 9 high bits, whose 32-bit sums over at most
+// 32 lanes cannot overflow.
+__device__ __forceinline__ bool warp_combine(bool valid, int32_t k, int64_t v, int64_t* gs, uint32_t* gc) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long tag = valid ? static_cast<unsigned long long>(static_cast<uint32_t>(k))
+                                       : (0x100000000ull | static_cast<unsigned long long>(lane));
+  const unsigned int m = __match_any_sync(0xffffffffu, tag);
+  if (__all_sync(0xffffffffu, (m & (m - 1)) == 0)) {  // no key repeats in this warp step
+    *gs = v;
+    *gc = 1;
+    return valid;
+  }
+  if (!valid) return false;
+  const uint64_t u = static_cast<uint64_t>(v + (int64_t(1) << 32));
+  const uint32_t lo = __reduce_add_sync(m, static_cast<uint32_t>(u & 0xffffffu));
+  const uint32_t hi = __reduce_add_sync(m, static_cast<uint32_t>(u >> 24));
+  const uint32_t c = __popc(m);
+  *gs = (static_cast<int64_t>(hi) << 24) + static_cast<int64_t>(lo) - (static_cast<int64_t>(c) << 32);
+  *gc = c;
+  return lane == __ffs(m) - 1;
+}
+
+__device__ __forceinline__ int32_t agg_key(int32_t key, int32_t key_offset) {
+  return static_cast<int32_t>(static_cast<uint32_t>(key) + static_cast<uint32_t>(key_offset));
+}
+
+// Rows [b, e) of the columns, 4 per thread per step (16-byte loads when
+// aligned), handed to f(valid, row, key, value) by every lane of the warp.
+template <class F>
+__device__ __forceinline__ void agg_rows(int64_t b, int64_t e, int64_t t0, int64_t stride, const int32_t* keys,
+                                         const int32_t* vals, const int32_t* vals2, bool vec, F&& f) {
+  const uint64_t pol = policy_evict_first();
+  const int64_t b4 = vec ? (b + 3) & ~int64_t(3) : e;  // first aligned row
+  const int64_t head = b4 < e ? b4 : e;
+  // head rows one by one (at most 3), then groups of 4, then the tail
+  for (int64_t base = b; base < head; base += stride) {
+    const int64_t r = base + t0;
+    const bool ok = r < head;
+    f(ok, ok ? keys[r] : 0, ok ? static_cast<int64_t>(vals[r]) + (vals2 ? vals2[r] : 0) : 0);
+  }
+  const int64_t n4 = (e - head) >> 2;
+  for (int64_t base = 0; base < n4; base += 2 * stride) {
+    // two groups of 4 rows per thread in flight before either is used
+    int4 k[2], v[2], w[2];
+    bool ok[2];
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      const int64_t i = base + g * stride + t0;
+      ok[g] = i < n4;
+      k[g] = make_int4(0, 0, 0, 0);
+      v[g] = k[g];
+      w[g] = k[g];
+      if (ok[g]) {
+        k[g] = ld_stream_v4(keys + head + 4 * i, pol);
+        v[g] = ld_stream_v4(vals + head + 4 * i, pol);
+        if (vals2) w[g] = ld_stream_v4(vals2 + head + 4 * i, pol);
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      f(ok[g], k[g].x, static_cast<int64_t>(v[g].x) + w[g].x);
+      f(ok[g], k[g].y, static_cast<int64_t>(v[g].y) + w[g].y);
+      f(ok[g], k[g].z, static_cast<int64_t>(v[g].z) + w[g].z);
+      f(ok[g], k[g].w, static_cast<int64_t>(v[g].w) + w[g].w);
+    }
+  }
+  for (int64_t base = head + 4 * n4; base < e; base += stride) {
+    const int64_t r = base + t0;
+    const bool ok = r < e;
+    f(ok, ok ? keys[r] : 0, ok ? static_cast<int64_t>(vals[r]) + (vals2 ? vals2[r] : 0) : 0);
+  }
+}
+
+// Plan 1: shared tables of `slots` = capacity slots per block, flushed into
+// the global table.
+__global__ void __launch_bounds__(kAggThreads) group_hash_smem_kernel(int64_t n, const int32_t* __restrict__ keys,
+                                                                      int32_t key_offset,
+                                                                      const int32_t* __restrict__ vals,
+                                                                      const int32_t* __restrict__ vals2,
+                                                                      uint32_t slots, int combine, HashAgg t,
+                                                                      unsigned long long* range_err) {
+  extern __shared__ __align__(16) unsigned char agg_smem[];
+  const SmemAgg st = smem_agg(agg_smem, slots);
+  smem_agg_clear(st);
   __syncthreads();
+  const bool vec = ((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(vals) |
+                     reinterpret_cast<uintptr_t>(vals2)) & 15) == 0;
+  // each block takes a contiguous share of the rows
+  const int64_t per = ((n + gridDim.x - 1) / gridDim.x + 3) & ~int64_t(3);
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * per;
+  const int64_t e = b + per < n ? b + per : n;
   unsigned int bad = 0;
-  auto add = [&](int32_t key, int64_t v) {
-    const int32_t k = static_cast<int32_t>(static_cast<uint32_t>(key) + static_cast<uint32_t>(key_offset));
-    if (k == kEmptyKey) {  // reserved as the empty marker
+  if (b < e)
+    agg_rows(b, e, threadIdx.x, blockDim.x, keys, vals, vals2, vec, [&](bool ok, int32_t key, int64_t v) {
+      const int32_t k = agg_key(key, key_offset);
+      if (ok && k == kEmptyKey) {  // reserved as the empty marker
+        ++bad;
+        ok = false;
+      }
+      int64_t gs = v;
+      uint32_t gc = 1;
+      if (combine ? warp_combine(ok, k, v, &gs, &gc) : ok)
+        if (!smem_agg_add(st, k, static_cast<uint64_t>(gs), gc)) global_add(t, k, static_cast<uint64_t>(gs), gc);
+    });
+  const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0 && wbad) atomicAdd(range_err, static_cast<unsigned long long>(wbad));
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x)
+    if (st.key[i] != kEmptyKey) global_add(t, st.key[i], st.sum[i], st.cnt[i]);
+}
+
+// Plan 2.  Partition of a key: the top bits of its hash (the shared tables
+// index with the low bits).
+__device__ __forceinline__ uint32_t agg_part(int32_t k, int part_shift) {
+  return part_shift >= 32 ? 0u : mix32(static_cast<uint32_t>(k)) >> part_shift;
+}
+
+struct PartPlan {
+  int64_t n;
+  int64_t per;        // rows per block of the histogram and scatter passes (multiple of 4)
+  int32_t n_blocks;   // blocks of those passes
+  int32_t n_parts;    // P (power of two)
+  int32_t part_shift; // 32 - log2(P)
+  int32_t key_offset;
+};
+
+// Per block and partition: rows of the block's share in the partition,
+// hist[b * P + p]; the partition totals are summed into ptot[p].
+__global__ void __launch_bounds__(1024) group_part_hist_kernel(PartPlan pp, const int32_t* __restrict__ keys,
+                                                               unsigned int* __restrict__ hist,
+                                                               unsigned long long* __restrict__ ptot,
+                                                               unsigned long long* range_err) {
+  extern __shared__ unsigned int s_hist[];
+  for (int p = threadIdx.x; p < pp.n_parts; p += blockDim.x) s_hist[p] = 0;
+  __syncthreads();
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * pp.per;
+  const int64_t e = b + pp.per < pp.n ? b + pp.per : pp.n;
+  const uint64_t pol = policy_evict_first();
+  const bool vec = (reinterpret_cast<uintptr_t>(keys) & 15) == 0;
+  unsigned int bad = 0;
+  auto one = [&](int32_t key) {
+    const int32_t k = agg_key(key, pp.key_offset);
+    if (k == kEmptyKey) {
       ++bad;
       return;
     }
-    uint32_t h = mix32(static_cast<uint32_t>(k)) & (kSmemSlots - 1);
-#pragma unroll 1
-    for (int step = 0; step < 8; ++step) {
-      const int32_t prev = atomicCAS(skey + h, kEmptyKey, k);
-      if (prev == kEmptyKey || prev == k) {
-        smem_add_u64(ssum + h, static_cast<uint64_t>(static_cast<int64_t>(v)));
-        atomicAdd(scnt + h, 1u);
-        return;
-      }
-      h = (h + 1) & (kSmemSlots - 1);
-    }
-    global_add(t, k, static_cast<uint64_t>(static_cast<int64_t>(v)), 1);  // block table crowded
+    atomicAdd(&s_hist[agg_part(k, pp.part_shift)], 1u);
   };
+  if (vec) {
+    for (int64_t r = b + 4 * threadIdx.x; r < e; r += 4 * blockDim.x) {
+      if (r + 4 <= e) {
+        const int4 k = ld_stream_v4(keys + r, pol);
+        one(k.x); one(k.y); one(k.z); one(k.w);
+      } else {
+        for (int64_t q = r; q < e; ++q) one(keys[q]);
+      }
+    }
+  } else {
+    for (int64_t r = b + threadIdx.x; r < e; r += blockDim.x) one(keys[r]);
+  }
+  const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0 && wbad) atomicAdd(range_err, static_cast<unsigned long long>(wbad));
+  __syncthreads();
+  for (int p = threadIdx.x; p < pp.n_parts; p += blockDim.x) {
+    const unsigned int c = s_hist[p];
+    hist[static_cast<int64_t>(blockIdx.x) * pp.n_parts + p] = c;
+    if (c) atomicAdd(&ptot[p], static_cast<unsigned long long>(c));
+  }
+}
+
+// Partition starts: part_begin[p] = rows of the partitions before p
+// (part_begin[P] = all rows); cursor[p] starts at part_begin[p].  One block.
+__global__ void __launch_bounds__(1024) group_part_scan_kernel(PartPlan pp, const unsigned long long* __restrict__ ptot,
+                                                               long long* __restrict__ part_begin,
+                                                               unsigned long long* __restrict__ cursor) {
+  __shared__ long long s_run[1024];
+  const int per = (pp.n_parts + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per;
+  const int e = b + per < pp.n_parts ? b + per : pp.n_parts;
+  long long s = 0;
+  for (int i = b; i < e; ++i) s += static_cast<long long>(ptot[i]);
+  s_run[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const long long y = threadIdx.x >= o ? s_run[threadIdx.x - o] : 0;
+    __syncthreads();
+    s_run[threadIdx.x] += y;
+    __syncthreads();
+  }
+  long long run = s_run[threadIdx.x] - s;
+  for (int i = b; i < e; ++i) {
+    part_begin[i] = run;
+    cursor[i] = static_cast<unsigned long long>(run);
+    run += static_cast<long long>(ptot[i]);
+  }
+  if (threadIdx.x == blockDim.x - 1) part_begin[pp.n_parts] = s_run[threadIdx.x];
+}
+
+// A partitioned row: {key, value} (8 bytes) or, with a second value
+// column, {key, pad, value as int64} (16 bytes): one store per row.
+template <bool HAS2>
+struct PartRow;
+template <>
+struct PartRow<false> {
+  using T = int2;
+  __device__ static T make(int32_t k, int32_t a, int32_t) { return make_int2(k, a); }
+  __device__ static int32_t key(const T& r) { return r.x; }
+  __device__ static int64_t val(const T& r) { return r.y; }
+};
+template <>
+struct PartRow<true> {
+  using T = longlong2;
+  __device__ static T make(int32_t k, int32_t a, int32_t c) {
+    return make_longlong2(static_cast<long long>(static_cast<uint32_t>(k)), static_cast<long long>(a) + c);
+  }
+  __device__ static int32_t key(const T& r) { return static_cast<int32_t>(static_cast<uint32_t>(r.x)); }
+  __device__ static int64_t val(const T& r) { return r.y; }
+};
+
+template <bool HAS2>
+__global__ void __launch_bounds__(1024) group_part_scatter_kernel(PartPlan pp, const int32_t* __restrict__ keys,
+                                                                  const int32_t* __restrict__ vals,
+                                                                  const int32_t* __restrict__ vals2,
+                                                                  const unsigned int* __restrict__ hist,
+                                                                  unsigned long long* __restrict__ cursor,
+                                                                  typename PartRow<HAS2>::T* __restrict__ rows) {
+  extern __shared__ unsigned int s_cur[];
+  // this block's run in each partition (order inside a partition is free)
+  for (int p = threadIdx.x; p < pp.n_parts; p += blockDim.x) {
+    const unsigned int c = hist[static_cast<int64_t>(blockIdx.x) * pp.n_parts + p];
+    s_cur[p] = c ? static_cast<unsigned int>(atomicAdd(&cursor[p], static_cast<unsigned long long>(c))) : 0u;
+  }
+  __syncthreads();
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * pp.per;
+  const int64_t e = b + pp.per < pp.n ? b + pp.per : pp.n;
   const uint64_t pol = policy_evict_first();
-  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid;
   const bool vec = ((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(vals) |
                      reinterpret_cast<uintptr_t>(vals2)) & 15) == 0;
-  const int64_t n4 = vec ? n >> 2 : 0;
-  for (int64_t i = t0; i < n4; i += stride) {
-    const int4 k = ld_stream_v4(keys + 4 * i, pol), v = ld_stream_v4(vals + 4 * i, pol);
-    const int4 w = vals2 ? ld_stream_v4(vals2 + 4 * i, pol) : make_int4(0, 0, 0, 0);
-    add(k.x, static_cast<int64_t>(v.x) + w.x);
-    add(k.y, static_cast<int64_t>(v.y) + w.y);
-    add(k.z, static_cast<int64_t>(v.z) + w.z);
-    add(k.w, static_cast<int64_t>(v.w) + w.w);
+  auto one = [&](int32_t key, int32_t a, int32_t c) {
+    const int32_t k = agg_key(key, pp.key_offset);
+    if (k == kEmptyKey) return;
+    const unsigned int pos = atomicAdd(&s_cur[agg_part(k, pp.part_shift)], 1u);
+    rows[pos] = PartRow<HAS2>::make(k, a, c);
+  };
+  if (vec) {
+    for (int64_t r = b + 4 * threadIdx.x; r < e; r += 4 * blockDim.x) {
+      if (r + 4 <= e) {
+        const int4 kk = ld_stream_v4(keys + r, pol), a = ld_stream_v4(vals + r, pol);
+        const int4 c = HAS2 ? ld_stream_v4(vals2 + r, pol) : make_int4(0, 0, 0, 0);
+        // the four cursor updates are independent: issue them together
+        const int32_t k[4] = {agg_key(kk.x, pp.key_offset), agg_key(kk.y, pp.key_offset),
+                              agg_key(kk.z, pp.key_offset), agg_key(kk.w, pp.key_offset)};
+        unsigned int pos[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          pos[u] = k[u] != kEmptyKey ? atomicAdd(&s_cur[agg_part(k[u], pp.part_shift)], 1u) : 0u;
+        const int32_t av[4] = {a.x, a.y, a.z, a.w}, cv[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (k[u] != kEmptyKey) rows[pos[u]] = PartRow<HAS2>::make(k[u], av[u], cv[u]);
+      } else {
+        for (int64_t q = r; q < e; ++q) one(keys[q], vals[q], HAS2 ? vals2[q] : 0);
+      }
+    }
+  } else {
+    for (int64_t r = b + threadIdx.x; r < e; r += blockDim.x) one(keys[r], vals[r], HAS2 ? vals2[r] : 0);
   }
-  for (int64_t r = 4 * n4 + t0; r < n; r += stride)
-    add(keys[r], static_cast<int64_t>(vals[r]) + (vals2 ? vals2[r] : 0));
-  const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
-  if ((tid & 31) == 0 && wbad) atomicAdd(range_err, static_cast<unsigned long long>(wbad));
+}
+
+// The same scatter with coalesced writes (P <= kTiledParts): each tile of
+// kScatterTile rows is counting-sorted by partition in shared memory, then
+// written out so that consecutive threads write consecutive rows of a
+// partition's run.  Shared memory: tile counts, tile offsets and the block's
+// cursors (P each), then the sorted rows.
+constexpr int kScatterTile = 4096;
+constexpr int kTiledParts = 4096;
+
+template <bool HAS2>
+__global__ void __launch_bounds__(1024) group_part_scatter_tiled_kernel(
+    PartPlan pp, const int32_t* __restrict__ keys, const int32_t* __restrict__ vals,
+    const int32_t* __restrict__ vals2, const unsigned int* __restrict__ hist, unsigned long long* __restrict__ cursor,
+    typename PartRow<HAS2>::T* __restrict__ rows) {
+  using Row = typename PartRow<HAS2>::T;
+  extern __shared__ __align__(16) unsigned char sc_smem[];
+  Row* s_rows = reinterpret_cast<Row*>(sc_smem);
+  unsigned int* s_cnt = reinterpret_cast<unsigned int*>(s_rows + kScatterTile);
+  unsigned int* s_off = s_cnt + pp.n_parts;
+  unsigned int* s_cur = s_off + pp.n_parts;
+  __shared__ unsigned int s_warp[32];
+  const int P = pp.n_parts;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int p = tid; p < P; p += blockDim.x) {
+    const unsigned int c = hist[static_cast<int64_t>(blockIdx.x) * P + p];
+    s_cur[p] = c ? static_cast<unsigned int>(atomicAdd(&cursor[p], static_cast<unsigned long long>(c))) : 0u;
+  }
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * pp.per;
+  const int64_t e = b + pp.per < pp.n ? b + pp.per : pp.n;
+  const uint64_t pol = policy_evict_first();
+  const bool vec = ((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(vals) |
+                     reinterpret_cast<uintptr_t>(vals2)) & 15) == 0;
+  const int per_thread = (P + blockDim.x - 1) / blockDim.x;  // partitions per thread in the scan
+  for (int64_t t0 = b; t0 < e; t0 += kScatterTile) {
+    for (int p = tid; p < P; p += blockDim.x) s_cnt[p] = 0;
+    __syncthreads();
+    // 1. this thread's 4 rows: key, partition, rank inside the tile
+    const int64_t r0 = t0 + 4 * tid;
+    int32_t k[4], a[4], c[4];
+    unsigned int rank[4];
+    if (vec && r0 + 4 <= e) {
+      const int4 kk = ld_stream_v4(keys + r0, pol), av = ld_stream_v4(vals + r0, pol);
+      const int4 cv = HAS2 ? ld_stream_v4(vals2 + r0, pol) : make_int4(0, 0, 0, 0);
+      k[0] = kk.x; k[1] = kk.y; k[2] = kk.z; k[3] = kk.w;
+      a[0] = av.x; a[1] = av.y; a[2] = av.z; a[3] = av.w;
+      c[0] = cv.x; c[1] = cv.y; c[2] = cv.z; c[3] = cv.w;
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool ok = r0 + u < e;
+        k[u] = ok ? keys[r0 + u] : 0;
+        a[u] = ok ? vals[r0 + u] : 0;
+        c[u] = ok && HAS2 ? vals2[r0 + u] : 0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      k[u] = agg_key(k[u], pp.key_offset);
+      const bool ok = r0 + u < e && k[u] != kEmptyKey;
+      rank[u] = ok ? atomicAdd(&s_cnt[agg_part(k[u], pp.part_shift)], 1u) : ~0u;
+    }
+    __syncthreads();
+    // 2. exclusive scan of the tile counts (each thread a run of partitions)
+    unsigned int run = 0;
+    for (int j = 0; j < per_thread; ++j) {
+      const int p = tid * per_thread + j;
+      if (p < P) run += s_cnt[p];
+    }
+    unsigned int inc = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      unsigned int w = lane < static_cast<int>(blockDim.x >> 5) ? s_warp[lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      s_warp[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    unsigned int off = (warp > 0 ? s_warp[warp - 1] : 0u) + inc - run;
+    const unsigned int n_valid = s_warp[(blockDim.x >> 5) - 1];
+    for (int j = 0; j < per_thread; ++j) {
+      const int p = tid * per_thread + j;
+      if (p < P) {
+        s_off[p] = off;
+        off += s_cnt[p];
+      }
+    }
+    __syncthreads();
+    // 3. rows into their sorted places
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (rank[u] != ~0u) s_rows[s_off[agg_part(k[u], pp.part_shift)] + rank[u]] = PartRow<HAS2>::make(k[u], a[u], c[u]);
+    __syncthreads();
+    // 4. coalesced writes: sorted row i goes to its partition's cursor
+    for (unsigned int i = tid; i < n_valid; i += blockDim.x) {
+      const Row row = s_rows[i];
+      const uint32_t p = agg_part(PartRow<HAS2>::key(row), pp.part_shift);
+      rows[s_cur[p] + (i - s_off[p])] = row;
+    }
+    __syncthreads();
+    for (int p = tid; p < P; p += blockDim.x) s_cur[p] += s_cnt[p];
+    __syncthreads();
+  }
+}
+
+// One block per partition: aggregate in a shared table, then append the
+// groups to the outputs (positions from one global counter per block).
+template <bool HAS2>
+__global__ void __launch_bounds__(kAggThreads) group_part_agg_kernel(
+    const long long* __restrict__ part_begin, const typename PartRow<HAS2>::T* __restrict__ rows, int combine,
+    int64_t capacity, int32_t* __restrict__ out_keys, int64_t* __restrict__ out_sums,
+    int64_t* __restrict__ out_counts, unsigned long long* d_groups, unsigned long long* overflow) {
+  extern __shared__ __align__(16) unsigned char agg_smem[];
+  __shared__ unsigned int s_n;
+  __shared__ unsigned long long s_base;
+  const SmemAgg st = smem_agg(agg_smem, kAggSlots);
+  smem_agg_clear(st);
+  if (threadIdx.x == 0) s_n = 0;
   __syncthreads();
-  for (int i = tid; i < kSmemSlots; i += blockDim.x)
-    if (skey[i] != kEmptyKey) global_add(t, skey[i], ssum[i], scnt[i]);
+  const int64_t b = part_begin[blockIdx.x], e = part_begin[blockIdx.x + 1];
+  unsigned int lost = 0;
+  // rows of the partition, 8 per thread in flight
+  for (int64_t base = b; base < e; base += 8 * static_cast<int64_t>(blockDim.x)) {
+    typename PartRow<HAS2>::T r[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t i = base + u * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+      if (i < e) r[u] = rows[i];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t i = base + u * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+      const bool ok = i < e;
+      const int32_t k = ok ? PartRow<HAS2>::key(r[u]) : 0;
+      int64_t gs = ok ? PartRow<HAS2>::val(r[u]) : 0;
+      uint32_t gc = 1;
+      if (combine ? warp_combine(ok, k, gs, &gs, &gc) : ok)
+        if (!smem_agg_add(st, k, static_cast<uint64_t>(gs), gc)) ++lost;
+    }
+  }
+  if (lost) atomicAdd(overflow, static_cast<unsigned long long>(lost));
+  __syncthreads();
+  constexpr int kPer = kAggSlots / kAggThreads;
+  unsigned int pos[kPer];
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int i = j * kAggThreads + threadIdx.x;
+    pos[j] = st.key[i] != kEmptyKey ? atomicAdd(&s_n, 1u) : ~0u;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) s_base = s_n ? atomicAdd(d_groups, static_cast<unsigned long long>(s_n)) : 0ull;
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    if (pos[j] == ~0u) continue;
+    const int i = j * kAggThreads + threadIdx.x;
+    const unsigned long long o = s_base + pos[j];
+    if (o >= static_cast<unsigned long long>(capacity)) {  // more groups than the outputs hold
+      atomicAdd(overflow, 1ull);
+      continue;
+    }
+    out_keys[o] = st.key[i];
+    out_sums[o] = static_cast<int64_t>(st.sum[i]);
+    if (out_counts) out_counts[o] = static_cast<int64_t>(st.cnt[i]);
+  }
 }
 
 // Compaction of the occupied slots into (key, sum, count) arrays.
@@ -280,6 +754,23 @@ __global__ void agg_f64_final_kernel(const double* __restrict__ partial, int nb,
   }
 }
 
+// The context's grow-only buffer, at least `bytes` long (the caller's stream
+// is synchronised before a smaller buffer is replaced).
+static char* big_scratch(olap_ctx* ctx, size_t bytes) {
+  if (bytes <= ctx->big_bytes) return ctx->big;
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return nullptr;
+  if (ctx->big) cudaFree(ctx->big);
+  ctx->big = nullptr;
+  ctx->big_bytes = 0;
+  const size_t want = bytes + bytes / 4;
+  if (cudaMalloc(reinterpret_cast<void**>(&ctx->big), want) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  ctx->big_bytes = want;
+  return ctx->big;
+}
+
 static unsigned grid_of(const olap_ctx* ctx, int64_t items, int threads, int per_sm) {
   int64_t g = (items + threads - 1) / threads;
   const int64_t cap = static_cast<int64_t>(ctx->sm_count) * per_sm;
@@ -338,30 +829,55 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
   OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   OLAP_REQUIRE(ctx, n >= 0 && capacity >= 1024 && (capacity & (capacity - 1)) == 0,
                "capacity must be a power of two >= 1024 (see olap_group_hash_capacity)");
+  OLAP_REQUIRE(ctx, n < (int64_t(1) << 32), "at most 2^32 - 1 rows per call");
   OLAP_REQUIRE(ctx, out_keys && out_sums && d_groups, "null output");
   OLAP_REQUIRE(ctx, n == 0 || (keys && vals), "null column");
-  // Table from the stream-ordered pool: keys, sums, counts.
-  char* mem = nullptr;
-  const size_t bytes = static_cast<size_t>(capacity) * (4 + 8 + 8);
-  OLAP_CUDA_TRY(ctx, cudaMallocAsync(reinterpret_cast<void**>(&mem), bytes, ctx->stream));
-  olap::HashAgg t;
-  t.sums = reinterpret_cast<unsigned long long*>(mem);
-  t.counts = t.sums + capacity;
-  t.keys = reinterpret_cast<int32_t*>(t.counts + capacity);
-  t.mask = static_cast<uint64_t>(capacity - 1);
   olap::Arena ar(ctx);
-  t.overflow = ar.take<unsigned long long>(1);
+  unsigned long long* overflow = ar.take<unsigned long long>(1);
+  if (!overflow) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(overflow, 0, sizeof(unsigned long long), ctx->stream));
   int st = OLAP_OK;
-  if (!t.overflow) st = olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
-  if (st == OLAP_OK) {
-    cudaMemsetAsync(t.overflow, 0, sizeof(unsigned long long), ctx->stream);
-    cudaMemsetAsync(mem, 0, static_cast<size_t>(capacity) * 16, ctx->stream);
+  char* mem = nullptr;
+  cudaError_t e = cudaSuccess;
+  // Warp combining of equal keys (match_any + reductions) costs more than the
+  // same-address shared atomics it saves on uniform and mildly skewed keys
+  // (measured on B200), so it is off unless the tuning knob asks for it.
+  const int combine = ctx->tune[olap::TUNE_GROUP_COMBINE] == 1 ? 1 : 0;
+  const int64_t plan_knob = ctx->tune[olap::TUNE_GROUP_PLAN];
+  const bool plan1 = plan_knob == 1 ? capacity <= olap::kAggSlots
+                                    : plan_knob == 2 ? false : capacity <= olap::kAggSlots;
+  if (plan1) {
+    // Plan 1: per-block shared tables of `capacity` slots, then the global
+    // table (in the context's grow-only buffer) and its compaction.
+    const size_t bytes = static_cast<size_t>(capacity) * (4 + 8 + 8);
+    mem = olap::big_scratch(ctx, bytes);
+    if (!mem) return olap::set_error(ctx, OLAP_ERR_NOMEM, "device memory for the group table");
+    olap::HashAgg t;
+    t.sums = reinterpret_cast<unsigned long long*>(mem);
+    t.counts = t.sums + capacity;
+    t.keys = reinterpret_cast<int32_t*>(t.counts + capacity);
+    t.mask = static_cast<uint64_t>(capacity - 1);
+    t.overflow = overflow;
+    e = cudaMemsetAsync(mem, 0, static_cast<size_t>(capacity) * 16, ctx->stream);
     olap::fill_i32_kernel<<<olap::grid_of(ctx, capacity, 256, 8), 256, 0, ctx->stream>>>(t.keys, capacity,
                                                                                        olap::kEmptyKey);
-    if (n)
-      olap::group_hash_kernel<<<olap::grid_of(ctx, (n + 3) / 4, olap::kGroupThreads, 2), olap::kGroupThreads,
-                                0, ctx->stream>>>(n, keys, key_offset, vals, vals2, t,
-                                                  &ctx->counters->range_errors);
+    const uint32_t slots = static_cast<uint32_t>(capacity);  // per-block table
+    if (n && e == cudaSuccess) {
+      const size_t smem = static_cast<size_t>(slots) * 16;
+      e = cudaFuncSetAttribute(olap::group_hash_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem));
+      int bps = 1;
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, olap::group_hash_smem_kernel, olap::kAggThreads,
+                                                          smem);
+      int64_t grid = static_cast<int64_t>(ctx->sm_count) * (bps < 1 ? 1 : bps);
+      grid = std::min<int64_t>(grid, (n + 4 * olap::kAggThreads - 1) / (4 * olap::kAggThreads));
+      if (e == cudaSuccess)
+        olap::group_hash_smem_kernel<<<static_cast<unsigned>(grid < 1 ? 1 : grid), olap::kAggThreads, smem,
+                                       ctx->stream>>>(n, keys, key_offset, vals, vals2,
+                                                      slots, combine, t,
+                                                      &ctx->counters->range_errors);
+    }
     olap::SlotOp op;
     std::memset(&op, 0, sizeof(op));
     op.keys = t.keys;
@@ -371,18 +887,103 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
     op.out_sums = out_sums;
     op.out_counts = out_counts;
     olap::ScanTiles sc;
-    st = olap::make_scan_tiles(ctx, ar, capacity, reinterpret_cast<unsigned long long*>(d_groups), ctx->stream,
-                               &sc, olap::compact_tile_items<olap::SlotOp>());
-    if (st == OLAP_OK)
+    if (e == cudaSuccess)
+      st = olap::make_scan_tiles(ctx, ar, capacity, reinterpret_cast<unsigned long long*>(d_groups), ctx->stream,
+                                 &sc, olap::compact_tile_items<olap::SlotOp>());
+    if (e == cudaSuccess && st == OLAP_OK)
       olap::compact_kernel<olap::SlotOp><<<olap::compact_grid(ctx, sc.n_tiles), olap::kCompactThreads, 0,
                                           ctx->stream>>>(op, capacity, sc);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess && st == OLAP_OK) st = olap::check_cuda(ctx, e, "group_hash");
+  } else {
+    // Plan 2: partition, then one block per partition.
+    olap::PartPlan pp;
+    pp.n = n;
+    pp.key_offset = key_offset;
+    int64_t parts = std::max<int64_t>(512, capacity / olap::kAggSlots);
+    int lg = 0;
+    while ((int64_t(1) << lg) < parts) ++lg;
+    if (lg > 15) return olap::set_error(ctx, OLAP_ERR_UNSUPPORTED, "hash group-by capacity above 2^27 slots");
+    pp.n_parts = 1 << lg;
+    pp.part_shift = 32 - lg;
+    pp.n_blocks = ctx->sm_count * 2;
+    pp.per = ((n + pp.n_blocks - 1) / pp.n_blocks + 3) & ~int64_t(3);
+    if (pp.per < 4) pp.per = 4;
+    const size_t hist_bytes = sizeof(unsigned int) * static_cast<size_t>(pp.n_parts) * pp.n_blocks;
+    // part_begin[P + 1], then ptot[P] and cursor[P] (zeroed together)
+    const size_t begin_bytes = sizeof(long long) * (3 * static_cast<size_t>(pp.n_parts) + 1);
+    const size_t row_bytes = vals2 ? 16 : 8;
+    const size_t bytes = hist_bytes + begin_bytes + static_cast<size_t>(n > 0 ? n : 1) * row_bytes + 256;
+    mem = olap::big_scratch(ctx, bytes);
+    if (!mem) return olap::set_error(ctx, OLAP_ERR_NOMEM, "device memory for the group partitions");
+    long long* part_begin = reinterpret_cast<long long*>(mem);
+    auto* ptot = reinterpret_cast<unsigned long long*>(part_begin + pp.n_parts + 1);
+    auto* cursor = ptot + pp.n_parts;
+    unsigned int* hist = reinterpret_cast<unsigned int*>(mem + begin_bytes);
+    char* rowbuf = mem + ((begin_bytes + hist_bytes + 255) & ~size_t(255));
+    e = cudaMemsetAsync(d_groups, 0, sizeof(int64_t), ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ptot, 0, sizeof(unsigned long long) * pp.n_parts, ctx->stream);
+    const size_t psmem = sizeof(unsigned int) * pp.n_parts;
+    if (e == cudaSuccess && psmem > 48 * 1024) {
+      e = cudaFuncSetAttribute(olap::group_part_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(psmem));
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(olap::group_part_scatter_kernel<true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(psmem));
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(olap::group_part_scatter_kernel<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(psmem));
+    }
+    const size_t asmem = static_cast<size_t>(olap::kAggSlots) * 16;
+    if (pp.n_parts <= olap::kTiledParts) {
+      const int tsm = static_cast<int>((vals2 ? 16 : 8) * olap::kScatterTile + 3 * psmem);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(olap::group_part_scatter_tiled_kernel<true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(olap::group_part_scatter_tiled_kernel<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
+    }
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(olap::group_part_agg_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(asmem));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(olap::group_part_agg_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(asmem));
+    if (e == cudaSuccess) {
+      olap::group_part_hist_kernel<<<pp.n_blocks, 1024, psmem, ctx->stream>>>(pp, keys, hist, ptot,
+                                                                              &ctx->counters->range_errors);
+      olap::group_part_scan_kernel<<<1, 1024, 0, ctx->stream>>>(pp, ptot, part_begin, cursor);
+      auto* d_groups_u = reinterpret_cast<unsigned long long*>(d_groups);
+      const bool tiled = pp.n_parts <= olap::kTiledParts;
+      const size_t tsmem = (vals2 ? 16 : 8) * static_cast<size_t>(olap::kScatterTile) + 3 * psmem;
+      if (vals2) {
+        auto* rows = reinterpret_cast<longlong2*>(rowbuf);
+        if (tiled)
+          olap::group_part_scatter_tiled_kernel<true><<<pp.n_blocks, 1024, tsmem, ctx->stream>>>(
+              pp, keys, vals, vals2, hist, cursor, rows);
+        else
+          olap::group_part_scatter_kernel<true><<<pp.n_blocks, 1024, psmem, ctx->stream>>>(pp, keys, vals, vals2,
+                                                                                          hist, cursor, rows);
+        olap::group_part_agg_kernel<true><<<pp.n_parts, olap::kAggThreads, asmem, ctx->stream>>>(
+            part_begin, rows, combine, capacity, out_keys, out_sums, out_counts, d_groups_u, overflow);
+      } else {
+        auto* rows = reinterpret_cast<int2*>(rowbuf);
+        if (tiled)
+          olap::group_part_scatter_tiled_kernel<false><<<pp.n_blocks, 1024, tsmem, ctx->stream>>>(
+              pp, keys, vals, nullptr, hist, cursor, rows);
+        else
+          olap::group_part_scatter_kernel<false><<<pp.n_blocks, 1024, psmem, ctx->stream>>>(pp, keys, vals,
+                                                                                           nullptr, hist, cursor,
+                                                                                           rows);
+        olap::group_part_agg_kernel<false><<<pp.n_parts, olap::kAggThreads, asmem, ctx->stream>>>(
+            part_begin, rows, combine, capacity, out_keys, out_sums, out_counts, d_groups_u, overflow);
+      }
+      e = cudaGetLastError();
+    }
   }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess && st == OLAP_OK) st = olap::check_cuda(ctx, e, "group_hash");
   unsigned long long ov = 0;
-  if (st == OLAP_OK && t.overflow)
-    cudaMemcpyAsync(&ov, t.overflow, sizeof(ov), cudaMemcpyDeviceToHost, ctx->stream);
-  cudaFreeAsync(mem, ctx->stream);
+  if (st == OLAP_OK) cudaMemcpyAsync(&ov, overflow, sizeof(ov), cudaMemcpyDeviceToHost, ctx->stream);
   OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (st == OLAP_OK && ov) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "group hash table full");
   if (st == OLAP_OK) st = olap::check_timeouts(ctx, ctx->stream);

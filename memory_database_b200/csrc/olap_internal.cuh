@@ -43,6 +43,11 @@ struct olap_ctx {
   size_t arena_bytes = 0;
   olap::DeviceCounters* counters = nullptr;  // first bytes of the arena
 
+  // Grow-only device buffer for the large temporaries of synchronous calls
+  // (hash group-by tables and partitions); kept between calls.
+  char* big = nullptr;
+  size_t big_bytes = 0;
+
   // Pinned host staging used by the host-memory entry points.
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -66,6 +71,8 @@ enum {
   TUNE_UNROLL = OLAP_TUNE_UNROLL,
   TUNE_PROBE_BITS = OLAP_TUNE_PROBE_BITS,
   TUNE_SMEM_BITS_BYTES = OLAP_TUNE_SMEM_BITS_BYTES,
+  TUNE_GROUP_COMBINE = OLAP_TUNE_GROUP_COMBINE,
+  TUNE_GROUP_PLAN = OLAP_TUNE_GROUP_PLAN,
 };
 
 int set_error(olap_ctx* ctx, int status, const std::string& msg);

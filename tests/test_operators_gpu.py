@@ -260,3 +260,53 @@ def test_starjoin_operator(ctx):
     live = np.nonzero(eres != 32767)[0]
     assert np.array_equal(np.intersect1d(host(pos), live), live)
     assert np.array_equal(host(grp)[np.isin(host(pos), live)], eres[live])
+
+
+def _group_expect(keys, vals, vals2):
+    v = vals.astype(np.int64) + (vals2.astype(np.int64) if vals2 is not None else 0)
+    uk, inv = np.unique(keys, return_inverse=True)
+    sums = np.zeros(len(uk), np.int64)
+    np.add.at(sums, inv, v)
+    return uk, sums, np.bincount(inv, minlength=len(uk))
+
+
+@pytest.mark.parametrize("dist,G,n,two", [
+    ("zipf", 300, 2_000_001, True),        # shared-table plan, skewed
+    ("uniform", 5000, 1_000_003, True),    # partitioned plan, few groups per partition
+    ("zipf", 1 << 16, 3_000_001, False),   # partitioned plan, skewed
+    ("wide", 1 << 18, 2_000_003, True),    # partitioned plan, keys over the whole int32 range
+])
+def test_group_hash_plans(ctx, dist, G, n, two):
+    rng = np.random.default_rng(G + n)
+    if dist == "uniform":
+        keys = rng.integers(0, G, n).astype(np.int32)
+    elif dist == "zipf":
+        keys = (rng.zipf(1.2, n) % G).astype(np.int32)
+    else:
+        pool = rng.integers(-2**31 + 1, 2**31, G, dtype=np.int64).astype(np.int32)
+        pool[:3] = [2**31 - 1, -2**31 + 1, 0]
+        keys = pool[rng.integers(0, G, n)]
+    vals = rng.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32)  # extremes of the value split
+    vals2 = rng.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32) if two else None
+    ek, es, ec = _group_expect(keys, vals, vals2)
+    for combine, plan in ((2, 0), (1, 0), (2, 2)):  # combining off (default) / on; forced partitioned plan
+        ctx.set_tuning(_lib.TUNE_GROUP_COMBINE, combine)
+        ctx.set_tuning(_lib.TUNE_GROUP_PLAN, plan)
+        k, s, c = ops.group_hash(dev(keys), dev(vals), dev(vals2) if two else None, max_groups=G, ctx=ctx)
+        order = np.argsort(host(k))
+        assert np.array_equal(host(k)[order], ek)
+        assert np.array_equal(host(s)[order], es) and np.array_equal(host(c)[order], ec)
+    ctx.set_tuning(_lib.TUNE_GROUP_COMBINE, 0)
+    ctx.set_tuning(_lib.TUNE_GROUP_PLAN, 0)
+    # a key equal to the empty marker after the offset is dropped and counted
+    off = ((-2**31 - int(keys[0])) + 2**31) % 2**32 - 2**31  # wraps keys[0] onto INT32_MIN
+    ops.group_hash(dev(keys[:1000]), dev(vals[:1000]), key_offset=off, max_groups=G, ctx=ctx)
+    assert ctx.take_range_errors() == int((keys[:1000] == keys[0]).sum())
+
+
+@pytest.mark.parametrize("max_groups,distinct", [(100, 5000), (5000, 40000)])
+def test_group_hash_more_keys_than_capacity_fails(ctx, max_groups, distinct):
+    keys = np.arange(distinct, dtype=np.int32)
+    vals = np.ones(distinct, np.int32)
+    with pytest.raises(_lib.OlapError):
+        ops.group_hash(dev(keys), dev(vals), max_groups=max_groups, ctx=ctx)

@@ -263,6 +263,11 @@ OLAP_API int olap_plan_olapcore(const double sele[4], const int bitmap[4], const
 OLAP_API int olap_select_rowids(olap_ctx* ctx, const int32_t* col, int64_t col_len, int32_t val,
                                 int cmp, const int32_t* in_rowids, int64_t n_in,
                                 int32_t* out_rowids, int64_t* d_count);
+/* Failure path of the bounded device waits (no counterpart in the
+ * reference): one look-back that waits for a tile status nothing publishes
+ * gives up after spin_limit polls and the call returns OLAP_ERR_TIMEOUT; the
+ * context stays usable.  For tests of the error handling. */
+OLAP_API int olap_debug_wait_timeout(olap_ctx* ctx, uint32_t spin_limit);
 /* Bitmap of cmp(col[r], val): sel_lt_T_bmp_independent_val_{branching,
  * non_branching} (select:206-228, 424-440); (n + 31) / 32 words written. */
 OLAP_API int olap_select_bitmap(olap_ctx* ctx, const int32_t* col, int64_t n, int32_t val, int cmp,

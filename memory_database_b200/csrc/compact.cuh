@@ -58,7 +58,8 @@ __device__ __forceinline__ int64_t claim_tile(const ScanTiles& st, unsigned int*
 
 // Exclusive prefix of this tile's count over all earlier tiles; run by one
 // full warp (warp 0).  Returns -1 on timeout.
-__device__ __forceinline__ int64_t lookback(const ScanTiles& st, int64_t tile, uint64_t count) {
+__device__ __forceinline__ int64_t lookback(const ScanTiles& st, int64_t tile, uint64_t count,
+                                           uint32_t spin_limit = kSpinLimit) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) {
     if (lane == 0) st_relaxed_u64(&st.status[0], kFlagInc | count);
@@ -72,7 +73,7 @@ __device__ __forceinline__ int64_t lookback(const ScanTiles& st, int64_t tile, u
     const int64_t idx = t - lane;
     uint64_t w = idx >= 0 ? ld_relaxed_u64(&st.status[idx]) : kFlagInc;
     while (__any_sync(0xffffffffu, (w >> 62) == 0)) {
-      if (++spins > kSpinLimit) {
+      if (++spins > spin_limit) {
         if (lane == 0) atomicAdd(st.timeouts, 1ull);
         return -1;
       }

@@ -253,6 +253,13 @@ static int run_compaction(olap_ctx* ctx, const Op& op, int64_t n_items, int64_t*
   return OLAP_OK;
 }
 
+// Look-back of tile 1 while tile 0's status is never published: the wait
+// runs out after spin_limit polls (the failure path of every compaction).
+__global__ void lookback_timeout_kernel(ScanTiles st, uint32_t spin_limit, long long* out) {
+  const int64_t b = lookback(st, 1, 1, spin_limit);
+  if (threadIdx.x == 0) *out = b;
+}
+
 static unsigned stream_grid(const olap_ctx* ctx, int64_t items, int threads) {
   int64_t g = (items + threads - 1) / threads;
   const int64_t cap = static_cast<int64_t>(ctx->sm_count) * (2048 / threads);
@@ -293,6 +300,22 @@ int olap_select_rowids(olap_ctx* ctx, const int32_t* col, int64_t col_len, int32
   olap::SelectOp<false> op;
   fill(op);
   return olap::run_compaction(ctx, op, n, d_count);
+}
+
+int olap_debug_wait_timeout(olap_ctx* ctx, uint32_t spin_limit) {
+  if (!ctx || spin_limit < 1) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  olap::Arena ar(ctx);
+  olap::ScanTiles st;
+  unsigned long long* total = ar.take<unsigned long long>(1);
+  long long* out = ar.take<long long>(1);
+  if (!total || !out) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
+  int rc = olap::make_scan_tiles(ctx, ar, 2, total, ctx->stream, &st, 1);  // two one-item tiles
+  if (rc != OLAP_OK) return rc;
+  olap::lookback_timeout_kernel<<<1, 32, 0, ctx->stream>>>(st, spin_limit, out);
+  OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  return olap::check_timeouts(ctx, ctx->stream);
 }
 
 int olap_select_bitmap(olap_ctx* ctx, const int32_t* col, int64_t n, int32_t val, int cmp,

@@ -310,3 +310,11 @@ def test_group_hash_more_keys_than_capacity_fails(ctx, max_groups, distinct):
     vals = np.ones(distinct, np.int32)
     with pytest.raises(_lib.OlapError):
         ops.group_hash(dev(keys), dev(vals), max_groups=max_groups, ctx=ctx)
+
+
+def test_bounded_device_wait_reports_timeout_and_context_survives(ctx):
+    # a look-back waiting for a tile status that nothing publishes gives up
+    st = _lib.lib.olap_debug_wait_timeout(ctx.handle, 1 << 14)
+    assert st == _lib.OLAP_ERR_TIMEOUT
+    col = np.arange(100_000, dtype=np.int32)
+    assert np.array_equal(host(ops.select_rowids(dev(col), 99, ctx=ctx)), np.arange(100, dtype=np.int32))

@@ -508,7 +508,7 @@ def main() -> None:
     # Plan choice for this query shape: the library's autotuner times its
     # candidate plans on a 64Mi-row sample of this rank's table (untimed).
     if a.tune:
-        knobs = [0] * 8
+        knobs = [0] * 16
         for kv in filter(None, a.tune.split(",")):
             k, v = kv.split("=")
             knobs[int(k)] = int(v)
@@ -517,7 +517,7 @@ def main() -> None:
                                      dimvec_lens=s.probe_lens, ctx=ctx)
     plan = {name: knobs[k] for k, name in enumerate(
         ["block_threads", "blocks_per_sm", "smem_dim_bytes", "smem_acc_bytes", "host_chunk_rows",
-         "rows_per_thread_mode", "probe_bits", "smem_bits_bytes"]) if knobs[k]}
+         "rows_per_thread_mode", "probe_bits", "smem_bits_bytes", "group_combine", "group_plan"]) if knobs[k]}
 
     def step():
         olapcore.starjoin_groupsum(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,

@@ -145,7 +145,7 @@ OLAP_API int olap_starjoin_groupsum_host(olap_ctx* ctx, const olap_starjoin_quer
  * thread counts are fixed by the caller): times candidate plans on rows
  * [row_begin, row_begin + sample_rows) of q (device pointers; 0 = 64Mi rows),
  * sets the fastest candidate's OLAP_TUNE_* knobs on the context and returns
- * them in knobs_out[8] (may be NULL) and its time in *best_ms (may be NULL).
+ * them in knobs_out[16] (may be NULL) and its time in *best_ms (may be NULL).
  * Synchronous; the query's outputs are not written. */
 OLAP_API int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q,
                                     int64_t sample_rows, int64_t* knobs_out, double* best_ms);

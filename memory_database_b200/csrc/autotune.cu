@@ -18,7 +18,7 @@ namespace olap {
 namespace {
 
 struct Candidate {
-  int64_t knob[8];  // indexed by OLAP_TUNE_*; 0 = automatic
+  int64_t knob[16];  // indexed by OLAP_TUNE_*; 0 = automatic
 };
 
 std::vector<Candidate> candidates(const olap_ctx* ctx, const olap_starjoin_query* q) {
@@ -64,7 +64,7 @@ extern "C" {
 
 // Times the candidate plans on rows [row_begin, row_begin + sample_rows) of
 // the query (device pointers), sets the fastest candidate's knobs on the
-// context and returns them in knobs_out[0..7] (may be NULL) with its time
+// context and returns them in knobs_out[0..15] (may be NULL) with its time
 // per sample in *best_ms (may be NULL).  Results of the timed runs are
 // discarded; the query's own outputs are not touched.
 int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q, int64_t sample_rows,
@@ -99,11 +99,11 @@ int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q, int64_t 
   OLAP_CUDA_TRY(ctx, cudaEventCreate(&e0));
   OLAP_CUDA_TRY(ctx, cudaEventCreate(&e1));
   double best = 1e30;
-  int64_t best_knob[8] = {0};
+  int64_t best_knob[16] = {0};
   int st = OLAP_OK;
   for (const auto& cand : olap::candidates(ctx, q)) {
     std::memcpy(ctx->tune, saved, sizeof(saved));
-    for (int k = 0; k < 8; ++k) if (cand.knob[k]) ctx->tune[k] = cand.knob[k];
+    for (int k = 0; k < 16; ++k) if (cand.knob[k]) ctx->tune[k] = cand.knob[k];
     float ms = 0.f, tot_ms = 1e30f;
     bool ok = true;
     for (int rep = 0; rep < 4 && ok; ++rep) {
@@ -128,7 +128,7 @@ int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q, int64_t 
   cudaEventDestroy(e1);
   std::memcpy(ctx->tune, saved, sizeof(saved));
   if (best >= 1e29) return olap::set_error(ctx, OLAP_ERR_CUDA, "no autotune candidate ran");
-  for (int k = 0; k < 8; ++k)
+  for (int k = 0; k < 16; ++k)
     if (best_knob[k]) ctx->tune[k] = best_knob[k];
   // Rows dropped in the timed runs were counted; the caller's query will
   // count them again, so restore the count from before the tuner ran.

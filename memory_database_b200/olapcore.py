@@ -225,13 +225,13 @@ def autotune(dimvecs: Sequence, fks: Sequence, factors: Sequence[int], m1, m2, g
     """Pick the launch plan of this query shape on a sample of its own data.
 
     Leaves the chosen ``TUNE_*`` knobs set on ``ctx`` and returns
-    ``(knobs[8], best_ms_per_sample)``."""
+    ``(knobs[16], best_ms_per_sample)``."""
     ctx = ctx or default_context()
     first = fks[0] if len(fks) else (m1 if m1 is not None else m2)
     n_rows = _nelem(first) if first is not None else 0
     q = _build_query(dimvecs, fks, factors, m1, m2, group_nums, aggs, 0, n_rows, dimvec_lens)
     ctx.follow_torch_stream()
-    knobs = (C.c_int64 * 8)()
+    knobs = (C.c_int64 * 16)()
     ms = C.c_double()
     check(lib.olap_starjoin_autotune(ctx.handle, C.byref(q), int(sample_rows), knobs, C.byref(ms)),
           ctx.handle)

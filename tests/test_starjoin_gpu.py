@@ -163,6 +163,7 @@ def test_dimvec_len_pads_like_reference(ctx):
     {_lib.TUNE_SMEM_BITS_BYTES: 200 * 1024},              # bitmaps staged in smem
     {_lib.TUNE_SMEM_BITS_BYTES: 8 * 1024, _lib.TUNE_PROBE_BITS: 1, _lib.TUNE_BLOCK_THREADS: 1024},
     {_lib.TUNE_SMEM_BITS_BYTES: 200 * 1024, _lib.TUNE_SMEM_DIM_BYTES: 1, _lib.TUNE_UNROLL: 2},
+    {_lib.TUNE_BLOCK_THREADS: 768},
 ])
 def test_tuning_knobs_do_not_change_results(ctx, knobs):
     sizes, groups, sele = [30000, 2000, 20000, 2556], [5, 25, 4, 7], [0.3, 0.5, 0.7, 0.9]
@@ -270,8 +271,8 @@ def test_autotuned_plan_gives_same_results(ctx):
         knobs, ms = olapcore.autotune([dev(d) for d in dvs], [dev(f) for f in fks], factor, dev(m1),
                                       dev(m2), G, aggs=(AGG_M1, AGG_M1_TIMES_M2),
                                       sample_rows=1_000_000, ctx=ctx)
-        assert ms > 0 and len(knobs) == 8
+        assert ms > 0 and len(knobs) == 16
         check_same(ctx, dvs, fks, factor, m1, m2, G, (AGG_M1, AGG_M1_TIMES_M2))
     finally:
-        for k in range(8):
+        for k in range(16):
             ctx.set_tuning(k, 0)

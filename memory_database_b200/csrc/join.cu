@@ -77,10 +77,8 @@ __global__ void hash_finish_kernel(uint64_t* __restrict__ slots, int64_t cap, co
 // Probe: SUM of matched payloads and the match count; optionally the matches
 // (probe row, payload) compacted in probe-row order by the caller's second
 // pass (see ProbeOp).
-__device__ __forceinline__ bool hash_lookup(const uint64_t* __restrict__ slots, uint64_t mask, int32_t k,
-                                            int32_t* payload) {
-  uint64_t h = hash32(static_cast<uint32_t>(k)) & mask;
-  const uint32_t uk = static_cast<uint32_t>(k);
+__device__ __forceinline__ bool hash_lookup_from(const uint64_t* __restrict__ slots, uint64_t mask, uint64_t h,
+                                                 uint32_t uk, int32_t* payload) {
   for (uint64_t step = 0; step <= mask; step += 4) {
     // the 4-slot bucket holding h (one 32-byte sector), starting at h
     const uint64_t b = h & ~3ull;
@@ -101,6 +99,59 @@ __device__ __forceinline__ bool hash_lookup(const uint64_t* __restrict__ slots, 
   return false;
 }
 
+__device__ __forceinline__ bool hash_lookup(const uint64_t* __restrict__ slots, uint64_t mask, int32_t k,
+                                            int32_t* payload) {
+  return hash_lookup_from(slots, mask, hash32(static_cast<uint32_t>(k)) & mask, static_cast<uint32_t>(k), payload);
+}
+
+// Four lookups with their first buckets read together (8 x 16-byte loads in
+// flight) before any is resolved; a key whose run continues past its first
+// bucket (rare at load <= 1/2) falls back to hash_lookup from the next one.
+// Returns the 4-bit mask of matches; pay[j] holds the matched payloads.
+__device__ __forceinline__ uint32_t hash_lookup4(const uint64_t* __restrict__ slots, uint64_t mask, const int4 k4,
+                                                 int32_t pay[4]) {
+  const int32_t k[4] = {k4.x, k4.y, k4.z, k4.w};
+  uint64_t h[4];
+  ulonglong2 lo[4], hi[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    h[j] = hash32(static_cast<uint32_t>(k[j])) & mask;
+    const uint64_t b = h[j] & ~3ull;
+    lo[j] = __ldg(reinterpret_cast<const ulonglong2*>(slots + b));
+    hi[j] = __ldg(reinterpret_cast<const ulonglong2*>(slots + b + 2));
+  }
+  uint32_t found = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const uint64_t s[4] = {lo[j].x, lo[j].y, hi[j].x, hi[j].y};
+    const uint32_t uk = static_cast<uint32_t>(k[j]);
+    int state = 0;  // 0 go on, 1 found, 2 absent
+    pay[j] = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (state != 0 || q < static_cast<int>(h[j] & 3)) continue;
+      if (s[q] == kEmptySlot) {
+        state = 2;
+      } else if ((s[q] >> 32) == uk) {
+        pay[j] = static_cast<int32_t>(static_cast<uint32_t>(s[q]));
+        state = 1;
+      }
+    }
+    if (state == 0) {
+      int32_t p = 0;
+      const uint64_t next = ((h[j] & ~3ull) + 4) & mask;
+      // continue the run from the next bucket: a key whose home slot is
+      // `next` has the same probe sequence from there on
+      if (hash_lookup_from(slots, mask, next, uk, &p)) {
+        pay[j] = p;
+        state = 1;
+      }
+    }
+    if (state == 1) found |= 1u << j;
+  }
+  return found;
+}
+
 __global__ void __launch_bounds__(512) hash_probe_sum_kernel(const int32_t* __restrict__ keys, int64_t n,
                                                              const uint64_t* __restrict__ slots, uint64_t mask,
                                                              int vec, unsigned long long* sum,
@@ -113,11 +164,10 @@ __global__ void __launch_bounds__(512) hash_probe_sum_kernel(const int32_t* __re
   const int64_t n4 = vec ? n >> 2 : 0;
   for (int64_t i = tid; i < n4; i += stride) {
     const int4 k = ld_stream_v4(keys + 4 * i, pol);
-    int32_t p0 = 0, p1 = 0, p2 = 0, p3 = 0;
-    const bool f0 = hash_lookup(slots, mask, k.x, &p0), f1 = hash_lookup(slots, mask, k.y, &p1);
-    const bool f2 = hash_lookup(slots, mask, k.z, &p2), f3 = hash_lookup(slots, mask, k.w, &p3);
-    s += (f0 ? p0 : 0) + static_cast<int64_t>(f1 ? p1 : 0) + (f2 ? p2 : 0) + static_cast<int64_t>(f3 ? p3 : 0);
-    c += f0 + f1 + f2 + f3;
+    int32_t p[4];
+    const uint32_t f = hash_lookup4(slots, mask, k, p);
+    s += static_cast<int64_t>(p[0]) + p[1] + static_cast<int64_t>(p[2]) + p[3];  // 0 where absent
+    c += __popc(f);
   }
   for (int64_t r = 4 * n4 + tid; r < n; r += stride) {
     int32_t p = 0;
@@ -174,9 +224,13 @@ struct ProbeOp {
     }
     int32_t p[4] = {0, 0, 0, 0};
     uint32_t m = 0;
+    if (nv == 4) {
+      m = hash_lookup4(slots, mask, make_int4(k[0], k[1], k[2], k[3]), p);
+    } else {
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-      if (j < nv && hash_lookup(slots, mask, k[j], &p[j])) m |= 1u << j;
+      for (int j = 0; j < 4; ++j)
+        if (j < nv && hash_lookup(slots, mask, k[j], &p[j])) m |= 1u << j;
+    }
     pay[u] = make_int4(p[0], p[1], p[2], p[3]);
     return m;
   }

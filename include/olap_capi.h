@@ -72,6 +72,8 @@ extern "C" {
 #define OLAP_TUNE_SMEM_BITS_BYTES 7 /* bytes of pass bitmaps staged in smem (default 0)          */
 #define OLAP_TUNE_GROUP_COMBINE 8   /* hash group-by warp combining of equal keys: 1 on, 2 off (default) */
 #define OLAP_TUNE_GROUP_PLAN 9      /* hash group-by: 1 per-block tables (capacity <= 8192), 2 partitioned */
+#define OLAP_TUNE_ASYNC_LOADS 10    /* star-join: 2 prefetches fact columns by bulk async copies (TMA), 1 off */
+#define OLAP_TUNE_COMPACT 11        /* star-join: 2 compacts survivors per warp before global probes, 1 off */
 
 typedef struct olap_ctx olap_ctx;
 
@@ -86,6 +88,8 @@ OLAP_API int olap_ctx_destroy(olap_ctx* ctx);
  * default stream.  The context's own stream is released on the first call. */
 OLAP_API int olap_ctx_set_stream(olap_ctx* ctx, void* cuda_stream);
 OLAP_API void* olap_ctx_get_stream(olap_ctx* ctx);
+/* Waits for the context stream; OLAP_ERR_TIMEOUT when a bounded device wait
+ * of an earlier call gave up (olap_ctx_take_range_errors reports it too). */
 OLAP_API int olap_ctx_synchronize(olap_ctx* ctx);
 OLAP_API int olap_ctx_set_tuning(olap_ctx* ctx, int knob, int64_t value);
 /* Synchronises, returns and clears the count of rows that kernels dropped

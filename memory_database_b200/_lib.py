@@ -45,6 +45,8 @@ TUNE_PROBE_BITS = 6
 TUNE_SMEM_BITS_BYTES = 7
 TUNE_GROUP_COMBINE = 8
 TUNE_GROUP_PLAN = 9
+TUNE_ASYNC_LOADS = 10
+TUNE_COMPACT = 11
 
 
 class OlapError(RuntimeError):

@@ -45,8 +45,18 @@ std::vector<Candidate> candidates(const olap_ctx* ctx, const olap_starjoin_query
     add({{OLAP_TUNE_PROBE_BITS, 1}, {OLAP_TUNE_SMEM_BITS_BYTES, budget}, {OLAP_TUNE_SMEM_ACC_BYTES, 1},
          {OLAP_TUNE_BLOCK_THREADS, 1024}});
   }
-  // Every plan also with 8 rows per thread (512-thread blocks).
+  // Every plan also with the survivors of the shared-memory probes compacted
+  // per warp, with the fact columns prefetched by bulk copies, and with 8
+  // rows per thread (512-thread blocks).
   const size_t n4 = c.size();
+  for (size_t i = 0; i < n4; ++i) {
+    Candidate x = c[i];
+    x.knob[OLAP_TUNE_COMPACT] = 2;
+    c.push_back(x);
+    x.knob[OLAP_TUNE_COMPACT] = 0;
+    x.knob[OLAP_TUNE_ASYNC_LOADS] = 2;  // bulk-copy prefetch of the fact columns
+    c.push_back(x);
+  }
   for (size_t i = 0; i < n4; ++i) {
     Candidate x = c[i];
     x.knob[OLAP_TUNE_UNROLL] = 2;
@@ -93,7 +103,7 @@ int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q, int64_t 
   std::memcpy(saved, ctx->tune, sizeof(saved));
   for (int k : {OLAP_TUNE_BLOCK_THREADS, OLAP_TUNE_BLOCKS_PER_SM, OLAP_TUNE_SMEM_DIM_BYTES,
                 OLAP_TUNE_SMEM_ACC_BYTES, OLAP_TUNE_UNROLL, OLAP_TUNE_PROBE_BITS,
-                OLAP_TUNE_SMEM_BITS_BYTES})
+                OLAP_TUNE_SMEM_BITS_BYTES, OLAP_TUNE_ASYNC_LOADS, OLAP_TUNE_COMPACT})
     saved[k] = 0;
   cudaEvent_t e0, e1;
   OLAP_CUDA_TRY(ctx, cudaEventCreate(&e0));

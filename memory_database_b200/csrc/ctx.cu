@@ -3,7 +3,7 @@
 #include <cstring>
 #include <new>
 
-#include "olap_internal.cuh"
+#include "compact.cuh"
 
 namespace olap {
 
@@ -125,7 +125,7 @@ int olap_ctx_synchronize(olap_ctx* ctx) {
   if (!ctx) return OLAP_ERR_INVALID;
   cudaSetDevice(ctx->device);
   OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  return OLAP_OK;
+  return olap::check_timeouts(ctx, ctx->stream);
 }
 
 int olap_ctx_set_tuning(olap_ctx* ctx, int knob, int64_t value) {
@@ -145,7 +145,8 @@ int olap_ctx_take_range_errors(olap_ctx* ctx, int64_t* count) {
   OLAP_CUDA_TRY(ctx, cudaMemsetAsync(&ctx->counters->range_errors, 0, sizeof(v), ctx->stream));
   OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   *count = static_cast<int64_t>(v);
-  return OLAP_OK;
+  // A bounded device wait that gave up (asynchronous calls record it here).
+  return olap::check_timeouts(ctx, ctx->stream);
 }
 
 const char* olap_ctx_last_error(const olap_ctx* ctx) {

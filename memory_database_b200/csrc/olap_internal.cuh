@@ -73,6 +73,8 @@ enum {
   TUNE_SMEM_BITS_BYTES = OLAP_TUNE_SMEM_BITS_BYTES,
   TUNE_GROUP_COMBINE = OLAP_TUNE_GROUP_COMBINE,
   TUNE_GROUP_PLAN = OLAP_TUNE_GROUP_PLAN,
+  TUNE_ASYNC_LOADS = OLAP_TUNE_ASYNC_LOADS,
+  TUNE_COMPACT = OLAP_TUNE_COMPACT,
 };
 
 int set_error(olap_ctx* ctx, int status, const std::string& msg);
@@ -189,6 +191,46 @@ __device__ __forceinline__ void smem_add_u64(unsigned long long* slot, uint64_t 
   uint32_t old = atomicAdd(w, lo);
   hi += (old + lo) < old ? 1u : 0u;
   if (hi) atomicAdd(w + 1, hi);
+}
+
+// ---- bulk asynchronous copies (TMA, untiled) and mbarriers ----------------
+// cp.async.bulk global -> shared: both addresses and the size 16-byte
+// aligned; completion is counted in bytes on an mbarrier of this CTA.  No
+// multicast form is used anywhere in this library.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// Non-blocking test of the phase with parity `parity`.
+__device__ __forceinline__ bool mbar_test(unsigned long long* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Generic-proxy accesses of shared memory before later async-proxy ones.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, unsigned long long* bar,
+                                              uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+      ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
+      : "memory");
 }
 
 __device__ __forceinline__ int64_t warp_sum_i64(int64_t v) {

@@ -58,6 +58,9 @@ struct StarParams {
   int32_t n_aggs, agg0, agg1;
   int32_t smem_dim_bytes;      // staged dimension bytes and bitmaps (multiple of 16)
   int32_t need_m1, need_m2;
+  int32_t pf_off, bar_off;     // ASYNC: per-warp prefetch buffers and mbarriers (shared-memory offsets)
+  int32_t cmp_off;             // CMP: per-warp survivor buffers (shared-memory offset)
+  unsigned long long* wait_timeouts;
 };
 
 enum { ACC_NONE = 0, ACC_SMEM = 1, ACC_GLOBAL = 2 };
@@ -181,7 +184,18 @@ __device__ __forceinline__ void finish_block(const StarParams& p, int64_t tot0, 
 // codes of bitmap-filtered dimensions for survivors, and accumulates.  Group
 // ids are int32: the host selects this kernel only when sum_j 128*|factor_j|
 // fits in int32, so every intermediate is exact.
-template <int ND, int ACC, int AGGK, int V>
+// ASYNC: each warp's next 32 x 16-byte vectors of every streamed column are
+// brought into shared memory by bulk asynchronous copies (one lane issues
+// them, an mbarrier counts the bytes) while the warp probes the current
+// ones, so the DRAM latency overlaps the dependent dimension probes instead
+// of adding to them; registers hold only the current vectors.
+constexpr uint32_t kAsyncWaitLimit = 1u << 24;  // polls of a prefetch barrier before giving up
+
+// CMP: after the shared-memory dimensions, each warp packs its surviving
+// rows (keys, partial group id, measures) densely into a shared buffer and
+// runs the global probes, group-code fetches and accumulation over them with
+// every lane busy, instead of once per row slot with most lanes idle.
+template <int ND, int ACC, int AGGK, int V, bool ASYNC, bool CMP>
 __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(const StarParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long red[32][2];
@@ -196,6 +210,18 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
   if (tid < OLAP_MAX_DIMS)
     s_code_nz[tid] = (tid < ND && p.dim[tid].code_flag >= 0) ? p.code_nonzero[p.dim[tid].code_flag] : 0;
   stage_block<ND, ACC>(p, sdim, sacc, nacc);
+  const int lane = tid & 31;
+  constexpr int NCOL = (ND > 0 ? ND : 1) + 2;
+  int4* pf = nullptr;
+  unsigned long long* bar = nullptr;
+  if (ASYNC) {
+    pf = reinterpret_cast<int4*>(smem + p.pf_off) + (tid >> 5) * (NG * NCOL * 32);
+    bar = reinterpret_cast<unsigned long long*>(smem + p.bar_off) + (tid >> 5);
+    if (lane == 0) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+    }
+  }
   __syncthreads();
   bool need_code[OLAP_MAX_DIMS];
 #pragma unroll
@@ -217,23 +243,91 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
 
   const uint32_t nvec = static_cast<uint32_t>((p.vec_end - p.vec_begin) >> 2);
   const uint32_t gstride = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + tid; i < nvec; i += NG * gstride) {
+  const uint32_t wstride = NG * gstride;
+  // ASYNC (lane 0): bulk copies of the warp's vectors w0 .. w0+31 (+ u*gstride)
+  // of every streamed column into its prefetch buffer.
+  auto issue = [&](uint32_t w0) {
+    uint32_t cnt[NG];
+    uint32_t bytes = 0;
+    const uint32_t ncols = ND + (need_m1 ? 1 : 0) + (need_m2 ? 1 : 0);
+#pragma unroll
+    for (int u = 0; u < NG; ++u) {
+      const uint32_t b = w0 + u * gstride;
+      cnt[u] = b < nvec ? min(32u, nvec - b) : 0u;
+      bytes += cnt[u] * 16u * ncols;
+    }
+    if (bytes == 0) return;
+    mbar_arrive_expect_tx(bar, bytes);
+#pragma unroll
+    for (int u = 0; u < NG; ++u) {
+      if (cnt[u] == 0) continue;
+      const uint32_t b = w0 + u * gstride;
+#pragma unroll
+      for (int j = 0; j < ND; ++j) bulk_copy_g2s(pf + (u * NCOL + j) * 32, fkb[j] + 4ull * b, cnt[u] * 16u, bar, pol_stream);
+      if (need_m1) bulk_copy_g2s(pf + (u * NCOL + ND) * 32, m1b + 4ull * b, cnt[u] * 16u, bar, pol_stream);
+      if (need_m2) bulk_copy_g2s(pf + (u * NCOL + ND + 1) * 32, m2b + 4ull * b, cnt[u] * 16u, bar, pol_stream);
+    }
+  };
+  uint32_t w0 = blockIdx.x * blockDim.x + (tid & ~31u);  // the warp's first vector of this step
+  uint32_t phase = 0;
+  if (ASYNC && lane == 0 && w0 < nvec) issue(w0);
+  // ASYNC and CMP use warp-wide operations in the loop, so a warp runs its
+  // steps together while any of its lanes has rows (w0 is warp-uniform).
+  for (uint32_t i = blockIdx.x * blockDim.x + tid; (ASYNC || CMP) ? w0 < nvec : i < nvec;
+       i += wstride, w0 += wstride) {
     int4 kf[NG][ND > 0 ? ND : 1];
     int4 ka[NG], kb[NG];
     uint32_t alive = 0;
+    if (ASYNC) {
+      // this step's vectors (issued one step earlier); bounded wait
+      bool ok = false;
+      for (uint32_t t = 0; t < kAsyncWaitLimit; ++t) {
+        if (mbar_test(bar, phase)) {
+          ok = true;
+          break;
+        }
+        __nanosleep(32);
+      }
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) atomicAdd(p.wait_timeouts, 1ull);
+        break;
+      }
+      phase ^= 1u;
 #pragma unroll
-    for (int u = 0; u < NG; ++u) {
-      const uint32_t gi = i + u * gstride;
-      if (u == 0 || gi < nvec) {
-        alive |= 0xFu << (4 * u);
+      for (int u = 0; u < NG; ++u) {
+        const uint32_t gi = i + u * gstride;
+        if (gi < nvec) {
+          alive |= 0xFu << (4 * u);
 #pragma unroll
-        for (int j = 0; j < ND; ++j) kf[u][j] = ld_stream_v4(fkb[j] + 4ull * gi, pol_stream);
-        ka[u] = need_m1 ? ld_stream_v4(m1b + 4ull * gi, pol_stream) : make_int4(0, 0, 0, 0);
-        kb[u] = need_m2 ? ld_stream_v4(m2b + 4ull * gi, pol_stream) : make_int4(0, 0, 0, 0);
-      } else {
+          for (int j = 0; j < ND; ++j) kf[u][j] = pf[(u * NCOL + j) * 32 + lane];
+          ka[u] = need_m1 ? pf[(u * NCOL + ND) * 32 + lane] : make_int4(0, 0, 0, 0);
+          kb[u] = need_m2 ? pf[(u * NCOL + ND + 1) * 32 + lane] : make_int4(0, 0, 0, 0);
+        } else {
 #pragma unroll
-        for (int j = 0; j < ND; ++j) kf[u][j] = make_int4(0, 0, 0, 0);
-        ka[u] = kb[u] = make_int4(0, 0, 0, 0);
+          for (int j = 0; j < ND; ++j) kf[u][j] = make_int4(0, 0, 0, 0);
+          ka[u] = kb[u] = make_int4(0, 0, 0, 0);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        fence_proxy_async_smem();  // the reads above before the buffer is refilled
+        if (w0 + wstride < nvec) issue(w0 + wstride);
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < NG; ++u) {
+        const uint32_t gi = i + u * gstride;
+        if ((u == 0 && !CMP) || gi < nvec) {
+          alive |= 0xFu << (4 * u);
+#pragma unroll
+          for (int j = 0; j < ND; ++j) kf[u][j] = ld_stream_v4(fkb[j] + 4ull * gi, pol_stream);
+          ka[u] = need_m1 ? ld_stream_v4(m1b + 4ull * gi, pol_stream) : make_int4(0, 0, 0, 0);
+          kb[u] = need_m2 ? ld_stream_v4(m2b + 4ull * gi, pol_stream) : make_int4(0, 0, 0, 0);
+        } else {
+#pragma unroll
+          for (int j = 0; j < ND; ++j) kf[u][j] = make_int4(0, 0, 0, 0);
+          ka[u] = kb[u] = make_int4(0, 0, 0, 0);
+        }
       }
     }
     auto key = [&](int r, int j) -> uint32_t {
@@ -264,6 +358,7 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
     for (int j = 0; j < ND; ++j) {
       if (alive == 0) break;
       const Probe& d = p.dim[j];
+      if (CMP && d.soff < 0 && d.boff < 0) continue;  // global dimensions: after the compaction
       if (d.soff >= 0) {
         const int8_t* sv = reinterpret_cast<const int8_t*>(sdim + d.soff);
 #pragma unroll
@@ -300,28 +395,12 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
         }
       }
     }
-    if (alive == 0) continue;
-#pragma unroll
-    for (int j = 0; j < ND; ++j) {
-      const Probe& d = p.dim[j];
-      if (d.soff < 0 && d.bits && need_code[j]) {
-        int32_t c[V];
-#pragma unroll
-        for (int r = 0; r < V; ++r)
-          c[r] = (alive & (1u << r)) ? ld_probe_s8(d.vec + key(r, j), pol_keep) : 0;
-#pragma unroll
-        for (int r = 0; r < V; ++r) g[r] += c[r] * d.factor;
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < V; ++r) {
-      if (!(alive & (1u << r))) continue;
-      const uint32_t gg = static_cast<uint32_t>(g[r]);
+    // One surviving row: group id check, aggregates, accumulate.
+    auto add_row = [&](uint32_t gg, int32_t x, int32_t y) {
       if (gg >= n_groups) {
         ++bad;
-        continue;
+        return;
       }
-      const int32_t x = mx(ka, r), y = mx(kb, r);
       int64_t v0, v1 = 0;
       if (AGGK == AGGK_M1PM2) {
         v0 = static_cast<int64_t>(x) + y;
@@ -340,7 +419,86 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
         if (ACC == ACC_SMEM) smem_add_u64(&sacc[n_groups + gg], static_cast<uint64_t>(v1));
         if (ACC == ACC_GLOBAL) atomicAdd(&p.out[n_groups + gg], static_cast<unsigned long long>(v1));
       }
+    };
+    if (CMP) {
+      // pack the warp's survivors: row (slot r, lane l) goes to position
+      // (survivors of slots < r) + (survivors of slot r in lanes < l)
+      constexpr int ROWS = 32 * V;  // rows of a warp step
+      uint32_t* sb = reinterpret_cast<uint32_t*>(smem + p.cmp_off) + (tid >> 5) * ((ND + 3) * ROWS);
+      const uint32_t lt = (1u << lane) - 1u;
+      uint32_t tot = 0;
+#pragma unroll
+      for (int r = 0; r < V; ++r) {
+        const uint32_t b = __ballot_sync(0xffffffffu, (alive >> r) & 1u);
+        if ((alive >> r) & 1u) {
+          const uint32_t at = tot + __popc(b & lt);
+#pragma unroll
+          for (int j = 0; j < ND; ++j) sb[j * ROWS + at] = key(r, j);
+          sb[ND * ROWS + at] = static_cast<uint32_t>(g[r]);
+          sb[(ND + 1) * ROWS + at] = static_cast<uint32_t>(mx(ka, r));
+          sb[(ND + 2) * ROWS + at] = static_cast<uint32_t>(mx(kb, r));
+        }
+        tot += __popc(b);
+      }
+      if (tot == 0) continue;
+      __syncwarp();
+      for (uint32_t base = 0; base < tot; base += 32) {
+        const uint32_t at = base + lane;
+        bool live = at < tot;
+        uint32_t k[ND > 0 ? ND : 1];
+        int32_t gg = 0, x = 0, y = 0;
+        if (live) {
+#pragma unroll
+          for (int j = 0; j < ND; ++j) k[j] = sb[j * ROWS + at];
+          gg = static_cast<int32_t>(sb[ND * ROWS + at]);
+          x = static_cast<int32_t>(sb[(ND + 1) * ROWS + at]);
+          y = static_cast<int32_t>(sb[(ND + 2) * ROWS + at]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < ND; ++j) k[j] = 0;
+        }
+#pragma unroll
+        for (int j = 0; j < ND; ++j) {
+          const Probe& d = p.dim[j];
+          if (d.soff >= 0 || d.boff >= 0) continue;
+          if (d.bits) {
+            const uint32_t w = live ? __ldg(d.bits + (k[j] >> 5)) : 0u;
+            if (!((w >> (k[j] & 31)) & 1u)) live = false;
+          } else {
+            const int32_t c = live ? ld_probe_s8(d.vec + k[j], pol_keep) : OLAP_DIM_NULL;
+            if (c == OLAP_DIM_NULL) live = false;
+            gg += c * d.factor;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < ND; ++j) {
+          const Probe& d = p.dim[j];
+          if (d.soff < 0 && d.bits && need_code[j]) {
+            const int32_t c = live ? ld_probe_s8(d.vec + k[j], pol_keep) : 0;
+            gg += c * d.factor;
+          }
+        }
+        if (live) add_row(static_cast<uint32_t>(gg), x, y);
+      }
+      __syncwarp();  // the buffer is rewritten in the next step
+      continue;
     }
+    if (alive == 0) continue;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      const Probe& d = p.dim[j];
+      if (d.soff < 0 && d.bits && need_code[j]) {
+        int32_t c[V];
+#pragma unroll
+        for (int r = 0; r < V; ++r)
+          c[r] = (alive & (1u << r)) ? ld_probe_s8(d.vec + key(r, j), pol_keep) : 0;
+#pragma unroll
+        for (int r = 0; r < V; ++r) g[r] += c[r] * d.factor;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < V; ++r)
+      if (alive & (1u << r)) add_row(static_cast<uint32_t>(g[r]), mx(ka, r), mx(kb, r));
   }
   // Head and tail rows outside the 16-byte aligned range (block 0).
   if (blockIdx.x == 0) {
@@ -465,38 +623,54 @@ __global__ void __launch_bounds__(1024, 1) starjoin_scalar_kernel(const StarPara
 
 using StarKernel = void (*)(const StarParams);
 
-template <int ND, int ACC>
-static StarKernel pick_vec(int aggk, int v) {
+template <int ND, int ACC, bool ASYNC>
+static StarKernel pick_vec_a(int aggk, int v) {
   if (v >= 8) {
     switch (aggk) {
-      case AGGK_M1PM2: return starjoin_vec_kernel<ND, ACC, AGGK_M1PM2, 8>;
-      case AGGK_M1_M1M2: return starjoin_vec_kernel<ND, ACC, AGGK_M1_M1M2, 8>;
-      default: return starjoin_vec_kernel<ND, ACC, AGGK_GENERIC, 8>;
+      case AGGK_M1PM2: return starjoin_vec_kernel<ND, ACC, AGGK_M1PM2, 8, ASYNC, false>;
+      case AGGK_M1_M1M2: return starjoin_vec_kernel<ND, ACC, AGGK_M1_M1M2, 8, ASYNC, false>;
+      default: return starjoin_vec_kernel<ND, ACC, AGGK_GENERIC, 8, ASYNC, false>;
     }
   }
   switch (aggk) {
-    case AGGK_M1PM2: return starjoin_vec_kernel<ND, ACC, AGGK_M1PM2, 4>;
-    case AGGK_M1_M1M2: return starjoin_vec_kernel<ND, ACC, AGGK_M1_M1M2, 4>;
-    default: return starjoin_vec_kernel<ND, ACC, AGGK_GENERIC, 4>;
+    case AGGK_M1PM2: return starjoin_vec_kernel<ND, ACC, AGGK_M1PM2, 4, ASYNC, false>;
+    case AGGK_M1_M1M2: return starjoin_vec_kernel<ND, ACC, AGGK_M1_M1M2, 4, ASYNC, false>;
+    default: return starjoin_vec_kernel<ND, ACC, AGGK_GENERIC, 4, ASYNC, false>;
   }
+}
+
+// Compaction: 4 rows per thread, loads straight to registers.
+template <int ND, int ACC>
+static StarKernel pick_vec_cmp(int aggk) {
+  switch (aggk) {
+    case AGGK_M1PM2: return starjoin_vec_kernel<ND, ACC, AGGK_M1PM2, 4, false, true>;
+    case AGGK_M1_M1M2: return starjoin_vec_kernel<ND, ACC, AGGK_M1_M1M2, 4, false, true>;
+    default: return starjoin_vec_kernel<ND, ACC, AGGK_GENERIC, 4, false, true>;
+  }
+}
+
+template <int ND, int ACC>
+static StarKernel pick_vec(int aggk, int v, bool async, bool cmp) {
+  if (cmp && ND >= 1) return pick_vec_cmp<ND, ACC>(aggk);
+  return async ? pick_vec_a<ND, ACC, true>(aggk, v) : pick_vec_a<ND, ACC, false>(aggk, v);
 }
 
 template <int ND>
-static StarKernel pick_kernel(int acc, bool vec, int aggk, int v) {
+static StarKernel pick_kernel(int acc, bool vec, int aggk, int v, bool async, bool cmp) {
   switch (acc) {
-    case ACC_NONE: return vec ? pick_vec<ND, ACC_NONE>(aggk, v) : starjoin_scalar_kernel<ND, ACC_NONE>;
-    case ACC_SMEM: return vec ? pick_vec<ND, ACC_SMEM>(aggk, v) : starjoin_scalar_kernel<ND, ACC_SMEM>;
-    default: return vec ? pick_vec<ND, ACC_GLOBAL>(aggk, v) : starjoin_scalar_kernel<ND, ACC_GLOBAL>;
+    case ACC_NONE: return vec ? pick_vec<ND, ACC_NONE>(aggk, v, async, cmp) : starjoin_scalar_kernel<ND, ACC_NONE>;
+    case ACC_SMEM: return vec ? pick_vec<ND, ACC_SMEM>(aggk, v, async, cmp) : starjoin_scalar_kernel<ND, ACC_SMEM>;
+    default: return vec ? pick_vec<ND, ACC_GLOBAL>(aggk, v, async, cmp) : starjoin_scalar_kernel<ND, ACC_GLOBAL>;
   }
 }
 
-static StarKernel select_kernel(int nd, int acc, bool vec, int aggk, int v) {
+static StarKernel select_kernel(int nd, int acc, bool vec, int aggk, int v, bool async, bool cmp) {
   switch (nd) {
-    case 0: return pick_kernel<0>(acc, vec, aggk, v);
-    case 1: return pick_kernel<1>(acc, vec, aggk, v);
-    case 2: return pick_kernel<2>(acc, vec, aggk, v);
-    case 3: return pick_kernel<3>(acc, vec, aggk, v);
-    default: return pick_kernel<4>(acc, vec, aggk, v);
+    case 0: return pick_kernel<0>(acc, vec, aggk, v, async, cmp);
+    case 1: return pick_kernel<1>(acc, vec, aggk, v, async, cmp);
+    case 2: return pick_kernel<2>(acc, vec, aggk, v, async, cmp);
+    case 3: return pick_kernel<3>(acc, vec, aggk, v, async, cmp);
+    default: return pick_kernel<4>(acc, vec, aggk, v, async, cmp);
   }
 }
 
@@ -510,6 +684,8 @@ struct StarPlan {
   bool vec = false;
   int aggk = 0;    // AGGK_* of the 128-bit path
   int rows_v = 4;  // rows per thread per iteration (4 or 8)
+  bool async = false;  // bulk-copy prefetch of the streamed columns (TUNE_ASYNC_LOADS)
+  bool cmp = false;    // warp compaction of the survivors of the shared-memory probes (TUNE_COMPACT)
   int block = 512;
   size_t smem = 0;
   int nbits = 0;                       // dims whose pass bitmap must be built
@@ -681,6 +857,34 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   else if (acc_bytes <= smem_acc_budget && soff + acc_bytes <= smem_cap) acc = ACC_SMEM;
   pl->acc = acc;
   pl->smem = static_cast<size_t>(soff + (acc == ACC_SMEM ? acc_bytes : 0));
+  // Bulk-copy prefetch: per warp, 32 vectors of each streamed column for each
+  // group of 4 rows per thread, and one mbarrier; only when it fits.
+  sp->wait_timeouts = &ctx->counters->wait_timeouts;
+  pl->async = false;
+  if (vec && tune_or(ctx, TUNE_ASYNC_LOADS, 1) == 2 && nd + (need_m1 ? 1 : 0) + (need_m2 ? 1 : 0) > 0) {
+    const int64_t warps = pl->block / 32;
+    const int64_t pf_bytes = warps * (pl->rows_v / 4) * (std::max(nd, 1) + 2) * 32 * 16;
+    const int64_t pf_off = (static_cast<int64_t>(pl->smem) + 127) & ~int64_t(127);
+    const int64_t bar_off = pf_off + pf_bytes;
+    const int64_t end = bar_off + warps * 8;
+    if (end <= smem_cap) {
+      pl->async = true;
+      sp->pf_off = static_cast<int32_t>(pf_off);
+      sp->bar_off = static_cast<int32_t>(bar_off);
+      pl->smem = static_cast<size_t>(end);
+    }
+  }
+  // Survivor compaction (4 rows per thread): per warp (ND + 3) x 128 words.
+  pl->cmp = false;
+  if (vec && !pl->async && pl->rows_v == 4 && nd >= 1 && tune_or(ctx, TUNE_COMPACT, 1) == 2) {
+    const int64_t cmp_off = (static_cast<int64_t>(pl->smem) + 127) & ~int64_t(127);
+    const int64_t end = cmp_off + (pl->block / 32) * (nd + 3) * 128 * 4;
+    if (end <= smem_cap) {
+      pl->cmp = true;
+      sp->cmp_off = static_cast<int32_t>(cmp_off);
+      pl->smem = static_cast<size_t>(end);
+    }
+  }
   return OLAP_OK;
 }
 
@@ -697,7 +901,7 @@ int launch_starjoin(olap_ctx* ctx, StarPlan& pl, cudaStream_t stream) {
       OLAP_CUDA_TRY(ctx, cudaGetLastError());
     }
   }
-  StarKernel k = select_kernel(pl.nd, pl.acc, pl.vec, pl.aggk, pl.rows_v);
+  StarKernel k = select_kernel(pl.nd, pl.acc, pl.vec, pl.aggk, pl.rows_v, pl.async, pl.cmp);
   if (pl.smem > 48 * 1024)
     OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             static_cast<int>(pl.smem)));

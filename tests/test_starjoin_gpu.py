@@ -104,6 +104,29 @@ def test_fewer_dimensions(ctx, nd):
 
 @pytest.mark.parametrize("n", [0, 1, 2, 3, 4, 5, 7, 8, 9, 1023, 1024, 1025, 4097])
 def test_ragged_sizes(ctx, n):
+    _ragged(ctx, n)
+
+
+@pytest.mark.parametrize("n", [0, 1, 3, 4, 5, 127, 128, 129, 131, 4095, 4097, 1_000_003])
+def test_ragged_sizes_with_bulk_copy_prefetch(ctx, n):
+    ctx.set_tuning(_lib.TUNE_ASYNC_LOADS, 2)
+    try:
+        _ragged(ctx, n)
+        ctx.synchronize()  # raises if a prefetch wait gave up
+    finally:
+        ctx.set_tuning(_lib.TUNE_ASYNC_LOADS, 0)
+
+
+@pytest.mark.parametrize("n", [1, 5, 129, 4097, 1_000_003])
+def test_ragged_sizes_with_survivor_compaction(ctx, n):
+    ctx.set_tuning(_lib.TUNE_COMPACT, 2)
+    try:
+        _ragged(ctx, n)
+    finally:
+        ctx.set_tuning(_lib.TUNE_COMPACT, 0)
+
+
+def _ragged(ctx, n):
     sizes, groups, sele = [300, 20, 700, 25], [3, 4, 5, 6], [0.7, 0.9, 0.8, 1.0]
     dv, fk, m1, m2 = random_star(n + 1, max(n, 1), sizes, sele, groups)
     fk = [f[:n] for f in fk]
@@ -164,6 +187,15 @@ def test_dimvec_len_pads_like_reference(ctx):
     {_lib.TUNE_SMEM_BITS_BYTES: 8 * 1024, _lib.TUNE_PROBE_BITS: 1, _lib.TUNE_BLOCK_THREADS: 1024},
     {_lib.TUNE_SMEM_BITS_BYTES: 200 * 1024, _lib.TUNE_SMEM_DIM_BYTES: 1, _lib.TUNE_UNROLL: 2},
     {_lib.TUNE_BLOCK_THREADS: 768},
+    {_lib.TUNE_ASYNC_LOADS: 2},                           # bulk-copy prefetch of the fact columns
+    {_lib.TUNE_ASYNC_LOADS: 2, _lib.TUNE_UNROLL: 2},
+    {_lib.TUNE_ASYNC_LOADS: 2, _lib.TUNE_SMEM_BITS_BYTES: 64 * 1024, _lib.TUNE_BLOCK_THREADS: 1024},
+    {_lib.TUNE_ASYNC_LOADS: 2, _lib.TUNE_BLOCK_THREADS: 128, _lib.TUNE_BLOCKS_PER_SM: 3},
+    {_lib.TUNE_ASYNC_LOADS: 2, _lib.TUNE_SMEM_ACC_BYTES: 1, _lib.TUNE_PROBE_BITS: 1},
+    {_lib.TUNE_COMPACT: 2},                               # per-warp survivor compaction
+    {_lib.TUNE_COMPACT: 2, _lib.TUNE_SMEM_BITS_BYTES: 64 * 1024, _lib.TUNE_BLOCK_THREADS: 1024},
+    {_lib.TUNE_COMPACT: 2, _lib.TUNE_PROBE_BITS: 1, _lib.TUNE_SMEM_ACC_BYTES: 1},
+    {_lib.TUNE_COMPACT: 2, _lib.TUNE_SMEM_DIM_BYTES: 1, _lib.TUNE_BLOCK_THREADS: 128, _lib.TUNE_BLOCKS_PER_SM: 3},
 ])
 def test_tuning_knobs_do_not_change_results(ctx, knobs):
     sizes, groups, sele = [30000, 2000, 20000, 2556], [5, 25, 4, 7], [0.3, 0.5, 0.7, 0.9]
@@ -252,7 +284,9 @@ def test_bitmap_plans_with_nonzero_codes_and_drops(ctx):
     m1 = rng.integers(1, 10000, n).astype(np.int32)
     m2 = rng.integers(1, 10000, n).astype(np.int32)
     for knobs in ({}, {_lib.TUNE_PROBE_BITS: 1}, {_lib.TUNE_SMEM_BITS_BYTES: 220 * 1024},
-                  {_lib.TUNE_SMEM_BITS_BYTES: 2 * 1024, _lib.TUNE_PROBE_BITS: 1}):
+                  {_lib.TUNE_SMEM_BITS_BYTES: 2 * 1024, _lib.TUNE_PROBE_BITS: 1},
+                  {_lib.TUNE_COMPACT: 2, _lib.TUNE_SMEM_BITS_BYTES: 2 * 1024},
+                  {_lib.TUNE_COMPACT: 2, _lib.TUNE_PROBE_BITS: 1}):
         try:
             for k, v in knobs.items():
                 ctx.set_tuning(k, v)

@@ -482,6 +482,7 @@ def main() -> None:
     import torch
     import torch.distributed as dist
     from memory_database_b200 import _lib, olapcore, workloads
+    from memory_database_b200.distributed import reduce_group_sums
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -498,8 +499,9 @@ def main() -> None:
         k, v = kv.split("=")
         ctx.set_tuning(int(k), int(v))
 
+    # dimension vectors replicated on every rank, fact rows a shard per rank
     s = workloads.make_star_schema(ctx, a.rows, DIM_SIZES, a.sele, a.groups, fk_dist=a.fk_dist,
-                                   seed=42 + rank)
+                                   seed=42, fact_seed=42 + 1000 * rank)
     aggs = (olapcore.AGG_M1, olapcore.AGG_M1_TIMES_M2)
     G = s.group_nums
     gs = torch.empty((2, G), dtype=torch.int64, device="cuda")
@@ -523,7 +525,7 @@ def main() -> None:
         olapcore.starjoin_groupsum(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,
                                    dimvec_lens=s.probe_lens, ctx=ctx, out=gs, totals_out=tot)
         if world > 1:
-            dist.all_reduce(gs)
+            reduce_group_sums(gs)
 
     for _ in range(max(3, a.warmup)):
         step()

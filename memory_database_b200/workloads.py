@@ -69,12 +69,15 @@ class StarSchema:
 
 def make_star_schema(ctx: Context, n_rows: int, dim_sizes, sele, groups, bitmap=(1, 1, 1, 1),
                      m_range=(1, 10_000), fk_dist="uniform", zipf_s=0.8, seed: int = 42,
-                     device: str = "cuda") -> StarSchema:
-    """Generate the star schema on ``device`` (torch tensors, HBM-resident)."""
+                     device: str = "cuda", fact_seed: int | None = None) -> StarSchema:
+    """Generate the star schema on ``device`` (torch tensors, HBM-resident).
+    ``fact_seed`` (default ``seed``) seeds the fact columns alone, so that the
+    shards of several ranks share the dimension vectors."""
     import torch
     L = _lib.lib
     h = ctx.handle
     s = StarSchema(n_rows, tuple(dim_sizes), tuple(sele), tuple(groups), tuple(bitmap))
+    fseed = seed if fact_seed is None else fact_seed
     for t in range(4):
         d = torch.empty(dim_sizes[t], dtype=torch.int8, device=device)
         g = max(1, int(groups[t])) if bitmap[t] else 1
@@ -83,16 +86,16 @@ def make_star_schema(ctx: Context, n_rows: int, dim_sizes, sele, groups, bitmap=
         s.dimvec.append(d)
         f = torch.empty(n_rows, dtype=torch.int32, device=device)
         if fk_dist == "zipf":
-            _lib.check(L.olap_gen_zipf_i32_dev(h, f.data_ptr(), n_rows, seed, 10 + t,
+            _lib.check(L.olap_gen_zipf_i32_dev(h, f.data_ptr(), n_rows, fseed, 10 + t,
                                                dim_sizes[t], float(zipf_s)), h)
         else:
-            _lib.check(L.olap_gen_uniform_i32_dev(h, f.data_ptr(), n_rows, seed, 10 + t, 0,
+            _lib.check(L.olap_gen_uniform_i32_dev(h, f.data_ptr(), n_rows, fseed, 10 + t, 0,
                                                   dim_sizes[t] - 1), h)
         s.fk.append(f)
     s.m1 = torch.empty(n_rows, dtype=torch.int32, device=device)
     s.m2 = torch.empty(n_rows, dtype=torch.int32, device=device)
-    _lib.check(L.olap_gen_uniform_i32_dev(h, s.m1.data_ptr(), n_rows, seed, 20, m_range[0], m_range[1]), h)
-    _lib.check(L.olap_gen_uniform_i32_dev(h, s.m2.data_ptr(), n_rows, seed, 21, m_range[0], m_range[1]), h)
+    _lib.check(L.olap_gen_uniform_i32_dev(h, s.m1.data_ptr(), n_rows, fseed, 20, m_range[0], m_range[1]), h)
+    _lib.check(L.olap_gen_uniform_i32_dev(h, s.m2.data_ptr(), n_rows, fseed, 21, m_range[0], m_range[1]), h)
     ctx.synchronize()
     s.orders, s.factor, s.dimvec_nums, s.group_nums = plan_olapcore(sele, bitmap, groups)
     return s

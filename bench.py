@@ -547,7 +547,7 @@ def main() -> None:
                                        totals_out=tot)
             ev[k][1].record()
             if world > 1:
-                dist.all_reduce(gs)
+                reduce_group_sums(gs)
         t1.record()
         torch.cuda.synchronize()
         if world > 1:

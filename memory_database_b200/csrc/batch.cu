@@ -176,27 +176,14 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
   __shared__ BatchQuery sq[kMaxBatchQueries];
   __shared__ int64_t sseg[kMaxSegments];
   __shared__ unsigned long long smask[kMaxSegments];
-  __shared__ unsigned long long suses[OLAP_MAX_DIMS];
   __shared__ unsigned long long sacc[kBatchSmemSlots];
+  __shared__ int4 s_qf[kMaxBatchQueries];  // per query: group factor at each probe position (0: not grouped)
+  __shared__ int4 s_qi[kMaxBatchQueries];  // per query: {group_nums, smem_off, out_offset lo, hi}
   __shared__ unsigned int s_bad;
   const BatchDesc& D = *p.desc;
   unsigned long long* const out = D.out;
   const int tid = threadIdx.x;
   const int nq = D.n_queries, nseg = D.n_seg;
-  for (int i = tid; i < nq; i += blockDim.x) sq[i] = D.q[i];
-  for (int i = tid; i < kBatchSmemSlots; i += blockDim.x) sacc[i] = 0ull;
-  for (int i = tid; i < nseg; i += blockDim.x) {
-    sseg[i] = D.seg_begin[i];
-    smask[i] = D.seg_mask[i];
-  }
-  if (tid < OLAP_MAX_DIMS) suses[tid] = D.uses_mask[tid];
-  if (tid == 0) s_bad = 0;
-  __syncthreads();
-  const uint64_t pol_stream = policy_evict_first();
-  const uint64_t pol_keep = policy_evict_last();
-  const int agg = p.agg;
-  const bool need_m1 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M1 || agg == OLAP_AGG_M1_TIMES_M2;
-  const bool need_m2 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M2 || agg == OLAP_AGG_M1_TIMES_M2;
   // The used tables in probe order (smallest first).
   int tab[OLAP_MAX_DIMS] = {0, 0, 0, 0};
   uint32_t tlen[OLAP_MAX_DIMS] = {0, 0, 0, 0};
@@ -211,11 +198,34 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
         if (w == ntab) {
           tab[w] = t;
           tlen[w] = p.dim_len[t];
-          tuses[w] = suses[t];
+          tuses[w] = D.uses_mask[t];
         }
       ++ntab;
     }
   }
+  for (int i = tid; i < nq; i += blockDim.x) {
+    const BatchQuery& Q = D.q[i];
+    sq[i] = Q;
+    int32_t f[OLAP_MAX_DIMS] = {0, 0, 0, 0};
+#pragma unroll
+    for (int o = 0; o < OLAP_MAX_DIMS; ++o)
+      if (o < ntab && ((Q.grouped >> tab[o]) & 1)) f[o] = Q.factor[tab[o]];
+    s_qf[i] = make_int4(f[0], f[1], f[2], f[3]);
+    s_qi[i] = make_int4(static_cast<int32_t>(Q.group_nums), Q.smem_off, static_cast<int32_t>(Q.out_offset),
+                        static_cast<int32_t>(Q.out_offset >> 32));
+  }
+  for (int i = tid; i < kBatchSmemSlots; i += blockDim.x) sacc[i] = 0ull;
+  for (int i = tid; i < nseg; i += blockDim.x) {
+    sseg[i] = D.seg_begin[i];
+    smask[i] = D.seg_mask[i];
+  }
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  const uint64_t pol_stream = policy_evict_first();
+  const uint64_t pol_keep = policy_evict_last();
+  const int agg = p.agg;
+  const bool need_m1 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M1 || agg == OLAP_AGG_M1_TIMES_M2;
+  const bool need_m2 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M2 || agg == OLAP_AGG_M1_TIMES_M2;
   unsigned int bad = 0;
   const int64_t n4 = (p.n_rows + 3) >> 2;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -282,7 +292,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
     }
     // Probe the tables, smallest first, breadth-first across the 4 rows; a
     // table is probed for a row only while a live query of the row uses it.
-    int32_t gr[OLAP_MAX_DIMS][4];
+    int32_t gr[OLAP_MAX_DIMS][4] = {};
 #pragma unroll
     for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
       if (o >= ntab) continue;
@@ -307,17 +317,21 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
       while (mk) {
         const int q = __ffsll(static_cast<long long>(mk)) - 1;
         mk &= mk - 1;
-        const BatchQuery& Q = sq[q];
-        int32_t g = 0;
-#pragma unroll
-        for (int o = 0; o < OLAP_MAX_DIMS; ++o)
-          if (o < ntab && ((Q.grouped >> tab[o]) & 1)) g += gr[o][k] * Q.factor[tab[o]];
-        if (static_cast<uint64_t>(static_cast<int64_t>(g)) >= static_cast<uint64_t>(Q.group_nums)) {
+        // two 16-byte shared reads per emission: the query's factors by probe
+        // position (0 for tables it does not group by) and its placement
+        const int4 f = s_qf[q];
+        const int4 qi = s_qi[q];
+        const int32_t g = gr[0][k] * f.x + gr[1][k] * f.y + gr[2][k] * f.z + gr[3][k] * f.w;
+        if (static_cast<uint32_t>(g) >= static_cast<uint32_t>(qi.x)) {
           ++bad;
           continue;
         }
-        if (Q.smem_off >= 0) smem_add_u64(&sacc[Q.smem_off + g], static_cast<uint64_t>(v));
-        else atomicAdd(&out[Q.out_offset + g], static_cast<unsigned long long>(v));
+        if (qi.y >= 0) {
+          smem_add_u64(&sacc[qi.y + g], static_cast<uint64_t>(v));
+        } else {
+          const int64_t base = (static_cast<int64_t>(qi.w) << 32) | static_cast<uint32_t>(qi.z);
+          atomicAdd(&out[base + g], static_cast<unsigned long long>(v));
+        }
       }
     }
   }
@@ -335,7 +349,6 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
   if (tid == 0 && s_bad) atomicAdd(p.range_err, static_cast<unsigned long long>(s_bad));
 }
 
-// totals[q] = sum of query q's group vector (one block per query).
 // Zero the batch's outputs (their location and size come with the descriptor,
 // so a recorded graph serves any output buffer and query count).
 __global__ void batch_zero_kernel(const BatchParams p) {
@@ -346,7 +359,8 @@ __global__ void batch_zero_kernel(const BatchParams p) {
   for (int64_t i = t0; i < D.n_queries; i += stride) D.totals[i] = 0ull;
 }
 
-// Launched with max_queries blocks; blocks past the batch's count return.
+// totals[q] = sum of query q's group vector (one block per query).  Launched
+// with max_queries blocks; blocks past the batch's count return.
 __global__ void batch_totals_kernel(const BatchParams p) {
   __shared__ long long red[32];
   const BatchDesc& D = *p.desc;

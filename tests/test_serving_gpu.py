@@ -41,7 +41,7 @@ def _alone(ctx, tables, r):
     return Q5.q5(ctx, q5d, *r.query).cpu().numpy()
 
 
-@pytest.mark.parametrize("rate,pool_bytes,plain_below", [(3000.0, 64 << 20, 1), (800.0, 512 << 10, 0)])
+@pytest.mark.parametrize("rate,pool_bytes,plain_below", [(3000.0, 64 << 20, 3), (800.0, 512 << 10, 0)])
 def test_mixed_requests_equal_queries_alone(ctx, tables, rate, pool_bytes, plain_below):
     dims, fk, m1, m2, n, q5d = tables
     rng = np.random.default_rng(int(rate))

@@ -519,7 +519,8 @@ def main() -> None:
                                      dimvec_lens=s.probe_lens, ctx=ctx)
     plan = {name: knobs[k] for k, name in enumerate(
         ["block_threads", "blocks_per_sm", "smem_dim_bytes", "smem_acc_bytes", "host_chunk_rows",
-         "rows_per_thread_mode", "probe_bits", "smem_bits_bytes", "group_combine", "group_plan", "async_loads", "compact"]) if knobs[k]}
+         "rows_per_thread_mode", "probe_bits", "smem_bits_bytes", "group_combine", "group_plan", "async_loads", "compact",
+         "smem_nib_bytes"]) if knobs[k]}
 
     def step():
         olapcore.starjoin_groupsum(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,

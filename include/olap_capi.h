@@ -74,6 +74,7 @@ extern "C" {
 #define OLAP_TUNE_GROUP_PLAN 9      /* hash group-by: 1 per-block tables (capacity <= 8192), 2 partitioned */
 #define OLAP_TUNE_ASYNC_LOADS 10    /* star-join: 2 prefetches fact columns by bulk async copies (TMA), 1 off */
 #define OLAP_TUNE_COMPACT 11        /* star-join: 2 compacts survivors per warp before global probes, 1 off */
+#define OLAP_TUNE_SMEM_NIB_BYTES 12 /* bytes of 4-bit code vectors staged in smem (default 0)        */
 
 typedef struct olap_ctx olap_ctx;
 

@@ -47,6 +47,7 @@ TUNE_GROUP_COMBINE = 8
 TUNE_GROUP_PLAN = 9
 TUNE_ASYNC_LOADS = 10
 TUNE_COMPACT = 11
+TUNE_SMEM_NIB_BYTES = 12
 
 
 class OlapError(RuntimeError):

@@ -45,6 +45,17 @@ std::vector<Candidate> candidates(const olap_ctx* ctx, const olap_starjoin_query
     add({{OLAP_TUNE_PROBE_BITS, 1}, {OLAP_TUNE_SMEM_BITS_BYTES, budget}, {OLAP_TUNE_SMEM_ACC_BYTES, 1},
          {OLAP_TUNE_BLOCK_THREADS, 1024}});
   }
+  // 4-bit codes of the dimensions that fit, with and without pass bitmaps for
+  // the rest (filter and group code of a dimension in one shared probe).
+  add({{OLAP_TUNE_PROBE_BITS, 2}, {OLAP_TUNE_SMEM_NIB_BYTES, cap}, {OLAP_TUNE_BLOCK_THREADS, 1024}});
+  add({{OLAP_TUNE_PROBE_BITS, 2}, {OLAP_TUNE_SMEM_NIB_BYTES, cap}, {OLAP_TUNE_SMEM_BITS_BYTES, int64_t(64) << 10},
+       {OLAP_TUNE_BLOCK_THREADS, 1024}});
+  add({{OLAP_TUNE_PROBE_BITS, 2}, {OLAP_TUNE_SMEM_NIB_BYTES, int64_t(112) << 10}, {OLAP_TUNE_BLOCK_THREADS, 1024}});
+  // ... and with the accumulators in L2, which leaves L1 more room
+  add({{OLAP_TUNE_PROBE_BITS, 2}, {OLAP_TUNE_SMEM_NIB_BYTES, cap}, {OLAP_TUNE_SMEM_ACC_BYTES, 1},
+       {OLAP_TUNE_BLOCK_THREADS, 1024}});
+  add({{OLAP_TUNE_PROBE_BITS, 2}, {OLAP_TUNE_SMEM_NIB_BYTES, int64_t(112) << 10}, {OLAP_TUNE_SMEM_ACC_BYTES, 1},
+       {OLAP_TUNE_BLOCK_THREADS, 1024}});
   // Every plan also with the survivors of the shared-memory probes compacted
   // per warp, with the fact columns prefetched by bulk copies, and with 8
   // rows per thread (512-thread blocks).
@@ -103,7 +114,8 @@ int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q, int64_t 
   std::memcpy(saved, ctx->tune, sizeof(saved));
   for (int k : {OLAP_TUNE_BLOCK_THREADS, OLAP_TUNE_BLOCKS_PER_SM, OLAP_TUNE_SMEM_DIM_BYTES,
                 OLAP_TUNE_SMEM_ACC_BYTES, OLAP_TUNE_UNROLL, OLAP_TUNE_PROBE_BITS,
-                OLAP_TUNE_SMEM_BITS_BYTES, OLAP_TUNE_ASYNC_LOADS, OLAP_TUNE_COMPACT})
+                OLAP_TUNE_SMEM_BITS_BYTES, OLAP_TUNE_ASYNC_LOADS, OLAP_TUNE_COMPACT,
+                OLAP_TUNE_SMEM_NIB_BYTES})
     saved[k] = 0;
   cudaEvent_t e0, e1;
   OLAP_CUDA_TRY(ctx, cudaEventCreate(&e0));

@@ -75,6 +75,7 @@ enum {
   TUNE_GROUP_PLAN = OLAP_TUNE_GROUP_PLAN,
   TUNE_ASYNC_LOADS = OLAP_TUNE_ASYNC_LOADS,
   TUNE_COMPACT = OLAP_TUNE_COMPACT,
+  TUNE_SMEM_NIB_BYTES = OLAP_TUNE_SMEM_NIB_BYTES,
 };
 
 int set_error(olap_ctx* ctx, int status, const std::string& msg);

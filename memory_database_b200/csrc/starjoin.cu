@@ -42,6 +42,9 @@ struct Probe {
   int32_t soff;           // byte offset of a staged int8 copy in shared memory, or -1
   int32_t boff;           // byte offset of a staged pass bitmap in shared memory, or -1
   int32_t code_flag;      // index into StarParams::code_nonzero (bitmap dims)
+  const uint8_t* nib;     // 4-bit codes, two entries per byte (15 = DIM_NULL), or null
+  int32_t noff;           // byte offset of the staged 4-bit codes in shared memory, or -1
+  int32_t nib_flag;       // index into code_nonzero[OLAP_MAX_DIMS + ...]: 1 when a code needs > 4 bits
 };
 
 struct StarParams {
@@ -54,7 +57,8 @@ struct StarParams {
   unsigned long long* out;     // [n_aggs][n_groups]
   unsigned long long* totals;  // [n_aggs] or null
   unsigned long long* range_err;
-  const int32_t* code_nonzero; // per bitmap dim: 1 when some live code != 0
+  const int32_t* code_nonzero; // [0, 4): per bitmap dim, 1 when some live code != 0;
+                               // [4, 8): per 4-bit dim, 1 when some code is outside [0, 14]
   int32_t n_aggs, agg0, agg1;
   int32_t smem_dim_bytes;      // staged dimension bytes and bitmaps (multiple of 16)
   int32_t need_m1, need_m2;
@@ -94,6 +98,31 @@ __global__ void build_pass_bits(const int8_t* __restrict__ vec, uint32_t len,
   if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) atomicOr(nonzero, 1);
 }
 
+// 4-bit codes of one dimension vector, two entries per byte (low nibble
+// first): DIM_NULL becomes 15, codes 0..14 stay; any other code sets *bad
+// (the kernel then probes the int8 vector instead).
+__global__ void build_nibbles(const int8_t* __restrict__ vec, uint32_t len, uint8_t* __restrict__ nib,
+                              int32_t* __restrict__ bad) {
+  const uint32_t nbytes = (len + 1) >> 1;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  bool any = false;
+  auto enc = [&](int32_t c) -> uint32_t {
+    if (c == OLAP_DIM_NULL) return 15u;
+    if (c < 0 || c > 14) {
+      any = true;
+      return 15u;
+    }
+    return static_cast<uint32_t>(c);
+  };
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nbytes; i += stride) {
+    const uint32_t k = 2 * i;
+    const uint32_t lo = enc(vec[k]);
+    const uint32_t hi = k + 1 < len ? enc(vec[k + 1]) : 15u;
+    nib[i] = static_cast<uint8_t>(lo | (hi << 4));
+  }
+  if (any) atomicOr(bad, 1);
+}
+
 // Aggregate sets fixed at compile time for the 128-bit path.
 enum {
   AGGK_GENERIC = 0,   // n_aggs / agg0 / agg1 read at run time
@@ -121,6 +150,16 @@ __device__ __forceinline__ void stage_block(const StarParams& p, unsigned char* 
       } else {
         for (uint32_t i = tid; i < n; i += blockDim.x) dst[i] = src[i];
       }
+    }
+    if (p.dim[j].noff >= 0) {
+      // 4-bit codes (built on the same stream before this kernel; 256-byte
+      // aligned arena buffer).
+      const uint32_t nb = (p.dim[j].len + 1) >> 1;
+      const uint32_t n16 = nb >> 4;
+      const int4* src = reinterpret_cast<const int4*>(p.dim[j].nib);
+      int4* dst = reinterpret_cast<int4*>(sdim + p.dim[j].noff);
+      for (uint32_t i = tid; i < n16; i += blockDim.x) dst[i] = __ldg(src + i);
+      for (uint32_t i = (n16 << 4) + tid; i < nb; i += blockDim.x) sdim[p.dim[j].noff + i] = p.dim[j].nib[i];
     }
     if (p.dim[j].boff >= 0) {
       // Pass bitmap (built on the same stream before this kernel; the arena
@@ -201,6 +240,7 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
   __shared__ long long red[32][2];
   __shared__ unsigned int red_bad;
   __shared__ int32_t s_code_nz[OLAP_MAX_DIMS];
+  __shared__ int32_t s_nib_ok[OLAP_MAX_DIMS];
   constexpr int NG = V / 4;
   unsigned char* sdim = smem;
   unsigned long long* sacc = reinterpret_cast<unsigned long long*>(smem + p.smem_dim_bytes);
@@ -209,6 +249,10 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
   if (tid == 0) red_bad = 0;
   if (tid < OLAP_MAX_DIMS)
     s_code_nz[tid] = (tid < ND && p.dim[tid].code_flag >= 0) ? p.code_nonzero[p.dim[tid].code_flag] : 0;
+  if (tid < OLAP_MAX_DIMS)
+    s_nib_ok[tid] = (tid < ND && p.dim[tid].noff >= 0)
+                        ? (p.code_nonzero[OLAP_MAX_DIMS + p.dim[tid].nib_flag] == 0 ? 1 : 0)
+                        : 0;
   stage_block<ND, ACC>(p, sdim, sacc, nacc);
   const int lane = tid & 31;
   constexpr int NCOL = (ND > 0 ? ND : 1) + 2;
@@ -223,9 +267,12 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
     }
   }
   __syncthreads();
-  bool need_code[OLAP_MAX_DIMS];
+  bool need_code[OLAP_MAX_DIMS], nib_ok[OLAP_MAX_DIMS];
 #pragma unroll
-  for (int j = 0; j < OLAP_MAX_DIMS; ++j) need_code[j] = s_code_nz[j] != 0;
+  for (int j = 0; j < OLAP_MAX_DIMS; ++j) {
+    need_code[j] = s_code_nz[j] != 0;
+    nib_ok[j] = s_nib_ok[j] != 0;
+  }
 
   const uint64_t pol_stream = policy_evict_first();
   const uint64_t pol_keep = policy_evict_last();
@@ -359,7 +406,19 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
       if (alive == 0) break;
       const Probe& d = p.dim[j];
       if (CMP && d.soff < 0 && d.boff < 0) continue;  // global dimensions: after the compaction
-      if (d.soff >= 0) {
+      if (d.noff >= 0 && nib_ok[j]) {
+        // 4-bit codes in shared memory: filter and group code in one probe
+        const uint8_t* sn = reinterpret_cast<const uint8_t*>(sdim + d.noff);
+#pragma unroll
+        for (int r = 0; r < V; ++r) {
+          if (alive & (1u << r)) {
+            const uint32_t k = key(r, j);
+            const int32_t c = (sn[k >> 1] >> ((k & 1u) << 2)) & 15;
+            if (c == 15) alive &= ~(1u << r);
+            g[r] += c * d.factor;
+          }
+        }
+      } else if (d.soff >= 0) {
         const int8_t* sv = reinterpret_cast<const int8_t*>(sdim + d.soff);
 #pragma unroll
         for (int r = 0; r < V; ++r) {
@@ -691,7 +750,10 @@ struct StarPlan {
   int nbits = 0;                       // dims whose pass bitmap must be built
   int bits_dim[OLAP_MAX_DIMS] = {};    // probe index of each
   uint32_t* bits_buf[OLAP_MAX_DIMS] = {};
-  int32_t* code_nz = nullptr;          // [OLAP_MAX_DIMS] in the arena
+  int32_t* code_nz = nullptr;          // [2 * OLAP_MAX_DIMS] in the arena
+  int nnib = 0;                        // dims whose 4-bit codes must be built
+  int nib_dim[OLAP_MAX_DIMS] = {};
+  uint8_t* nib_buf[OLAP_MAX_DIMS] = {};
 };
 
 static bool agg_needs(int ag, bool* m1, bool* m2) {
@@ -739,7 +801,7 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   int idx[OLAP_MAX_DIMS];
   for (int j = 0; j < nd; ++j) idx[j] = j;
   std::stable_sort(idx, idx + nd, [&](int a, int b) { return q->dimvec_len[a] < q->dimvec_len[b]; });
-  int kind[OLAP_MAX_DIMS] = {0, 0, 0, 0};  // 1 int8 staged, 2 bitmap staged, 3 global bitmap
+  int kind[OLAP_MAX_DIMS] = {0, 0, 0, 0};  // 1 int8 staged, 2 bitmap staged, 3 global bitmap, 4 nibbles staged
   int64_t used = 0;
   for (int t = 0; t < nd; ++t) {
     const int j = idx[t];
@@ -749,6 +811,19 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
       used += bytes;
     }
   }
+  // 4-bit codes (filter and group code in one shared-memory probe) up to
+  // TUNE_SMEM_NIB_BYTES, in the caller's order.
+  const int64_t smem_nib_budget = tune_or(ctx, TUNE_SMEM_NIB_BYTES, 0);
+  int64_t nib_used = 0;
+  for (int j = 0; j < nd; ++j) {
+    if (kind[j] || empty) continue;
+    const int64_t nbytes = ((q->dimvec_len[j] + 1) / 2 + 15) & ~int64_t(15);
+    if (nib_used + nbytes <= smem_nib_budget && used + nib_used + nbytes <= smem_cap) {
+      kind[j] = 4;
+      nib_used += nbytes;
+    }
+  }
+  used += nib_used;
   int64_t bits_used = 0;
   for (int j = 0; j < nd; ++j) {
     if (kind[j] || empty) continue;
@@ -761,14 +836,17 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
     }
   }
   pl->nbits = 0;
+  pl->nnib = 0;
   pl->code_nz = nullptr;
   int out = 0;
   int64_t soff = 0;
-  // Probe order: shared-memory int8, then shared-memory bitmaps, then the rest.
-  for (int pass = 1; pass <= 3; ++pass) {
+  // Probe order: shared-memory int8, shared-memory 4-bit codes, shared-memory
+  // bitmaps, then the rest.
+  const int pass_kind[4] = {1, 4, 2, 0};
+  for (int pass = 0; pass < 4; ++pass) {
     for (int j = 0; j < nd; ++j) {
       const int kj = kind[j] == 3 ? 0 : kind[j];
-      if (pass == 3 ? kj != 0 : kj != pass) continue;
+      if (kj != pass_kind[pass]) continue;
       OLAP_REQUIRE(ctx, q->dimvec[j] && (empty || q->fk[j]), "null dimension vector or fk column");
       OLAP_REQUIRE(ctx, q->dimvec_len[j] >= 1 && q->dimvec_len[j] <= INT32_MAX,
                    "dimvec_len must be in [1, 2^31)");
@@ -782,15 +860,30 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
       pr.boff = -1;
       pr.bits = nullptr;
       pr.code_flag = -1;
+      pr.nib = nullptr;
+      pr.noff = -1;
+      pr.nib_flag = -1;
+      if ((kind[j] >= 2) && !pl->code_nz) {
+        pl->code_nz = ar.take<int32_t>(2 * OLAP_MAX_DIMS);
+        if (!pl->code_nz) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
+      }
+      if (kind[j] == 4) {
+        const size_t nbytes = static_cast<size_t>((q->dimvec_len[j] + 1) / 2);
+        uint8_t* nb = ar.take<uint8_t>(nbytes);
+        if (!nb) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for 4-bit codes");
+        pr.nib = nb;
+        pr.noff = static_cast<int32_t>(soff);
+        soff += (static_cast<int64_t>(nbytes) + 15) & ~int64_t(15);
+        pr.nib_flag = pl->nnib;
+        pl->nib_dim[pl->nnib] = k;
+        pl->nib_buf[pl->nnib] = nb;
+        ++pl->nnib;
+      }
       if (kind[j] == 1) {
         pr.soff = static_cast<int32_t>(soff);
         soff += (q->dimvec_len[j] + 15) & ~int64_t(15);
       }
       if (kind[j] == 2 || kind[j] == 3) {
-        if (!pl->code_nz) {
-          pl->code_nz = ar.take<int32_t>(OLAP_MAX_DIMS);
-          if (!pl->code_nz) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
-        }
         uint32_t* b = ar.take<uint32_t>((q->dimvec_len[j] + 31) / 32);
         if (!b) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for pass bitmaps");
         pr.bits = b;
@@ -890,8 +983,16 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
 
 int launch_starjoin(olap_ctx* ctx, StarPlan& pl, cudaStream_t stream) {
   // Pass bitmaps (and their code flags) first, on the same stream.
+  if (pl.nbits || pl.nnib) OLAP_CUDA_TRY(ctx, cudaMemsetAsync(pl.code_nz, 0, sizeof(int32_t) * 2 * OLAP_MAX_DIMS, stream));
+  for (int b = 0; b < pl.nnib; ++b) {
+    const Probe& d = pl.sp.dim[pl.nib_dim[b]];
+    const uint64_t nbytes = (static_cast<uint64_t>(d.len) + 1) / 2;
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((nbytes + 255) / 256,
+                                                                   static_cast<uint64_t>(ctx->sm_count) * 8));
+    build_nibbles<<<grid, 256, 0, stream>>>(d.vec, d.len, pl.nib_buf[b], pl.code_nz + OLAP_MAX_DIMS + b);
+    OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  }
   if (pl.nbits) {
-    OLAP_CUDA_TRY(ctx, cudaMemsetAsync(pl.code_nz, 0, sizeof(int32_t) * OLAP_MAX_DIMS, stream));
     for (int b = 0; b < pl.nbits; ++b) {
       const Probe& d = pl.sp.dim[pl.bits_dim[b]];
       const uint64_t threads = ((static_cast<uint64_t>(d.len) + 31) / 32) * 32;

@@ -192,6 +192,10 @@ def test_dimvec_len_pads_like_reference(ctx):
     {_lib.TUNE_ASYNC_LOADS: 2, _lib.TUNE_SMEM_BITS_BYTES: 64 * 1024, _lib.TUNE_BLOCK_THREADS: 1024},
     {_lib.TUNE_ASYNC_LOADS: 2, _lib.TUNE_BLOCK_THREADS: 128, _lib.TUNE_BLOCKS_PER_SM: 3},
     {_lib.TUNE_ASYNC_LOADS: 2, _lib.TUNE_SMEM_ACC_BYTES: 1, _lib.TUNE_PROBE_BITS: 1},
+    {_lib.TUNE_SMEM_NIB_BYTES: 200 * 1024},               # 4-bit codes staged in smem
+    {_lib.TUNE_SMEM_NIB_BYTES: 16 * 1024, _lib.TUNE_SMEM_BITS_BYTES: 64 * 1024, _lib.TUNE_BLOCK_THREADS: 1024},
+    {_lib.TUNE_SMEM_NIB_BYTES: 200 * 1024, _lib.TUNE_SMEM_DIM_BYTES: 1, _lib.TUNE_UNROLL: 2},
+    {_lib.TUNE_SMEM_NIB_BYTES: 200 * 1024, _lib.TUNE_COMPACT: 2},
     {_lib.TUNE_COMPACT: 2},                               # per-warp survivor compaction
     {_lib.TUNE_COMPACT: 2, _lib.TUNE_SMEM_BITS_BYTES: 64 * 1024, _lib.TUNE_BLOCK_THREADS: 1024},
     {_lib.TUNE_COMPACT: 2, _lib.TUNE_PROBE_BITS: 1, _lib.TUNE_SMEM_ACC_BYTES: 1},
@@ -286,7 +290,8 @@ def test_bitmap_plans_with_nonzero_codes_and_drops(ctx):
     for knobs in ({}, {_lib.TUNE_PROBE_BITS: 1}, {_lib.TUNE_SMEM_BITS_BYTES: 220 * 1024},
                   {_lib.TUNE_SMEM_BITS_BYTES: 2 * 1024, _lib.TUNE_PROBE_BITS: 1},
                   {_lib.TUNE_COMPACT: 2, _lib.TUNE_SMEM_BITS_BYTES: 2 * 1024},
-                  {_lib.TUNE_COMPACT: 2, _lib.TUNE_PROBE_BITS: 1}):
+                  {_lib.TUNE_COMPACT: 2, _lib.TUNE_PROBE_BITS: 1},
+                  {_lib.TUNE_SMEM_NIB_BYTES: 200 * 1024}):  # negative codes: the int8 fallback
         try:
             for k, v in knobs.items():
                 ctx.set_tuning(k, v)
@@ -310,3 +315,28 @@ def test_autotuned_plan_gives_same_results(ctx):
     finally:
         for k in range(16):
             ctx.set_tuning(k, 0)
+
+
+@pytest.mark.parametrize("hi", [14, 15, 40])
+def test_four_bit_staging_and_its_fallback(ctx, hi):
+    """Codes 0..14 use the staged 4-bit vectors; a code of 15 or more makes
+    the kernel fall back to the int8 vector: same results either way."""
+    rng = np.random.default_rng(hi)
+    n = 300_001
+    sizes = [5_000, 70_000, 2_000]
+    dv = [rng.integers(0, hi + 1, s_).astype(np.int8) for s_ in sizes]
+    for d in dv:
+        d[rng.random(len(d)) < 0.3] = 127
+    fk = [rng.integers(0, s_, n).astype(np.int32) for s_ in sizes]
+    m1 = rng.integers(1, 10000, n).astype(np.int32)
+    m2 = rng.integers(-50, 50, n).astype(np.int32)
+    G = (hi + 1) ** 3
+    for knobs in ({_lib.TUNE_SMEM_NIB_BYTES: 200 * 1024, _lib.TUNE_SMEM_DIM_BYTES: 1},
+                  {_lib.TUNE_SMEM_NIB_BYTES: 4 * 1024, _lib.TUNE_SMEM_BITS_BYTES: 16 * 1024}):
+        try:
+            for k, v in knobs.items():
+                ctx.set_tuning(k, v)
+            check_same(ctx, dv, fk, [(hi + 1) ** 2, hi + 1, 1], m1, m2, G, (AGG_M1, AGG_M1_TIMES_M2))
+        finally:
+            for k in knobs:
+                ctx.set_tuning(k, 0)

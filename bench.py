@@ -153,7 +153,7 @@ def cpu_reference(rows: int, sele, groups, steps: int, warmup: int, seed: int = 
             return ref.ref_OLAPcore_vwm_sv(dva, fka, oracle._p(o), nd, oracle._p(f), rows, G,
                                            oracle._p(s.m1), oracle._p(s.m2), cores)
         threads = cores
-        what = "OLAPcore_vwm_sv (reference source, -O3 -march=native)"
+        what = "OLAPcore_vwm_sv (reference source, -O3 -march=x86-64-v3)"
     else:
         def run():
             return oracle.starjoin(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G)

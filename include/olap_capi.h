@@ -402,6 +402,22 @@ OLAP_API int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int 
                             int use_graph);
 /* Number of graphs recorded by olap_batch_run so far. */
 OLAP_API int olap_batch_graph_captures(olap_batch* b, int64_t* captures);
+/* Launch shape of the batched scan: threads per block (multiple of 32 in
+ * [128, 1024]) and per-block shared int64 accumulators (0..24576 slots; the
+ * queries with the fewest groups accumulate there, the rest in L2).  A change
+ * re-records the graphs on the next run. */
+OLAP_API int olap_batch_tune(olap_batch* b, int block, int smem_slots);
+/* Times the block sizes {256, 512, 1024} x accumulator slots {0, 2048, 4096,
+ * 8192, 16384} on the first sample_rows rows (0 = 64 Mi) of the fact table
+ * with these queries (their ranges cut to the sample), keeps the fastest on
+ * the handle and returns it (pointers may be NULL).  out/out_slots/totals as
+ * for olap_batch_run; their contents afterwards are unspecified.
+ * Synchronous. */
+OLAP_API int olap_batch_autotune(olap_batch* b, const olap_batch_query* queries, int n_queries,
+                                 const int32_t* const* fk, const int32_t* m1, const int32_t* m2,
+                                 int64_t n_rows, int agg, int64_t* out, int64_t out_slots,
+                                 int64_t* totals, int64_t sample_rows, int* best_block,
+                                 int* best_slots, double* best_ms);
 
 /* ---- TPC-H Q5-shaped join chain (code/TPCH_Q5/Q5.cpp) ---------------------
  * Tables by column (device pointers).  Supplier and customer keys are 1-based

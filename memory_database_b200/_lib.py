@@ -168,6 +168,9 @@ def _load() -> C.CDLL:
         "olap_batch_set_dimension": (C.c_int, [vp, C.c_int, vp, vp, i64]),
         "olap_batch_run": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, i64, C.c_int, vp, i64, vp, C.c_int]),
         "olap_batch_graph_captures": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+        "olap_batch_tune": (C.c_int, [vp, C.c_int, C.c_int]),
+        "olap_batch_autotune": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, i64, C.c_int, vp, i64, vp, i64,
+                                          C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
         "olap_debug_wait_timeout": (C.c_int, [vp, C.c_uint32]),
         "olap_q5_chain": (C.c_int, [vp, C.POINTER(Q5Tables), i32, i32, i32, vp]),
         "olap_q5_batch": (C.c_int, [vp, C.POINTER(Q5Tables), C.POINTER(Q5Query), C.c_int, vp]),

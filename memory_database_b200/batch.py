@@ -130,6 +130,26 @@ class BatchEngine:
         check(lib.olap_batch_graph_captures(self._h, C.byref(n)), self.ctx.handle)
         return n.value
 
+    def tune(self, block: int, smem_slots: int) -> None:
+        """Launch shape of the scan (threads per block, shared accumulators)."""
+        check(lib.olap_batch_tune(self._h, int(block), int(smem_slots)), self.ctx.handle)
+
+    def autotune(self, queries: list[Query], fk, m1, m2, agg: int = AGG_M1_PLUS_M2, sample_rows: int = 0):
+        """Times the candidate launch shapes on a sample of the fact table with
+        these queries and keeps the fastest; returns (block, smem_slots, ms)."""
+        import torch
+        self.ctx.follow_torch_stream()
+        qs = (BatchQuery * len(queries))(*[q.to_c() for q in queries])
+        slots = max(1, sum(int(q.group_nums) for q in queries))
+        out = torch.empty(slots, dtype=torch.int64, device="cuda")
+        tot = torch.empty(len(queries), dtype=torch.int64, device="cuda")
+        fka = (C.c_void_p * 4)(*[_ptr(f) for f in fk])
+        bb, bs, ms = C.c_int(), C.c_int(), C.c_double()
+        check(lib.olap_batch_autotune(self._h, qs, len(queries), fka, _ptr(m1), _ptr(m2), int(fk[0].numel()),
+                                      int(agg), _ptr(out), slots, _ptr(tot), int(sample_rows), C.byref(bb),
+                                      C.byref(bs), C.byref(ms)), self.ctx.handle)
+        return bb.value, bs.value, ms.value
+
     def run(self, queries: list[Query], fk, m1, m2, agg: int = AGG_M1_PLUS_M2, use_graph: bool = True,
             out=None, totals=None):
         """Returns (out int64[sum group_nums], totals int64[n], offsets list)."""

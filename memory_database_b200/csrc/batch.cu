@@ -74,7 +74,7 @@ struct BatchQuery {
 };
 
 constexpr int kMaxBatchQueries = 64;
-constexpr int kBatchSmemSlots = 4096;           // 32 KiB of per-block int64 accumulators            // one bit per query in a 64-bit mask
+constexpr int kBatchSmemSlots = 4096;  // default per-block int64 accumulators (32 KiB); tunable
 constexpr int kMaxSegments = 2 * kMaxBatchQueries + 2;
 
 // Everything a batch uploads (one pinned staging copy per slot).
@@ -108,10 +108,14 @@ struct BatchParams {
   int32_t tables_used;                // union of the queries' `uses`
   int32_t probe_order;                // 4 x 2-bit table ids, smallest table first
   int32_t agg;                        // OLAP_AGG_* of every query (one aggregate)
+  int32_t smem_slots;                 // per-block shared accumulators (dynamic shared memory)
+  int32_t block;                      // threads per block of the scan (part of a recorded graph)
   unsigned long long* range_err;
 };
 
-constexpr int kBatchThreads = 512;
+constexpr int kBatchThreads = 512;     // default block size; tunable (128..1024)
+constexpr int kBatchMaxThreads = 1024;
+constexpr int kBatchMaxSmemSlots = 24576;  // 192 KiB
 
 __device__ __forceinline__ int64_t batch_value(int agg, int32_t x, int32_t y) {
   switch (agg) {
@@ -172,11 +176,11 @@ __device__ __forceinline__ ulonglong2 ld_record(const DimRecord* r, uint64_t pol
 }
 
 // The fact pass: persistent, 4 rows per thread per step (128-bit loads).
-__global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const BatchParams p) {
+__global__ void __launch_bounds__(kBatchMaxThreads, 1) batch_scan_kernel(const BatchParams p) {
   __shared__ BatchQuery sq[kMaxBatchQueries];
   __shared__ int64_t sseg[kMaxSegments];
   __shared__ unsigned long long smask[kMaxSegments];
-  __shared__ unsigned long long sacc[kBatchSmemSlots];
+  extern __shared__ unsigned long long sacc[];  // p.smem_slots per-block accumulators
   __shared__ int4 s_qf[kMaxBatchQueries];  // per query: group factor at each probe position (0: not grouped)
   __shared__ int4 s_qi[kMaxBatchQueries];  // per query: {group_nums, smem_off, out_offset lo, hi}
   __shared__ unsigned int s_bad;
@@ -214,7 +218,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) batch_scan_kernel(const Batc
     s_qi[i] = make_int4(static_cast<int32_t>(Q.group_nums), Q.smem_off, static_cast<int32_t>(Q.out_offset),
                         static_cast<int32_t>(Q.out_offset >> 32));
   }
-  for (int i = tid; i < kBatchSmemSlots; i += blockDim.x) sacc[i] = 0ull;
+  for (int i = tid; i < p.smem_slots; i += blockDim.x) sacc[i] = 0ull;
   for (int i = tid; i < nseg; i += blockDim.x) {
     sseg[i] = D.seg_begin[i];
     smask[i] = D.seg_mask[i];
@@ -406,6 +410,8 @@ struct olap_batch {
   int2* attrs[OLAP_MAX_DIMS] = {};
   olap::DimRecord* rec[OLAP_MAX_DIMS] = {};
   int64_t attr_len[OLAP_MAX_DIMS] = {};
+  int block = olap::kBatchThreads;        // scan kernel block size (olap_batch_tune / _autotune)
+  int smem_slots = olap::kBatchSmemSlots; // per-block shared accumulators
 };
 
 extern "C" {
@@ -568,7 +574,7 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
     int64_t used = 0;
     for (int q : byg) {
       D.q[q].smem_off = -1;
-      if (used + D.q[q].group_nums <= olap::kBatchSmemSlots) {
+      if (used + D.q[q].group_nums <= b->smem_slots) {
         D.q[q].smem_off = static_cast<int32_t>(used);
         used += D.q[q].group_nums;
       }
@@ -614,13 +620,19 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
   p.desc = b->d_desc[slot];
   p.tables_used = tables;
   p.agg = agg;
+  p.smem_slots = b->smem_slots;
+  p.block = b->block;
   p.range_err = &ctx->counters->range_errors;
   const bool need_m1 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M1 || agg == OLAP_AGG_M1_TIMES_M2;
   const bool need_m2 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M2 || agg == OLAP_AGG_M1_TIMES_M2;
   OLAP_REQUIRE(ctx, n_rows == 0 || ((!need_m1 || m1) && (!need_m2 || m2)), "measure columns required");
+  const size_t scan_smem = sizeof(unsigned long long) * static_cast<size_t>(b->smem_slots);
+  if (scan_smem > 48 * 1024)
+    OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::batch_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(scan_smem)));
   int bps = 1;
-  OLAP_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, olap::batch_scan_kernel,
-                                                                   olap::kBatchThreads, 0));
+  OLAP_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, olap::batch_scan_kernel, b->block,
+                                                                   scan_smem));
   const unsigned grid = static_cast<unsigned>(ctx->sm_count) * static_cast<unsigned>(bps < 1 ? 1 : bps);
   // The work of one batch: descriptors H2D, zero outputs, query masks of the
   // used tables, one persistent pass over the fact table.
@@ -637,7 +649,7 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
       e = cudaGetLastError();
     }
     if (e == cudaSuccess && n_rows > 0) {
-      olap::batch_scan_kernel<<<grid, olap::kBatchThreads, 0, st>>>(p);
+      olap::batch_scan_kernel<<<grid, b->block, scan_smem, st>>>(p);
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
@@ -680,6 +692,91 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
   OLAP_CUDA_TRY(ctx, cudaEventRecord(b->done[slot], ctx->stream));
   b->pending[slot] = true;
   ++b->runs;
+  return OLAP_OK;
+}
+
+int olap_batch_tune(olap_batch* b, int block, int smem_slots) {
+  if (!b) return OLAP_ERR_INVALID;
+  olap_ctx* ctx = b->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_REQUIRE(ctx, block >= 128 && block <= olap::kBatchMaxThreads && block % 32 == 0,
+               "block must be a multiple of 32 in [128, 1024]");
+  OLAP_REQUIRE(ctx, smem_slots >= 0 && smem_slots <= olap::kBatchMaxSmemSlots,
+               "smem_slots must be in [0, 24576]");
+  b->block = block;
+  b->smem_slots = smem_slots;
+  return OLAP_OK;
+}
+
+int olap_batch_autotune(olap_batch* b, const olap_batch_query* queries, int n_queries,
+                        const int32_t* const* fk, const int32_t* m1, const int32_t* m2, int64_t n_rows,
+                        int agg, int64_t* out, int64_t out_slots, int64_t* totals, int64_t sample_rows,
+                        int* best_block, int* best_slots, double* best_ms) {
+  if (!b || !queries || n_queries < 1 || n_queries > b->max_queries) return OLAP_ERR_INVALID;
+  olap_ctx* ctx = b->ctx;
+  if (sample_rows <= 0) sample_rows = int64_t(64) << 20;
+  const int64_t rows = std::min(n_rows, sample_rows);
+  // The queries restricted to the sample's rows [0, rows).
+  std::vector<olap_batch_query> qs(queries, queries + n_queries);
+  for (auto& q : qs) {
+    q.row_begin = std::min(q.row_begin, rows);
+    q.row_end = std::min(q.row_end, rows);
+  }
+  cudaEvent_t e0, e1;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    OLAP_CUDA_TRY(ctx, cudaEventCreate(&e0));
+    OLAP_CUDA_TRY(ctx, cudaEventCreate(&e1));
+  }
+  unsigned long long errs_before = 0;
+  cudaMemcpyAsync(&errs_before, &ctx->counters->range_errors, sizeof(errs_before), cudaMemcpyDeviceToHost,
+                  ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  const int saved_block = b->block, saved_slots = b->smem_slots;
+  double best = 1e30;
+  int bb = saved_block, bs = saved_slots;
+  for (int block : {256, 512, 1024}) {
+    for (int slots : {0, 2048, 4096, 8192, 16384}) {
+      b->block = block;
+      b->smem_slots = slots;
+      float ms = 0.f, best_c = 1e30f;
+      bool ok = true;
+      for (int rep = 0; rep < 3 && ok; ++rep) {
+        cudaEventRecord(e0, ctx->stream);
+        const int st = olap_batch_run(b, qs.data(), n_queries, fk, m1, m2, rows, agg, out, out_slots, totals, 0);
+        cudaEventRecord(e1, ctx->stream);
+        if (st != OLAP_OK || cudaEventSynchronize(e1) != cudaSuccess) {
+          cudaGetLastError();
+          ok = false;
+          break;
+        }
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) best_c = std::min(best_c, ms);  // the first run warms caches
+      }
+      if (ok && best_c < best) {
+        best = best_c;
+        bb = block;
+        bs = slots;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // Rows the timed runs dropped were counted; restore the earlier count.
+  cudaMemcpyAsync(&ctx->counters->range_errors, &errs_before, sizeof(errs_before), cudaMemcpyHostToDevice,
+                  ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  if (best >= 1e29) {
+    b->block = saved_block;
+    b->smem_slots = saved_slots;
+    return olap::set_error(ctx, OLAP_ERR_CUDA, "no batch autotune candidate ran");
+  }
+  b->block = bb;
+  b->smem_slots = bs;
+  if (best_block) *best_block = bb;
+  if (best_slots) *best_slots = bs;
+  if (best_ms) *best_ms = best;
   return OLAP_OK;
 }
 

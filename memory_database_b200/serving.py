@@ -419,8 +419,10 @@ def make_pool(capacity_bytes: int):
 
 
 def gpu_servers(dims, fk, m1, m2, q5data, pool_bytes: int = 256 << 20, agg: int | None = None,
-                max_batch: int = 64, depth: int = 2, plain_depth: int = 4, plain_below: int = 3):
-    """(batched, plain) servers over the same tables and one result pool.
+                max_batch: int = 64, depth: int = 2, plain_depth: int = 4, plain_below: int = 3,
+                tune_queries=None):
+    """(batched, plain) servers over the same tables and one result pool;
+    with tune_queries, the batched engine's launch shape is autotuned first.
 
     Four contexts (own streams and scratch): the batched star lane, the
     batched Q5 lane, and the two plain lanes.  The two servers share the
@@ -431,6 +433,8 @@ def gpu_servers(dims, fk, m1, m2, q5data, pool_bytes: int = 256 << 20, agg: int 
     pool_dev, pool_host = make_pool(pool_bytes)
     ctxs = [Context() for _ in range(4)]
     eng = BatchEngine(ctxs[0], dims, max_queries=max_batch)
+    if tune_queries:  # launch shape of the batched scan, timed on these queries
+        eng.autotune(list(tune_queries)[:max_batch], fk, m1, m2, agg=agg)
     batched = Server({"star": StarBatchLane(eng, fk, m1, m2, agg, pool_dev, pool_host, max_batch, depth,
                                             plain_below=plain_below),
                       "q5": Q5BatchLane(ctxs[1], q5data, pool_dev, pool_host, max_batch, depth)},

@@ -106,3 +106,27 @@ def test_batch_counts_out_of_range_keys_like_the_plain_path(ctx, setup):
     rng = np.random.default_rng(6)
     qs = batch.random_queries(rng, 16, n, GROUPS)
     _check_batch(ctx, (dims, bad, m1, m2, n), qs, olapcore.AGG_M1_PLUS_M2, use_graph=True)
+
+
+@pytest.mark.parametrize("block,slots", [(256, 0), (1024, 16384), (128, 2048), (768, 24576)])
+def test_launch_shapes_do_not_change_results(ctx, setup, block, slots):
+    rng = np.random.default_rng(block + slots)
+    eng = batch.BatchEngine(ctx, setup[0], max_queries=64)
+    eng.tune(block, slots)
+    for nq in (64, 5):
+        qs = batch.random_queries(rng, nq, setup[4], GROUPS)
+        _check_batch(ctx, setup, qs, olapcore.AGG_M1_PLUS_M2, use_graph=True, eng=eng)
+    with pytest.raises(_lib.OlapError):
+        eng.tune(100, 0)
+    with pytest.raises(_lib.OlapError):
+        eng.tune(512, 1 << 20)
+
+
+def test_autotuned_batch_shape(ctx, setup):
+    rng = np.random.default_rng(17)
+    eng = batch.BatchEngine(ctx, setup[0], max_queries=64)
+    qs = batch.random_queries(rng, 64, setup[4], GROUPS)
+    block, slots, ms = eng.autotune(qs, *setup[1:4], sample_rows=1 << 20)
+    assert block in (256, 512, 1024) and slots in (0, 2048, 4096, 8192, 16384) and ms > 0
+    assert ctx.take_range_errors() == 0
+    _check_batch(ctx, setup, qs, olapcore.AGG_M1_PLUS_M2, use_graph=True, eng=eng)

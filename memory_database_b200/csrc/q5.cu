@@ -59,11 +59,10 @@ __global__ void q5_orders_kernel(const int32_t* __restrict__ o_custkey, const in
                                  int8_t* __restrict__ dim_o, unsigned long long* range_err) {
   const uint64_t nmask = *d_mask;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const uint64_t pol = policy_evict_first();
   unsigned int bad = 0;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_orders; i += stride) {
-    const int32_t d = ld_stream_s32(o_orderdate + i, pol);
-    const int32_t c = ld_stream_s32(o_custkey + i, pol);
+  auto one = [&](int64_t i, int32_t d, int32_t c) {
     int8_t v = -1;
     if (d >= date1 && d < date2) {
       if (c < 1 || c > n_cust) {
@@ -74,7 +73,31 @@ __global__ void q5_orders_kernel(const int32_t* __restrict__ o_custkey, const in
       }
     }
     dim_o[i] = v;
+  };
+  // 4 orders per thread (16-byte loads; their customer gathers together)
+  const bool vec = ((reinterpret_cast<uintptr_t>(o_custkey) | reinterpret_cast<uintptr_t>(o_orderdate) |
+                     reinterpret_cast<uintptr_t>(dim_o)) & 15) == 0;
+  const int64_t n4 = vec ? n_orders >> 2 : 0;
+  for (int64_t i = t0; i < n4; i += stride) {
+    const int4 dv = ld_stream_v4(o_orderdate + 4 * i, pol), cv = ld_stream_v4(o_custkey + 4 * i, pol);
+    const int32_t d[4] = {dv.x, dv.y, dv.z, dv.w}, c[4] = {cv.x, cv.y, cv.z, cv.w};
+    int32_t n[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const bool want = d[e] >= date1 && d[e] < date2;
+      const bool okc = c[e] >= 1 && c[e] <= n_cust;
+      bad += want && !okc;
+      n[e] = (want && okc) ? __ldg(c_nationkey + (c[e] - 1)) : -1;
+    }
+    uint32_t packed = 0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int8_t v = (n[e] >= 0 && nation_ok(nmask, n[e])) ? static_cast<int8_t>(n[e]) : static_cast<int8_t>(-1);
+      packed |= static_cast<uint32_t>(static_cast<uint8_t>(v)) << (8 * e);
+    }
+    reinterpret_cast<uint32_t*>(dim_o)[i] = packed;
   }
+  for (int64_t i = 4 * n4 + t0; i < n_orders; i += stride) one(i, o_orderdate[i], o_custkey[i]);
   if (bad) atomicAdd(range_err, static_cast<unsigned long long>(bad));
 }
 
@@ -115,10 +138,23 @@ __global__ void __launch_bounds__(512) q5_lines_kernel(const int32_t* __restrict
   for (int64_t i = t0; i < n4; i += stride) {
     const int4 a = ld_stream_v4(l_suppkey + 4 * i, pol), b = ld_stream_v4(l_order + 4 * i, pol);
     const int4 c = ld_stream_v4(price + 4 * i, pol), d = ld_stream_v4(disc + 4 * i, pol);
-    one(a.x, b.x, c.x, d.x);
-    one(a.y, b.y, c.y, d.y);
-    one(a.z, b.z, c.z, d.z);
-    one(a.w, b.w, c.w, d.w);
+    // The four lines in stages, so that their order-vector gathers are in
+    // flight together: supplier nation, then order nation, then the sums.
+    const int32_t sk[4] = {a.x, a.y, a.z, a.w}, ok[4] = {b.x, b.y, b.z, b.w};
+    const int32_t pr[4] = {c.x, c.y, c.z, c.w}, dc[4] = {d.x, d.y, d.z, d.w};
+    int32_t ns[4], no[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      ns[e] = -1;
+      if (sk[e] < 1 || sk[e] > n_supp || ok[e] < 0 || ok[e] >= n_orders) ++bad;
+      else ns[e] = stage_s ? s_dim[sk[e] - 1] : dim_s[sk[e] - 1];
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) no[e] = ns[e] >= 0 ? static_cast<int8_t>(ld_probe_s8(dim_o + ok[e], keep)) : -2;
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (ns[e] >= 0 && no[e] == ns[e])
+        smem_add_u64(&s_sum[ns[e]], static_cast<uint64_t>(static_cast<int64_t>(pr[e]) * (100 - dc[e])));
   }
   for (int64_t r = 4 * n4 + t0; r < n_lines; r += stride) one(l_suppkey[r], l_order[r], price[r], disc[r]);
   const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
@@ -271,10 +307,32 @@ __global__ void __launch_bounds__(1024, 1) q5b_lines_kernel(
   for (int64_t i = t0; i < n4; i += stride) {
     const int4 a = ld_stream_v4(l_suppkey + 4 * i, pol), b = ld_stream_v4(l_order + 4 * i, pol);
     const int4 c = ld_stream_v4(price + 4 * i, pol), d = ld_stream_v4(disc + 4 * i, pol);
-    one(a.x, b.x, c.x, d.x);
-    one(a.y, b.y, c.y, d.y);
-    one(a.z, b.z, c.z, d.z);
-    one(a.w, b.w, c.w, d.w);
+    // Stages over the four lines (gathers of a stage in flight together):
+    // supplier nation, order nation, order date of the matches, the sums.
+    const int32_t sk[4] = {a.x, a.y, a.z, a.w}, ok[4] = {b.x, b.y, b.z, b.w};
+    const int32_t pr[4] = {c.x, c.y, c.z, c.w}, dc[4] = {d.x, d.y, d.z, d.w};
+    int32_t ns[4], no[4], dt[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      ns[e] = -1;
+      if (sk[e] < 1 || sk[e] > n_supp || ok[e] < 0 || ok[e] >= n_orders) ++bad;
+      else ns[e] = stage_s ? s_dim[sk[e] - 1] : dim_s[sk[e] - 1];
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) no[e] = ns[e] >= 0 ? static_cast<int8_t>(ld_probe_s8(dim_o + ok[e], keep)) : -2;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) dt[e] = (ns[e] >= 0 && no[e] == ns[e]) ? __ldg(o_orderdate + ok[e]) : 0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (ns[e] < 0 || no[e] != ns[e]) continue;
+      uint64_t m = s_nat[ns[e]] & q5_date_mask(D, s_date, dt[e]);
+      const uint64_t v = static_cast<uint64_t>(static_cast<int64_t>(pr[e]) * (100 - dc[e]));
+      while (m) {
+        const int q = __ffsll(static_cast<long long>(m)) - 1;
+        m &= m - 1;
+        smem_add_u64(&s_sum[q * n_nation + ns[e]], v);
+      }
+    }
   }
   for (int64_t r = 4 * n4 + t0; r < n_lines; r += stride) one(l_suppkey[r], l_order[r], price[r], disc[r]);
   const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);

@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--groups", type=int, nargs=4, default=[8, 8, 8, 8])
     ap.add_argument("--fk-dist", default="uniform", choices=["uniform", "zipf"])
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-rows", type=int, default=0,
+                    help="rows per rank of the e2e leg (0: the whole table at N=1, 150M per rank at N>1)")
     ap.add_argument("--cpu-sample-rows", type=int, default=100_000_000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -526,6 +528,10 @@ def main() -> None:
          "rows_per_thread_mode", "probe_bits", "smem_bits_bytes", "group_combine", "group_plan", "async_loads", "compact",
          "smem_nib_bytes"]) if knobs[k]}
 
+    # kernels per query with this plan (the star-join and its staging prepasses)
+    per_query = olapcore.launch_count(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,
+                                      dimvec_lens=s.probe_lens, ctx=ctx)
+
     def step():
         olapcore.starjoin_groupsum(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,
                                    dimvec_lens=s.probe_lens, ctx=ctx, out=gs, totals_out=tot)
@@ -594,7 +600,7 @@ def main() -> None:
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_src} MEASURED_PEAKS.json hbm_gbs" if peak_src == "measured" else "fallback 6650 GB/s",
                      "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms": kernel_ms},
-        "gpu_launches": a.steps,
+        "gpu_launches": a.steps * per_query,
         "clocks": clk.summary(),
     }
 
@@ -603,7 +609,7 @@ def main() -> None:
     # sums are inside the timed region.
     if not a.no_e2e:
         line["e2e"] = e2e_host(a, s, ctx, aggs, world, knobs)
-        line["gpu_launches"] = a.steps + line["e2e"].pop("_launches")
+        line["gpu_launches"] = a.steps * per_query + line["e2e"].pop("_launches") * per_query
     if rank == 0 and world == 1 and not a.no_cpu:
         try:
             cb = cpu_reference(min(a.rows, a.cpu_sample_rows), a.sele, a.groups, 3, 1)
@@ -623,14 +629,18 @@ def e2e_host(a, s, ctx, aggs, world, knobs) -> dict:
     import numpy as np
     import torch
     from memory_database_b200 import _lib, olapcore
-    n = a.rows
+    # rows of this rank's table in pinned host memory: all of them on one GPU;
+    # with several ranks a 150M-row prefix each (the host's pinned memory is
+    # shared by all ranks), the rate scaled by rows
+    n = a.e2e_rows or (a.rows if world == 1 else min(a.rows, 150_000_000))
+    n = min(n, a.rows)
     pin = [torch.empty(n, dtype=torch.int32, pin_memory=True) for _ in range(4)]
     pm1 = torch.empty(n, dtype=torch.int32, pin_memory=True)
     pm2 = torch.empty(n, dtype=torch.int32, pin_memory=True)
     for t in range(4):
-        pin[t].copy_(s.fk[t])
-    pm1.copy_(s.m1)
-    pm2.copy_(s.m2)
+        pin[t].copy_(s.fk[t][:n])
+    pm1.copy_(s.m1[:n])
+    pm2.copy_(s.m2[:n])
     dims_host = [d.cpu().numpy() for d in s.dimvec]
     G = s.group_nums
     hctx = olapcore.Context(ctx.device, scratch_bytes=1 << 30)
@@ -661,7 +671,7 @@ def e2e_host(a, s, ctx, aggs, world, knobs) -> dict:
     h2d = n * 4 * (s.dimvec_nums + 2) + sum(DIM_SIZES[t] for t in s.orders)
     hctx.close()
     return {"value": n * world / dt, "unit": "rows/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": 8 * 2 * G + 16, "ms_per_step": dt * 1e3, "steps": steps,
+            "d2h_bytes_per_step": 8 * 2 * G + 16, "ms_per_step": dt * 1e3, "steps": steps, "rows_per_rank": n,
             "path": "olap_starjoin_groupsum_host, pinned host columns, chunked H2D overlapped with the scan",
             "_launches": steps * nchunks}
 

@@ -137,6 +137,11 @@ typedef struct olap_starjoin_query {
  * either may be NULL when not wanted. */
 OLAP_API int olap_starjoin_groupsum(olap_ctx* ctx, const olap_starjoin_query* q,
                            int64_t* group_sums, int64_t* totals);
+/* Kernels one olap_starjoin_groupsum call of this query launches with the
+ * context's current knobs (the star-join plus one prepass per dimension
+ * staged as a pass bitmap or as 4-bit codes); nothing is launched. */
+OLAP_API int olap_starjoin_launch_count(olap_ctx* ctx, const olap_starjoin_query* q, int want_groups,
+                                        int* kernels);
 
 /* Host pointers; synchronous.  The fact columns are streamed through the GPU
  * in pinned chunks with copies overlapped with the scan.  A dimvec_len[j] of

@@ -133,6 +133,7 @@ def _load() -> C.CDLL:
         "olap_device_count": (C.c_int, []),
         "olap_build_info": (C.c_char_p, []),
         "olap_starjoin_groupsum": (C.c_int, [vp, C.POINTER(StarjoinQuery), vp, vp]),
+        "olap_starjoin_launch_count": (C.c_int, [vp, C.POINTER(StarjoinQuery), C.c_int, C.POINTER(C.c_int)]),
         "olap_starjoin_groupsum_host": (C.c_int, [vp, C.POINTER(StarjoinQuery), vp, vp]),
         "olap_starjoin_autotune": (C.c_int, [vp, C.POINTER(StarjoinQuery), i64, C.POINTER(i64),
                                              C.POINTER(C.c_double)]),

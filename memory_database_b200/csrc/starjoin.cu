@@ -1232,6 +1232,19 @@ int olap_starjoin_groupsum(olap_ctx* ctx, const olap_starjoin_query* q, int64_t*
   return olap::starjoin_device(ctx, q, group_sums, totals, false, ctx->stream, ar);
 }
 
+int olap_starjoin_launch_count(olap_ctx* ctx, const olap_starjoin_query* q, int want_groups, int* kernels) {
+  if (!ctx || !q || !kernels) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  olap::Arena ar(ctx);
+  olap::StarPlan pl;
+  int64_t probe = 0;  // only its address: the plan records the output pointers
+  const int st = olap::plan_starjoin(ctx, q, want_groups ? &probe : nullptr, &probe, ar, &pl);
+  if (st != OLAP_OK) return st;
+  *kernels = q->row_end > q->row_begin ? 1 + pl.nbits + pl.nnib : 0;
+  return OLAP_OK;
+}
+
 int olap_starjoin_groupsum_host(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_sums,
                                 int64_t* totals) {
   if (!ctx || !q) return OLAP_ERR_INVALID;

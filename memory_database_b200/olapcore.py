@@ -219,6 +219,18 @@ def starjoin_groupsum(dimvecs: Sequence, fks: Sequence, factors: Sequence[int], 
     return gs, tot
 
 
+def launch_count(dimvecs: Sequence, fks: Sequence, factors: Sequence[int], m1, m2, group_nums: int,
+                 aggs: Sequence[int] = (AGG_M1_PLUS_M2,), dimvec_lens=None, ctx: Context | None = None) -> int:
+    """Kernels one device-side star-join call of this query launches."""
+    ctx = ctx or default_context()
+    first = fks[0] if len(fks) else (m1 if m1 is not None else m2)
+    n_rows = _nelem(first) if first is not None else 0
+    q = _build_query(dimvecs, fks, factors, m1, m2, group_nums, aggs, 0, n_rows, dimvec_lens)
+    k = C.c_int()
+    check(lib.olap_starjoin_launch_count(ctx.handle, C.byref(q), 1, C.byref(k)), ctx.handle)
+    return k.value
+
+
 def autotune(dimvecs: Sequence, fks: Sequence, factors: Sequence[int], m1, m2, group_nums: int,
              aggs: Sequence[int] = (AGG_M1_PLUS_M2,), dimvec_lens=None, sample_rows: int = 0,
              ctx: Context | None = None):

@@ -340,3 +340,19 @@ def test_four_bit_staging_and_its_fallback(ctx, hi):
         finally:
             for k in knobs:
                 ctx.set_tuning(k, 0)
+
+
+def test_launch_count_follows_the_plan(ctx):
+    sizes, groups, sele = [30000, 2000, 20000, 2556], [5, 5, 4, 7], [0.3, 0.5, 0.7, 0.9]
+    orders, factor, nd, G = olapcore.plan_olapcore(sele, [1] * 4, groups)
+    dv, fk, m1, m2 = random_star(8, 100_000, sizes, sele, groups)
+    dvs, fks = [dev(dv[t]) for t in orders], [dev(fk[t]) for t in orders]
+    args = (dvs, fks, factor, dev(m1), dev(m2), G)
+    try:
+        ctx.set_tuning(_lib.TUNE_SMEM_DIM_BYTES, 1)   # nothing staged as int8
+        assert olapcore.launch_count(*args, ctx=ctx) == 1
+        ctx.set_tuning(_lib.TUNE_SMEM_NIB_BYTES, 200 * 1024)  # every dimension as 4-bit codes
+        assert olapcore.launch_count(*args, ctx=ctx) == 1 + nd
+    finally:
+        ctx.set_tuning(_lib.TUNE_SMEM_DIM_BYTES, 0)
+        ctx.set_tuning(_lib.TUNE_SMEM_NIB_BYTES, 0)

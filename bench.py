@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--rates", type=float, nargs="+", default=[50, 200, 500, 1000, 2000])
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--queries", type=int, default=64)
+    ap.add_argument("--batch-shape", type=str, default="",
+                    help="block,slots of the batched scan (skips its autotuner), e.g. 1024,16384")
     return ap.parse_args()
 
 
@@ -214,7 +216,11 @@ def run_batched(a) -> None:
     out = torch.empty(offs_max, dtype=torch.int64, device="cuda")
     tot = torch.empty(a.queries, dtype=torch.int64, device="cuda")
     # launch shape (block size, shared accumulators) by the engine's autotuner, untimed
-    tuned_block, tuned_slots, _ = eng.autotune(batches[0], s.fk, s.m1, s.m2)
+    if a.batch_shape:
+        tuned_block, tuned_slots = (int(x) for x in a.batch_shape.split(","))
+        eng.tune(tuned_block, tuned_slots)
+    else:
+        tuned_block, tuned_slots, _ = eng.autotune(batches[0], s.fk, s.m1, s.m2)
     for qs in batches[: max(1, a.warmup)]:
         eng.run(qs, s.fk, s.m1, s.m2, out=out, totals=tot)
     torch.cuda.synchronize()
@@ -250,7 +256,8 @@ def run_batched(a) -> None:
                                    "fact range 5-100%), one persistent launch per batch replayed as a CUDA graph",
                        "fact_rows_covered_per_batch": rows_scanned,
                        "launch_shape": {"block_threads": tuned_block, "shared_accumulator_slots": tuned_slots,
-                                        "chosen_by": "olap_batch_autotune on a 64Mi-row sample"}},
+                                        "chosen_by": "--batch-shape" if a.batch_shape
+                                        else "olap_batch_autotune on a 64Mi-row sample"}},
             "data": "synthetic (seeded counter-based generator, generated in HBM)"}
     print(json.dumps(line), flush=True)
     eng.close()

@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--groups", type=int, nargs=4, default=[8, 8, 8, 8])
     ap.add_argument("--fk-dist", default="uniform", choices=["uniform", "zipf"])
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-mode", default="inplace", choices=["inplace", "copy"],
+                    help="host call reads pinned columns in place (OLAP_TUNE_HOST_INPLACE) or copies them")
     ap.add_argument("--e2e-rows", type=int, default=0,
                     help="rows per rank of the e2e leg (0: the whole table at N=1, 150M per rank at N>1)")
     ap.add_argument("--cpu-sample-rows", type=int, default=100_000_000)
@@ -616,7 +618,8 @@ def main() -> None:
     # sums are inside the timed region.
     if not a.no_e2e:
         line["e2e"] = e2e_host(a, s, ctx, aggs, world, knobs)
-        line["gpu_launches"] = a.steps * per_query + line["e2e"].pop("_launches") * per_query
+        line["gpu_launches"] = a.steps * per_query + line["e2e"].pop("_launches") * (
+            1 if a.e2e_mode == "inplace" else per_query)
     if rank == 0 and world == 1 and not a.no_cpu:
         try:
             cb = cpu_reference(min(a.rows, a.cpu_sample_rows), a.sele, a.groups, 3, 1)
@@ -632,8 +635,6 @@ def main() -> None:
 
 
 def e2e_host(a, s, ctx, aggs, world, knobs) -> dict:
-    import ctypes as C
-    import numpy as np
     import torch
     from memory_database_b200 import _lib, olapcore
     # rows of this rank's table in pinned host memory: all of them on one GPU;
@@ -654,6 +655,7 @@ def e2e_host(a, s, ctx, aggs, world, knobs) -> dict:
     for k, v in enumerate(knobs):
         if v and k != _lib.TUNE_HOST_CHUNK_ROWS:
             hctx.set_tuning(k, v)
+    ref = None
 
     def run():
         # the public call with host (pinned) buffers: olap_starjoin_groupsum_host
@@ -661,26 +663,52 @@ def e2e_host(a, s, ctx, aggs, world, knobs) -> dict:
                                           s.factor, pm1, pm2, G, aggs=aggs,
                                           dimvec_lens=[DIM_SIZES[t] for t in s.orders], ctx=hctx)
 
-    run()
-    steps = max(1, a.e2e_steps)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        run()
-    dt = (time.perf_counter() - t0) / steps
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([dt], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dt = t.item()
-    chunk = 1 << 22
-    nchunks = (n + chunk - 1) // chunk
-    h2d = n * 4 * (s.dimvec_nums + 2) + sum(DIM_SIZES[t] for t in s.orders)
+    def measure(mode):
+        nonlocal ref
+        hctx.set_tuning(_lib.TUNE_HOST_INPLACE, 1 if mode == "inplace" else 2)
+        out = run()
+        if ref is None:
+            ref = out
+        else:  # both host paths give the same sums
+            assert all(np_equal(x, y) for x, y in zip(out, ref)), "host paths disagree"
+        steps = max(1, a.e2e_steps)
+        torch.cuda.synchronize()
+        hctx.take_host_bytes()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            run()
+        dt = (time.perf_counter() - t0) / steps
+        h2d = hctx.take_host_bytes() // steps
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = t.item()
+        return dt, h2d, steps
+
+    other = "copy" if a.e2e_mode == "inplace" else "inplace"
+    dt, h2d, steps = measure(a.e2e_mode)
+    dt_o, h2d_o, _ = measure(other)
     hctx.close()
+    chunk = 1 << 22
+    launches = {"inplace": 1 + s.dimvec_nums, "copy": (n + chunk - 1) // chunk}
+    paths = {"inplace": "olap_starjoin_groupsum_host with OLAP_TUNE_HOST_INPLACE=1: one kernel reads the pinned "
+                        "host columns in place over PCIe, the most selective dimension's keys whole and every "
+                        "later column only for rows still alive (32-byte sectors counted on the device)",
+             "copy": "olap_starjoin_groupsum_host, pinned host columns, chunked H2D copies overlapped with the scan"}
     return {"value": n * world / dt, "unit": "rows/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": 8 * 2 * G + 16, "ms_per_step": dt * 1e3, "steps": steps, "rows_per_rank": n,
-            "path": "olap_starjoin_groupsum_host, pinned host columns, chunked H2D overlapped with the scan",
-            "_launches": steps * nchunks}
+            # group sums, totals, the dropped-row count (+ the dimensions' pass counts in place)
+            "d2h_bytes_per_step": 8 * 2 * G + 16 + 8 + (32 if a.e2e_mode == "inplace" else 0),
+            "ms_per_step": dt * 1e3, "steps": steps, "rows_per_rank": n,
+            "path": paths[a.e2e_mode],
+            "other_path": {"path": paths[other], "value": n * world / dt_o, "unit": "rows/s",
+                           "h2d_bytes_per_step": h2d_o, "ms_per_step": dt_o * 1e3},
+            "_launches": steps * launches[a.e2e_mode]}
+
+
+def np_equal(x, y) -> bool:
+    import numpy as np
+    return (x is None and y is None) or np.array_equal(x, y)
 
 
 if __name__ == "__main__":

@@ -75,6 +75,8 @@ extern "C" {
 #define OLAP_TUNE_ASYNC_LOADS 10    /* star-join: 2 prefetches fact columns by bulk async copies (TMA), 1 off */
 #define OLAP_TUNE_COMPACT 11        /* star-join: 2 compacts survivors per warp before global probes, 1 off */
 #define OLAP_TUNE_SMEM_NIB_BYTES 12 /* bytes of 4-bit code vectors staged in smem (default 0)        */
+#define OLAP_TUNE_HOST_INPLACE 13   /* _host star-join over pinned columns: 1 reads them in place
+                                       (late materialisation over PCIe), 2 chunked copies (default) */
 
 typedef struct olap_ctx olap_ctx;
 
@@ -96,6 +98,11 @@ OLAP_API int olap_ctx_set_tuning(olap_ctx* ctx, int knob, int64_t value);
 /* Synchronises, returns and clears the count of rows that kernels dropped
  * because an fk or a group id was out of range. */
 OLAP_API int olap_ctx_take_range_errors(olap_ctx* ctx, int64_t* count);
+/* Synchronises, returns and clears the bytes that _host calls moved from
+ * host memory to the device since the last take: the copied chunks and
+ * dimension vectors, and for in-place reads (OLAP_TUNE_HOST_INPLACE) every
+ * 32-byte sector of host memory that a kernel requested. */
+OLAP_API int olap_ctx_take_host_bytes(olap_ctx* ctx, int64_t* bytes);
 OLAP_API const char* olap_ctx_last_error(const olap_ctx* ctx);
 OLAP_API const char* olap_status_string(int status);
 /* Number of CUDA devices (0 when none; never fails). */
@@ -144,7 +151,12 @@ OLAP_API int olap_starjoin_launch_count(olap_ctx* ctx, const olap_starjoin_query
                                         int* kernels);
 
 /* Host pointers; synchronous.  The fact columns are streamed through the GPU
- * in pinned chunks with copies overlapped with the scan.  A dimvec_len[j] of
+ * in pinned chunks with copies overlapped with the scan.  With
+ * OLAP_TUNE_HOST_INPLACE = 1 and every column in pinned (device-mapped) host
+ * memory, one kernel reads the columns in place instead: the foreign keys of
+ * the dimension that drops the most rows first, each later column only for
+ * the rows still alive (late materialisation over PCIe); its dropped-row count
+ * then covers the keys it read, while the sums are the same.  A dimvec_len[j] of
  * 0 means "unknown": the library then copies dimvec[j][0 .. max fk] (the
  * bytes the reference itself would read).  Returns OLAP_ERR_RANGE (results
  * still written) when rows were dropped. */

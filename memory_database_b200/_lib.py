@@ -48,6 +48,7 @@ TUNE_GROUP_PLAN = 9
 TUNE_ASYNC_LOADS = 10
 TUNE_COMPACT = 11
 TUNE_SMEM_NIB_BYTES = 12
+TUNE_HOST_INPLACE = 13
 
 
 class OlapError(RuntimeError):
@@ -128,6 +129,7 @@ def _load() -> C.CDLL:
         "olap_ctx_synchronize": (C.c_int, [vp]),
         "olap_ctx_set_tuning": (C.c_int, [vp, C.c_int, i64]),
         "olap_ctx_take_range_errors": (C.c_int, [vp, C.POINTER(i64)]),
+        "olap_ctx_take_host_bytes": (C.c_int, [vp, C.POINTER(i64)]),
         "olap_ctx_last_error": (C.c_char_p, [vp]),
         "olap_status_string": (C.c_char_p, [C.c_int]),
         "olap_device_count": (C.c_int, []),

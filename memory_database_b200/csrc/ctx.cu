@@ -149,6 +149,20 @@ int olap_ctx_take_range_errors(olap_ctx* ctx, int64_t* count) {
   return olap::check_timeouts(ctx, ctx->stream);
 }
 
+int olap_ctx_take_host_bytes(olap_ctx* ctx, int64_t* bytes) {
+  if (!ctx || !bytes) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  unsigned long long sectors = 0;
+  OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(&sectors, &ctx->counters->host_sectors, sizeof(sectors),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(&ctx->counters->host_sectors, 0, sizeof(sectors), ctx->stream));
+  OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  *bytes = ctx->host_bytes + static_cast<int64_t>(sectors) * 32;
+  ctx->host_bytes = 0;
+  return OLAP_OK;
+}
+
 const char* olap_ctx_last_error(const olap_ctx* ctx) {
   return ctx ? ctx->last_error.c_str() : "null context";
 }

@@ -23,7 +23,8 @@ namespace olap {
 struct DeviceCounters {
   unsigned long long range_errors;  // rows dropped: fk or group id out of range
   unsigned long long wait_timeouts;  // bounded device waits that gave up
-  unsigned long long pad[14];
+  unsigned long long host_sectors;   // 32-byte host-memory sectors read in place
+  unsigned long long pad[13];
 };
 
 }  // namespace olap
@@ -52,6 +53,10 @@ struct olap_ctx {
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
 
+  // Bytes the host-memory entry points copied to the device (host side;
+  // the in-place sectors are counted on the device).
+  int64_t host_bytes = 0;
+
   // Tuning knobs (0 = automatic); set by olap_ctx_set_tuning.
   int64_t tune[16] = {0};
 
@@ -76,6 +81,7 @@ enum {
   TUNE_ASYNC_LOADS = OLAP_TUNE_ASYNC_LOADS,
   TUNE_COMPACT = OLAP_TUNE_COMPACT,
   TUNE_SMEM_NIB_BYTES = OLAP_TUNE_SMEM_NIB_BYTES,
+  TUNE_HOST_INPLACE = OLAP_TUNE_HOST_INPLACE,
 };
 
 int set_error(olap_ctx* ctx, int status, const std::string& msg);
@@ -115,6 +121,15 @@ struct Arena {
 // `accumulate`, builds pass bitmaps and launches on `stream`; scratch from `ar`.
 int starjoin_device(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_sums,
                     int64_t* totals, bool accumulate, cudaStream_t stream, Arena& ar);
+
+// Host-memory star-join helpers (starjoin.cu, hostscan.cu).  stage_host_dims
+// copies the query's host dimension vectors into `ar` (a dimvec_len of 0 is
+// resolved from the largest key) and points dq at the copies.
+int stage_host_dims(olap_ctx* ctx, const olap_starjoin_query* q, Arena& ar, olap_starjoin_query* dq);
+// In-place scan of pinned host columns; *handled is false (and nothing ran)
+// when a column is not device-mapped or the columns' 16-byte phases differ.
+int starjoin_host_inplace(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_sums,
+                          int64_t* totals, bool* handled);
 
 inline int64_t tune_or(const olap_ctx* c, int knob, int64_t dflt) {
   return c->tune[knob] > 0 ? c->tune[knob] : dflt;
@@ -232,6 +247,17 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
       ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
       : "memory");
+}
+
+// Value of aggregate OLAP_AGG_* `a` for a row with measures x, y.
+__device__ __forceinline__ int64_t agg_value(int a, int32_t x, int32_t y) {
+  switch (a) {
+    case OLAP_AGG_M1_PLUS_M2: return static_cast<int64_t>(x) + y;
+    case OLAP_AGG_M1: return x;
+    case OLAP_AGG_M2: return y;
+    case OLAP_AGG_M1_TIMES_M2: return static_cast<int64_t>(x) * y;
+    default: return 1;
+  }
 }
 
 __device__ __forceinline__ int64_t warp_sum_i64(int64_t v) {

@@ -69,16 +69,6 @@ struct StarParams {
 
 enum { ACC_NONE = 0, ACC_SMEM = 1, ACC_GLOBAL = 2 };
 
-__device__ __forceinline__ int64_t agg_value(int a, int32_t x, int32_t y) {
-  switch (a) {
-    case OLAP_AGG_M1_PLUS_M2: return static_cast<int64_t>(x) + y;
-    case OLAP_AGG_M1: return x;
-    case OLAP_AGG_M2: return y;
-    case OLAP_AGG_M1_TIMES_M2: return static_cast<int64_t>(x) * y;
-    default: return 1;
-  }
-}
-
 // Pass bitmap of one dimension vector: bit k of word k/32 is set when
 // vec[k] != DIM_NULL; *nonzero becomes 1 when a live code is not 0 (then the
 // code must be fetched for surviving rows).  One warp ballot per word.
@@ -1065,6 +1055,26 @@ static bool is_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
+int stage_host_dims(olap_ctx* ctx, const olap_starjoin_query* q, Arena& ar, olap_starjoin_query* dq) {
+  const int64_t rows = q->row_end - q->row_begin;
+  for (int j = 0; j < q->dimvec_nums; ++j) {
+    OLAP_REQUIRE(ctx, q->dimvec[j] && (rows == 0 || q->fk[j]), "null dimension vector or fk column");
+    int64_t len = q->dimvec_len[j];
+    if (len <= 0) {
+      const int32_t m = rows ? host_max_i32(q->fk[j] + q->row_begin, rows) : 0;
+      len = static_cast<int64_t>(m < 0 ? 0 : m) + 1;
+    }
+    int8_t* d = ar.take<int8_t>(static_cast<size_t>(len));
+    if (!d) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for dimension vectors");
+    OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(d, q->dimvec[j], static_cast<size_t>(len),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+    ctx->host_bytes += len;
+    dq->dimvec[j] = d;
+    dq->dimvec_len[j] = len;
+  }
+  return OLAP_OK;
+}
+
 // Host-memory star-join: dimension vectors are copied once; the fact columns
 // stream through two device buffers in chunks, H2D copies of chunk c+1
 // overlapping the scan of chunk c.
@@ -1086,23 +1096,15 @@ int starjoin_host(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   OLAP_REQUIRE(ctx, rows == 0 || !need_m1 || q->m1, "M1 column required by the aggregate");
   OLAP_REQUIRE(ctx, rows == 0 || !need_m2 || q->m2, "M2 column required by the aggregate");
 
+  if (tune_or(ctx, TUNE_HOST_INPLACE, 2) == 1 && rows > 0) {
+    bool handled = false;
+    const int s = starjoin_host_inplace(ctx, q, group_sums, totals, &handled);
+    if (handled) return s;
+  }
   Arena ar(ctx);
   olap_starjoin_query dq = *q;
-  // Dimension vectors.
-  for (int j = 0; j < nd; ++j) {
-    OLAP_REQUIRE(ctx, q->dimvec[j] && (rows == 0 || q->fk[j]), "null dimension vector or fk column");
-    int64_t len = q->dimvec_len[j];
-    if (len <= 0) {
-      const int32_t m = rows ? host_max_i32(q->fk[j] + q->row_begin, rows) : 0;
-      len = static_cast<int64_t>(m < 0 ? 0 : m) + 1;
-    }
-    int8_t* d = ar.take<int8_t>(static_cast<size_t>(len));
-    if (!d) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for dimension vectors");
-    OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(d, q->dimvec[j], static_cast<size_t>(len),
-                                       cudaMemcpyHostToDevice, ctx->stream));
-    dq.dimvec[j] = d;
-    dq.dimvec_len[j] = len;
-  }
+  const int sd = stage_host_dims(ctx, q, ar, &dq);
+  if (sd != OLAP_OK) return sd;
   const int64_t nacc = q->group_nums * q->n_aggs;
   int64_t* dsum = group_sums ? ar.take<int64_t>(static_cast<size_t>(nacc)) : nullptr;
   int64_t* dtot = ar.take<int64_t>(2);
@@ -1174,6 +1176,7 @@ int starjoin_host(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
       cudaError_t e = cudaMemcpyAsync(dbuf[b][k], src, static_cast<size_t>(n) * 4,
                                       cudaMemcpyHostToDevice, cs);
       if (e != cudaSuccess) { st = check_cuda(ctx, e, "cudaMemcpyAsync(H2D chunk)"); break; }
+      ctx->host_bytes += n * 4;
     }
     cudaEventRecord(copied[b], cs);
     cudaStreamWaitEvent(ctx->stream, copied[b], 0);

@@ -119,6 +119,13 @@ class Context:
         check(lib.olap_ctx_take_range_errors(self.handle, C.byref(v)), self.handle)
         return int(v.value)
 
+    def take_host_bytes(self) -> int:
+        """Bytes the host-memory calls moved to the device since the last take
+        (copies, plus the 32-byte sectors read in place)."""
+        v = C.c_int64()
+        check(lib.olap_ctx_take_host_bytes(self.handle, C.byref(v)), self.handle)
+        return int(v.value)
+
     def close(self) -> None:
         if self._h is not None:
             lib.olap_ctx_destroy(self._h)

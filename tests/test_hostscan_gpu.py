@@ -1,0 +1,177 @@
+"""GPU parity tests of the in-place host scan (OLAP_TUNE_HOST_INPLACE = 1):
+olap_starjoin_groupsum_host reading pinned host columns where they are, the
+most selective dimension first.  Sums and totals must equal the oracle's bit
+for bit; the dropped-row count must equal the count of the keys the scan
+reads (restated below in numpy); pageable or differently aligned columns
+must fall back to the chunked copies with the oracle's exact count."""
+import ctypes as C
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from memory_database_b200 import _lib, olapcore
+from memory_database_b200.olapcore import AGG_M1, AGG_M1_PLUS_M2, AGG_M1_TIMES_M2, AGG_M2
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+DIM_NULL = 127
+
+
+def random_star(seed, n, sizes, sele, groups, key_lo=0, key_hi_extra=0):
+    rng = np.random.default_rng(seed)
+    dv = []
+    for s, p, g in zip(sizes, sele, groups):
+        c = rng.integers(0, g, s).astype(np.int8)
+        c[rng.random(s) >= p] = DIM_NULL
+        dv.append(c)
+    fk = [rng.integers(key_lo, s + key_hi_extra, n).astype(np.int32) for s in sizes]
+    m1 = rng.integers(-10000, 10001, n).astype(np.int32)
+    m2 = rng.integers(1, 10001, n).astype(np.int32)
+    return dv, fk, m1, m2
+
+
+def inplace_dropped(dvs, fks, factors, G, row_range):
+    """Rows the in-place scan counts as dropped: dimensions in ascending order
+    of passing entries (stable), a key is range-checked only while its row is
+    alive, then the group id of each surviving row."""
+    rb, re_ = row_range
+    nd = len(dvs)
+    frac = [np.count_nonzero(dvs[j] != DIM_NULL) / len(dvs[j]) for j in range(nd)]
+    order = sorted(range(nd), key=lambda j: frac[j])
+    n = re_ - rb
+    alive = np.ones(n, bool)
+    gid = np.zeros(n, np.int64)
+    bad = 0
+    for j in order:
+        k = fks[j][rb:re_].astype(np.int64)
+        oob = alive & ((k < 0) | (k >= len(dvs[j])))
+        bad += int(oob.sum())
+        alive &= ~oob
+        c = np.full(n, DIM_NULL, np.int64)
+        c[alive] = dvs[j][k[alive]]
+        alive &= c != DIM_NULL
+        gid[alive] += c[alive] * factors[j]
+    bad += int((alive & ((gid < 0) | (gid >= G))).sum())
+    return bad
+
+
+def pinned(a):
+    t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    return t, t.numpy()
+
+
+def run_host(ctx, dvs, fks, factors, m1, m2, G, aggs, row_range):
+    """olap_starjoin_groupsum_host; returns (status, dropped, sums, totals)."""
+    q = olapcore._build_query(dvs, fks, factors, m1, m2, G, aggs, row_range[0], row_range[1],
+                              [len(d) for d in dvs])
+    gs = np.zeros((len(aggs), G), np.int64)
+    tot = np.zeros(len(aggs), np.int64)
+    st = _lib.lib.olap_starjoin_groupsum_host(ctx.handle, C.byref(q), gs.ctypes.data, tot.ctypes.data)
+    dropped = 0
+    if st == _lib.OLAP_ERR_RANGE:
+        msg = _lib.lib.olap_ctx_last_error(ctx.handle).decode()
+        dropped = int(re.match(r"(\d+) rows dropped", msg).group(1))
+    else:
+        assert st == 0, _lib.lib.olap_ctx_last_error(ctx.handle).decode()
+    return st, dropped, gs, tot
+
+
+@pytest.fixture
+def inplace(ctx):
+    ctx.set_tuning(_lib.TUNE_HOST_INPLACE, 1)
+    ctx.take_host_bytes()
+    yield ctx
+    ctx.set_tuning(_lib.TUNE_HOST_INPLACE, 0)
+
+
+SIZES, GROUPS, SELE = [30000, 2000, 200000, 2556], [5, 25, 4, 7], [0.5, 0.2, 0.1, 1.0]
+
+
+@pytest.mark.parametrize("n,row_range", [
+    (1, None), (3, None), (4, None), (5, None), (4097, None), (1_000_003, None),
+    (1_000_003, (1, 999_998)), (1_000_003, (3, 1_000_003)), (100_000, (50_000, 50_001)),
+])
+@pytest.mark.parametrize("aggs", [(AGG_M1_PLUS_M2,), (AGG_M1, AGG_M1_TIMES_M2), (AGG_M2,)])
+def test_inplace_matches_oracle(inplace, n, row_range, aggs):
+    ctx = inplace
+    orders, factor, nd, G = olapcore.plan_olapcore(SELE, [1] * 4, GROUPS)
+    dv, fk, m1, m2 = random_star(n + 7, n, SIZES, SELE, GROUPS)
+    dvs, fks = [dv[t] for t in orders], [fk[t] for t in orders]
+    hold = [pinned(f) for f in fks] + [pinned(m1), pinned(m2)]
+    pf = [h[1] for h in hold[:nd]]
+    pm1, pm2 = hold[nd][1], hold[nd + 1][1]
+    rr = row_range or (0, n)
+    st, dropped, gs, tot = run_host(ctx, dvs, pf, factor, pm1, pm2, G, aggs, rr)
+    o_gs, o_tot, o_err = oracle.starjoin(dvs, fks, factor, m1, m2, G, aggs=aggs, row_range=rr)
+    assert st == 0 and dropped == 0 == o_err
+    assert np.array_equal(tot, o_tot)
+    assert np.array_equal(gs, o_gs)
+    rows = rr[1] - rr[0]
+    ncol = nd + (2 if aggs != (AGG_M2,) and aggs != (AGG_M1,) else 1)
+    hb = ctx.take_host_bytes() - sum(len(d) for d in dvs)
+    assert hb > 0
+    if rows >= 100_000:
+        # the selective dimension (0.1) is read whole, the rest sparsely
+        assert hb < 0.6 * rows * 4 * ncol
+
+
+@pytest.mark.parametrize("nd", [0, 1, 2, 3])
+def test_inplace_fewer_dimensions(inplace, nd):
+    ctx = inplace
+    n = 300_001
+    dv, fk, m1, m2 = random_star(3, n, SIZES[:nd], SELE[:nd], GROUPS[:nd])
+    factor = [int(np.prod(GROUPS[j + 1:nd])) for j in range(nd)]
+    G = int(np.prod(GROUPS[:nd])) if nd else 1
+    hold = [pinned(f) for f in fk] + [pinned(m1), pinned(m2)]
+    st, dropped, gs, tot = run_host(ctx, dv, [h[1] for h in hold[:nd]], factor, hold[nd][1],
+                                    hold[nd + 1][1], G, (AGG_M1, AGG_M1_TIMES_M2), (0, n))
+    o_gs, o_tot, _ = oracle.starjoin(dv, fk, factor, m1, m2, G, aggs=(AGG_M1, AGG_M1_TIMES_M2))
+    assert st == 0 and np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
+
+
+@pytest.mark.parametrize("groups_g", [None, 20])
+def test_inplace_dropped_rows_counted_as_read(inplace, groups_g):
+    """Out-of-range keys (negative and past the end) and group ids: the sums
+    equal the oracle's, the count equals the keys the scan reads."""
+    ctx = inplace
+    n = 500_003
+    dv, fk, m1, m2 = random_star(11, n, SIZES, SELE, GROUPS, key_lo=-3, key_hi_extra=4)
+    factor = [int(np.prod(GROUPS[j + 1:])) for j in range(4)]
+    G = groups_g or int(np.prod(GROUPS))
+    hold = [pinned(f) for f in fk] + [pinned(m1), pinned(m2)]
+    st, dropped, gs, tot = run_host(ctx, dv, [h[1] for h in hold[:4]], factor, hold[4][1], hold[5][1], G,
+                                    (AGG_M1_PLUS_M2, AGG_M1_TIMES_M2), (0, n))
+    o_gs, o_tot, o_err = oracle.starjoin(dv, fk, factor, m1, m2, G, aggs=(AGG_M1_PLUS_M2, AGG_M1_TIMES_M2))
+    assert st == _lib.OLAP_ERR_RANGE
+    assert np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
+    assert dropped == inplace_dropped(dv, fk, factor, G, (0, n))
+    assert 0 < dropped <= o_err
+
+
+def test_inplace_falls_back_to_copies(inplace):
+    """Pageable columns, and pinned columns at different 16-byte phases, take
+    the chunked copy path: the oracle's exact dropped-row count, and the
+    copied bytes counted in full."""
+    ctx = inplace
+    n = 200_000
+    dv, fk, m1, m2 = random_star(5, n + 1, SIZES, SELE, GROUPS, key_hi_extra=2)
+    factor = [int(np.prod(GROUPS[j + 1:])) for j in range(4)]
+    G = int(np.prod(GROUPS))
+    aggs = (AGG_M1_PLUS_M2,)
+    o_gs, o_tot, o_err = oracle.starjoin(dv, [f[1:] for f in fk], factor, m1[1:], m2[1:], G, aggs=aggs)
+    # pageable
+    st, dropped, gs, tot = run_host(ctx, dv, [np.ascontiguousarray(f[1:]) for f in fk], factor,
+                                    np.ascontiguousarray(m1[1:]), np.ascontiguousarray(m2[1:]), G, aggs, (0, n))
+    assert dropped == o_err > 0 and np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
+    assert ctx.take_host_bytes() == n * 4 * 6 + sum(len(d) for d in dv)
+    # pinned, one column shifted by one row against the others
+    hold = [pinned(f) for f in fk] + [pinned(m1), pinned(m2)]
+    cols = [h[1][1:] for h in hold]
+    cols[0] = pinned(fk[0][1:])[1]
+    hold.append(cols[0])
+    st, dropped, gs, tot = run_host(ctx, dv, cols[:4], factor, cols[4], cols[5], G, aggs, (0, n))
+    assert dropped == o_err and np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
+    assert ctx.take_host_bytes() == n * 4 * 6 + sum(len(d) for d in dv)

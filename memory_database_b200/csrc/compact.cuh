@@ -16,6 +16,8 @@
 // call reports OLAP_ERR_TIMEOUT.
 #pragma once
 
+#include <type_traits>
+
 #include "olap_internal.cuh"
 
 namespace olap {
@@ -115,54 +117,84 @@ __device__ __forceinline__ int64_t lookback(const ScanTiles& st, int64_t tile, u
 //   void op.emit(int u, int k, int64_t item, int64_t pos)  -> write selected
 //       item `item` (= first + k of group u) at output position `pos`.
 // A larger G keeps more bytes in flight per block for ops that cache little.
+// Rounds per tile: an op whose emit() needs nothing cached from flags()
+// (Op::kRounds > 1) takes that many consecutive sub-tiles of kGroups loads
+// per thread into one tile, keeping only their 4-bit masks, so that one
+// look-back covers R times the bytes.
+template <class Op, class = void>
+struct OpRounds {
+  static constexpr int value = 1;
+};
+template <class Op>
+struct OpRounds<Op, std::void_t<decltype(Op::kRounds)>> {
+  static constexpr int value = Op::kRounds;
+};
+
+template <class Op>
+constexpr int64_t compact_sub_items() {
+  return static_cast<int64_t>(kCompactThreads) * 4 * Op::kGroups;
+}
 template <class Op>
 constexpr int64_t compact_tile_items() {
-  return static_cast<int64_t>(kCompactThreads) * 4 * Op::kGroups;
+  return compact_sub_items<Op>() * OpRounds<Op>::value;
 }
 
 template <class Op>
 __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const Op op_in, int64_t n_items, ScanTiles st) {
   constexpr int G = Op::kGroups;
+  constexpr int R = OpRounds<Op>::value;
   constexpr int W = kCompactThreads / 32;
-  constexpr int E = G * W;  // warp counts per tile
+  constexpr int E = R * G * W;  // warp counts per tile
   static_assert(G <= 16 && E % 32 == 0, "groups per thread: a multiple of 4, at most 16");
   constexpr int PER = E / 32;
+  constexpr int64_t SUB = compact_sub_items<Op>();
   Op op = op_in;  // per-thread copy: ops cache the loaded items between flags() and emit()
   __shared__ unsigned int s_tile;
-  __shared__ uint32_t s_cnt[E];  // warp counts of (u, w), then their exclusive prefixes in the tile
+  __shared__ uint32_t s_cnt[E];  // warp counts of (r, u, w), then their exclusive prefixes in the tile
   __shared__ long long s_base;
+  // masks of the rounds before the last (one round in flight at a time keeps
+  // the registers of a single round)
+  __shared__ uint64_t s_mask[R > 1 ? R - 1 : 1][kCompactThreads];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
   for (;;) {
     const int64_t tile = claim_tile(st, &s_tile);
     if (tile >= st.n_tiles) return;
     const int64_t tile_first = tile * compact_tile_items<Op>();
-    uint64_t masks = 0;  // 4 bits per group
-    if (op.vec_ok() && tile_first + compact_tile_items<Op>() <= n_items) {
-      // full tile, aligned columns: every group's loads are issued before
-      // the first is used, so G x 16 bytes per thread are in flight
+    const bool full = op.vec_ok() && tile_first + compact_tile_items<Op>() <= n_items;
+    uint64_t last = 0;  // 4 bits per group of the last round
+#pragma unroll 1
+    for (int r = 0; r < R; ++r) {
+      const int64_t sub_first = tile_first + r * SUB;
+      uint64_t mk = 0;
+      if (full) {
+        // full tile, aligned columns: every group's loads are issued before
+        // the first is used, so G x 16 bytes per thread are in flight
 #pragma unroll
-      for (int u = 0; u < G; ++u)
-        op.prefetch(u, tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x);
+        for (int u = 0; u < G; ++u)
+          op.prefetch(u, sub_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x);
+#pragma unroll
+        for (int u = 0; u < G; ++u) {
+          const int64_t first = sub_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
+          mk |= static_cast<uint64_t>(op.template flags<true>(u, first, 4)) << (4 * u);
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < G; ++u) {
+          const int64_t first = sub_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
+          const int64_t left = n_items - first;
+          const int nv = left >= 4 ? 4 : (left > 0 ? static_cast<int>(left) : 0);
+          const uint32_t m = nv > 0 ? op.template flags<false>(u, first, nv) : 0u;
+          mk |= static_cast<uint64_t>(m) << (4 * u);
+        }
+      }
+      if (r + 1 < R) s_mask[r][threadIdx.x] = mk;
+      else last = mk;
 #pragma unroll
       for (int u = 0; u < G; ++u) {
-        const int64_t first = tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
-        masks |= static_cast<uint64_t>(op.template flags<true>(u, first, 4)) << (4 * u);
+        const uint32_t c = __reduce_add_sync(0xffffffffu, __popc(static_cast<uint32_t>(mk >> (4 * u)) & 15u));
+        if (lane == 0) s_cnt[(r * G + u) * W + warp] = c;
       }
-    } else {
-#pragma unroll
-      for (int u = 0; u < G; ++u) {
-        const int64_t first = tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
-        const int64_t left = n_items - first;
-        const int nv = left >= 4 ? 4 : (left > 0 ? static_cast<int>(left) : 0);
-        const uint32_t m = nv > 0 ? op.template flags<false>(u, first, nv) : 0u;
-        masks |= static_cast<uint64_t>(m) << (4 * u);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < G; ++u) {
-      const uint32_t c = __reduce_add_sync(0xffffffffu, __popc(static_cast<uint32_t>(masks >> (4 * u)) & 15u));
-      if (lane == 0) s_cnt[u * W + warp] = c;
     }
     __syncthreads();
     if (warp == 0) {
@@ -195,18 +227,22 @@ __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const Op op_in
     __syncthreads();
     const long long base = s_base;
     if (base < 0) return;  // timed out: the host reports it
+#pragma unroll 1
+    for (int r = 0; r < R; ++r) {
+      const uint64_t mk = r + 1 < R ? s_mask[r][threadIdx.x] : last;
 #pragma unroll
-    for (int u = 0; u < G; ++u) {
-      const uint32_t m = static_cast<uint32_t>(masks >> (4 * u)) & 15u;
-      uint32_t before = 0;
+      for (int u = 0; u < G; ++u) {
+        const uint32_t m = static_cast<uint32_t>(mk >> (4 * u)) & 15u;
+        uint32_t before = 0;
 #pragma unroll
-      for (int k = 0; k < 4; ++k) before += __popc(__ballot_sync(0xffffffffu, (m >> k) & 1u) & lt);
-      if (!m) continue;
-      int64_t pos = base + s_cnt[u * W + warp] + before;
-      const int64_t first = tile_first + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
+        for (int k = 0; k < 4; ++k) before += __popc(__ballot_sync(0xffffffffu, (m >> k) & 1u) & lt);
+        if (!m) continue;
+        int64_t pos = base + s_cnt[(r * G + u) * W + warp] + before;
+        const int64_t first = tile_first + r * SUB + static_cast<int64_t>(u) * kCompactThreads * 4 + 4 * threadIdx.x;
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if ((m >> k) & 1u) op.emit(u, k, first + k, pos++);
+        for (int k = 0; k < 4; ++k)
+          if ((m >> k) & 1u) op.emit(u, k, first + k, pos++);
+      }
     }
   }
 }

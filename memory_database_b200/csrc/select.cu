@@ -23,10 +23,12 @@ __device__ __forceinline__ int32_t lane4(const int4& v, int k) {
 
 // Items are rows (kRid false) or positions of an input selection vector.
 // The plain column case caches nothing between flags() and emit(), so it
-// takes 16 groups per thread (64 KB tiles); with row ids, 8.
+// takes 16 groups per thread and 4 rounds per tile (256 KB tiles); with row
+// ids, 8 groups and one round.
 template <bool kRid>
 struct SelectOp {
   static constexpr int kGroups = kRid ? 8 : 16;
+  static constexpr int kRounds = kRid ? 1 : 4;  // emit() of a plain column needs nothing cached
   const int32_t* col;
   const int32_t* in_rowids;  // optional input selection vector
   int32_t* out;

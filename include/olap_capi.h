@@ -77,6 +77,7 @@ extern "C" {
 #define OLAP_TUNE_SMEM_NIB_BYTES 12 /* bytes of 4-bit code vectors staged in smem (default 0)        */
 #define OLAP_TUNE_HOST_INPLACE 13   /* _host star-join over pinned columns: 1 reads them in place
                                        (late materialisation over PCIe), 2 chunked copies (default) */
+#define OLAP_TUNE_MERGE_PROBES 14   /* star-join: 1 probes consecutive L2 int8 dimensions together, 2 off */
 
 typedef struct olap_ctx olap_ctx;
 

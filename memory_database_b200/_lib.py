@@ -49,6 +49,7 @@ TUNE_ASYNC_LOADS = 10
 TUNE_COMPACT = 11
 TUNE_SMEM_NIB_BYTES = 12
 TUNE_HOST_INPLACE = 13
+TUNE_MERGE_PROBES = 14
 
 
 class OlapError(RuntimeError):

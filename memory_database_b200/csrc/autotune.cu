@@ -57,8 +57,8 @@ std::vector<Candidate> candidates(const olap_ctx* ctx, const olap_starjoin_query
   add({{OLAP_TUNE_PROBE_BITS, 2}, {OLAP_TUNE_SMEM_NIB_BYTES, int64_t(112) << 10}, {OLAP_TUNE_SMEM_ACC_BYTES, 1},
        {OLAP_TUNE_BLOCK_THREADS, 1024}});
   // Every plan also with the survivors of the shared-memory probes compacted
-  // per warp, with the fact columns prefetched by bulk copies, and with 8
-  // rows per thread (512-thread blocks).
+  // per warp, with the fact columns prefetched by bulk copies, with 8 rows
+  // per thread (512-thread blocks) and with merged L2 probes.
   const size_t n4 = c.size();
   for (size_t i = 0; i < n4; ++i) {
     Candidate x = c[i];
@@ -72,6 +72,12 @@ std::vector<Candidate> candidates(const olap_ctx* ctx, const olap_starjoin_query
     Candidate x = c[i];
     x.knob[OLAP_TUNE_UNROLL] = 2;
     x.knob[OLAP_TUNE_BLOCK_THREADS] = 512;
+    c.push_back(x);
+  }
+  // ... and with consecutive L2 probes issued together (one round trip).
+  for (size_t i = 0; i < n4; ++i) {
+    Candidate x = c[i];
+    x.knob[OLAP_TUNE_MERGE_PROBES] = 1;
     c.push_back(x);
   }
   return c;
@@ -115,7 +121,7 @@ int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q, int64_t 
   for (int k : {OLAP_TUNE_BLOCK_THREADS, OLAP_TUNE_BLOCKS_PER_SM, OLAP_TUNE_SMEM_DIM_BYTES,
                 OLAP_TUNE_SMEM_ACC_BYTES, OLAP_TUNE_UNROLL, OLAP_TUNE_PROBE_BITS,
                 OLAP_TUNE_SMEM_BITS_BYTES, OLAP_TUNE_ASYNC_LOADS, OLAP_TUNE_COMPACT,
-                OLAP_TUNE_SMEM_NIB_BYTES})
+                OLAP_TUNE_SMEM_NIB_BYTES, OLAP_TUNE_MERGE_PROBES})
     saved[k] = 0;
   cudaEvent_t e0, e1;
   OLAP_CUDA_TRY(ctx, cudaEventCreate(&e0));

@@ -82,6 +82,7 @@ enum {
   TUNE_COMPACT = OLAP_TUNE_COMPACT,
   TUNE_SMEM_NIB_BYTES = OLAP_TUNE_SMEM_NIB_BYTES,
   TUNE_HOST_INPLACE = OLAP_TUNE_HOST_INPLACE,
+  TUNE_MERGE_PROBES = OLAP_TUNE_MERGE_PROBES,
 };
 
 int set_error(olap_ctx* ctx, int status, const std::string& msg);

@@ -64,6 +64,7 @@ struct StarParams {
   int32_t need_m1, need_m2;
   int32_t pf_off, bar_off;     // ASYNC: per-warp prefetch buffers and mbarriers (shared-memory offsets)
   int32_t cmp_off;             // CMP: per-warp survivor buffers (shared-memory offset)
+  int32_t merge_global;        // probe consecutive global int8 dimensions together
   unsigned long long* wait_timeouts;
 };
 
@@ -391,9 +392,14 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
     int32_t g[V];
 #pragma unroll
     for (int r = 0; r < V; ++r) g[r] = 0;
+    bool skip = false;  // this dimension was probed with the previous one
 #pragma unroll
     for (int j = 0; j < ND; ++j) {
       if (alive == 0) break;
+      if (skip) {
+        skip = false;
+        continue;
+      }
       const Probe& d = p.dim[j];
       if (CMP && d.soff < 0 && d.boff < 0) continue;  // global dimensions: after the compaction
       if (d.noff >= 0 && nib_ok[j]) {
@@ -433,14 +439,33 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
         for (int r = 0; r < V; ++r)
           if (!((w[r] >> (key(r, j) & 31)) & 1u)) alive &= ~(1u << r);
       } else {
-        int32_t c[V];
+        // int8 probe through L2; with merge_global, the next dimension's too
+        // when it is also one (both in flight: one round trip instead of two)
+        const int j1 = j + 1 < ND ? j + 1 : j;
+        const Probe& d1 = p.dim[j1];
+        const bool two = !CMP && p.merge_global && j + 1 < ND && d1.soff < 0 && d1.boff < 0 && !d1.bits &&
+                         !(d1.noff >= 0 && nib_ok[j1]);
+        int32_t c[V], c1[V];
 #pragma unroll
         for (int r = 0; r < V; ++r)
           c[r] = (alive & (1u << r)) ? ld_probe_s8(d.vec + key(r, j), pol_keep) : OLAP_DIM_NULL;
+        if (two) {
+#pragma unroll
+          for (int r = 0; r < V; ++r)
+            c1[r] = (alive & (1u << r)) ? ld_probe_s8(d1.vec + key(r, j1), pol_keep) : OLAP_DIM_NULL;
+        }
 #pragma unroll
         for (int r = 0; r < V; ++r) {
           if (c[r] == OLAP_DIM_NULL) alive &= ~(1u << r);
           g[r] += c[r] * d.factor;
+        }
+        if (two) {
+#pragma unroll
+          for (int r = 0; r < V; ++r) {
+            if (c1[r] == OLAP_DIM_NULL) alive &= ~(1u << r);
+            g[r] += c1[r] * d1.factor;
+          }
+          skip = true;
         }
       }
     }
@@ -943,6 +968,7 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   // Bulk-copy prefetch: per warp, 32 vectors of each streamed column for each
   // group of 4 rows per thread, and one mbarrier; only when it fits.
   sp->wait_timeouts = &ctx->counters->wait_timeouts;
+  sp->merge_global = tune_or(ctx, TUNE_MERGE_PROBES, 2) == 1 ? 1 : 0;
   pl->async = false;
   if (vec && tune_or(ctx, TUNE_ASYNC_LOADS, 1) == 2 && nd + (need_m1 ? 1 : 0) + (need_m2 ? 1 : 0) > 0) {
     const int64_t warps = pl->block / 32;

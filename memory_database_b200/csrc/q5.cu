@@ -10,8 +10,8 @@
 // Here the sum is int64 fixed point: SUM price_cents * (100 - discount_pct),
 // exactly 100 x 100 x the decimal revenue.
 //
-// Three passes: suppliers -> int8 nation vector (small: staged in shared
-// memory by the line pass), orders -> int8 nation vector (one byte per order,
+// Three passes: suppliers -> int8 nation vector and its 4-bit codes (staged
+// in shared memory by the line pass), orders -> int8 nation vector (one byte per order,
 // L2-resident for the line pass), lines -> per-nation int64 sums in shared
 // memory, flushed once per block.  Customer and supplier keys are 1-based as
 // in the reference; orders are addressed by row (l_orderkey_new).
@@ -50,6 +50,26 @@ __global__ void q5_supplier_kernel(const int32_t* __restrict__ s_nationkey, int6
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_supp; i += stride) {
     const int32_t n = s_nationkey[i];
     dim_s[i] = nation_ok(nmask, n) ? static_cast<int8_t>(n) : static_cast<int8_t>(-1);
+  }
+}
+
+// 4-bit codes of the supplier nations for the line pass: code c < 15 is the
+// c-th nation of the region's mask, 15 none.  Exact when the region has at
+// most 15 nations; the line pass checks that before it uses them.
+__global__ void q5_supplier_nib_kernel(const int8_t* __restrict__ dim_s, int64_t n_supp,
+                                       const unsigned long long* __restrict__ d_mask, uint8_t* __restrict__ nib) {
+  const uint64_t nmask = *d_mask;
+  auto code = [&](int32_t n) -> uint32_t {
+    if (n < 0) return 15u;
+    const uint32_t c = static_cast<uint32_t>(__popcll(nmask & ((1ull << n) - 1ull)));
+    return c < 15u ? c : 15u;
+  };
+  const int64_t nbytes = (n_supp + 1) >> 1;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nbytes; i += stride) {
+    const uint32_t lo = code(dim_s[2 * i]);
+    const uint32_t hi = 2 * i + 1 < n_supp ? code(dim_s[2 * i + 1]) : 15u;
+    nib[i] = static_cast<uint8_t>(lo | (hi << 4));
   }
 }
 
@@ -101,21 +121,44 @@ __global__ void q5_orders_kernel(const int32_t* __restrict__ o_custkey, const in
   if (bad) atomicAdd(range_err, static_cast<unsigned long long>(bad));
 }
 
-__global__ void __launch_bounds__(512) q5_lines_kernel(const int32_t* __restrict__ l_suppkey,
+// stage_s: 0 probes the int8 supplier vector through L1/L2; 2 stages the
+// 4-bit codes in shared memory (half the bytes of the int8 vector, so more
+// blocks fit an SM), and falls back to 0 when the region has more than 15
+// nations.
+__global__ void __launch_bounds__(512, 3) q5_lines_kernel(const int32_t* __restrict__ l_suppkey,
                                                        const int32_t* __restrict__ l_order,
                                                        const int32_t* __restrict__ price,
                                                        const int32_t* __restrict__ disc, int64_t n_lines,
                                                        const int8_t* __restrict__ dim_s, int64_t n_supp,
+                                                       const uint8_t* __restrict__ nib_s,
+                                                       const unsigned long long* __restrict__ d_mask,
                                                        const int8_t* __restrict__ dim_o, int64_t n_orders,
                                                        unsigned long long* __restrict__ sums,
                                                        unsigned long long* range_err, int stage_s) {
-  extern __shared__ int8_t s_dim[];  // staged supplier nations (stage_s)
+  extern __shared__ int8_t s_dim[];  // staged supplier nations or their 4-bit codes (stage_s)
   __shared__ unsigned long long s_sum[kQ5MaxNations];
+  __shared__ int8_t s_nat[16];       // 4-bit code -> nation
   const int tid = threadIdx.x;
+  const uint64_t nmask = stage_s == 2 ? *d_mask : 0ull;
+  const int mode = stage_s == 2 && __popcll(nmask) > 15 ? 0 : stage_s;
   for (int i = tid; i < kQ5MaxNations; i += blockDim.x) s_sum[i] = 0;
-  if (stage_s)
-    for (int64_t i = tid; i < n_supp; i += blockDim.x) s_dim[i] = dim_s[i];
+  if (mode == 2 && tid < 16) {
+    // the tid-th set bit of the mask
+    uint64_t m = nmask;
+    for (int k = 0; k < tid && m; ++k) m &= m - 1;
+    s_nat[tid] = m ? static_cast<int8_t>(__ffsll(static_cast<long long>(m)) - 1) : static_cast<int8_t>(-1);
+  }
+  if (mode == 2)
+    for (int64_t i = tid; i < ((n_supp + 1) >> 1); i += blockDim.x) s_dim[i] = static_cast<int8_t>(nib_s[i]);
   __syncthreads();
+  // nation of supplier row s (0-based), -1 when it is not in the region
+  auto snation = [&](int32_t s) -> int32_t {
+    if (mode == 2) {
+      const uint32_t c = (static_cast<uint8_t>(s_dim[s >> 1]) >> ((s & 1) << 2)) & 15u;
+      return c == 15u ? -1 : s_nat[c];
+    }
+    return dim_s[s];
+  };
   const uint64_t pol = policy_evict_first();
   const uint64_t keep = policy_evict_last();
   unsigned int bad = 0;
@@ -124,7 +167,7 @@ __global__ void __launch_bounds__(512) q5_lines_kernel(const int32_t* __restrict
       ++bad;
       return;
     }
-    const int32_t ns = stage_s ? s_dim[sk - 1] : dim_s[sk - 1];
+    const int32_t ns = snation(sk - 1);
     if (ns < 0) return;
     const int32_t no = static_cast<int8_t>(ld_probe_s8(dim_o + ok, keep));
     if (no != ns) return;
@@ -147,7 +190,7 @@ __global__ void __launch_bounds__(512) q5_lines_kernel(const int32_t* __restrict
     for (int e = 0; e < 4; ++e) {
       ns[e] = -1;
       if (sk[e] < 1 || sk[e] > n_supp || ok[e] < 0 || ok[e] >= n_orders) ++bad;
-      else ns[e] = stage_s ? s_dim[sk[e] - 1] : dim_s[sk[e] - 1];
+      else ns[e] = snation(sk[e] - 1);
     }
 #pragma unroll
     for (int e = 0; e < 4; ++e) no[e] = ns[e] >= 0 ? static_cast<int8_t>(ld_probe_s8(dim_o + ok[e], keep)) : -2;
@@ -370,9 +413,10 @@ int olap_q5_chain(olap_ctx* ctx, const olap_q5_tables* t, int32_t region, int32_
                "null lineitem column");
   olap::Arena ar(ctx);
   int8_t* dim_s = ar.take<int8_t>(static_cast<size_t>(t->n_supp > 0 ? t->n_supp : 1));
+  uint8_t* nib_s = ar.take<uint8_t>(static_cast<size_t>(t->n_supp > 0 ? (t->n_supp + 1) / 2 : 1));
   int8_t* dim_o = ar.take<int8_t>(static_cast<size_t>(t->n_orders > 0 ? t->n_orders : 1));
   unsigned long long* nmask = ar.take<unsigned long long>(1);
-  if (!dim_s || !dim_o || !nmask)
+  if (!dim_s || !nib_s || !dim_o || !nmask)
     return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for Q5 vectors");
   olap::q5_nation_mask_kernel<<<1, 64, 0, ctx->stream>>>(t->r_regionkey, t->n_region, t->n_regionkey, t->n_nation,
                                                         region, nmask);
@@ -384,9 +428,13 @@ int olap_q5_chain(olap_ctx* ctx, const olap_q5_tables* t, int32_t region, int32_
     olap::q5_orders_kernel<<<olap::grid_q5(ctx, t->n_orders, 256), 256, 0, ctx->stream>>>(
         t->o_custkey, t->o_orderdate, t->n_orders, t->c_nationkey, t->n_cust, nmask, date1, date2, dim_o,
         &ctx->counters->range_errors);
+  // Supplier nations in shared memory as 4-bit codes when they fit (160 KB).
+  const int stage = t->n_lines && t->n_supp > 0 && (t->n_supp + 1) / 2 <= 160 * 1024 ? 2 : 0;
+  if (stage == 2)
+    olap::q5_supplier_nib_kernel<<<olap::grid_q5(ctx, (t->n_supp + 1) / 2, 256), 256, 0, ctx->stream>>>(
+        dim_s, t->n_supp, nmask, nib_s);
   if (t->n_lines) {
-    const bool stage = t->n_supp <= 160 * 1024;
-    const size_t smem = stage ? static_cast<size_t>((t->n_supp + 15) & ~int64_t(15)) : 0;
+    const size_t smem = stage == 2 ? static_cast<size_t>(((t->n_supp + 1) / 2 + 15) & ~int64_t(15)) : 0;
     if (smem > 48 * 1024)
       OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::q5_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast<int>(smem)));
@@ -395,8 +443,8 @@ int olap_q5_chain(olap_ctx* ctx, const olap_q5_tables* t, int32_t region, int32_
     int64_t grid = static_cast<int64_t>(ctx->sm_count) * (bps < 1 ? 1 : bps);
     grid = std::min<int64_t>(grid, (t->n_lines / 4 + 511) / 512 + 1);
     olap::q5_lines_kernel<<<static_cast<unsigned>(grid), 512, smem, ctx->stream>>>(
-        t->l_suppkey, t->l_orderkey, t->l_price, t->l_discount, t->n_lines, dim_s, t->n_supp, dim_o, t->n_orders,
-        reinterpret_cast<unsigned long long*>(nation_sums), &ctx->counters->range_errors, stage ? 1 : 0);
+        t->l_suppkey, t->l_orderkey, t->l_price, t->l_discount, t->n_lines, dim_s, t->n_supp, nib_s, nmask, dim_o,
+        t->n_orders, reinterpret_cast<unsigned long long*>(nation_sums), &ctx->counters->range_errors, stage);
   }
   OLAP_CUDA_TRY(ctx, cudaGetLastError());
   return OLAP_OK;

@@ -178,7 +178,7 @@ int oracle_gen_olapcore_compat(double sf, const double* sele, const int* bitmap,
   return 0;
 }
 
-/* ---- operators (config 2) ----------------------------------------------- */
+/* ---- operators: select, project, join, group-by, aggregation ----------- */
 
 enum { CMP_LE = 0, CMP_LT = 1 };
 static int cmp_pass(int32_t v, int32_t val, int cmp) { return cmp == CMP_LT ? v < val : v <= val; }

@@ -601,7 +601,7 @@ def main() -> None:
     plan = {name: knobs[k] for k, name in enumerate(
         ["block_threads", "blocks_per_sm", "smem_dim_bytes", "smem_acc_bytes", "host_chunk_rows",
          "rows_per_thread_mode", "probe_bits", "smem_bits_bytes", "group_combine", "group_plan", "async_loads", "compact",
-         "smem_nib_bytes", "host_inplace", "merge_probes"]) if knobs[k]}
+         "smem_nib_bytes", "host_inplace", "merge_probes", "probe_order"]) if knobs[k]}
 
     # kernels per query with this plan (the star-join and its staging prepasses)
     per_query = olapcore.launch_count(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,

@@ -78,6 +78,7 @@ extern "C" {
 #define OLAP_TUNE_HOST_INPLACE 13   /* _host star-join over pinned columns: 1 reads them in place
                                        (late materialisation over PCIe), 2 chunked copies (default) */
 #define OLAP_TUNE_MERGE_PROBES 14   /* star-join: 1 probes consecutive L2 int8 dimensions together, 2 off */
+#define OLAP_TUNE_PROBE_ORDER 15    /* star-join: 1 probes the dimensions staged as int8 last, 2 first */
 
 typedef struct olap_ctx olap_ctx;
 

@@ -50,6 +50,7 @@ TUNE_COMPACT = 11
 TUNE_SMEM_NIB_BYTES = 12
 TUNE_HOST_INPLACE = 13
 TUNE_MERGE_PROBES = 14
+TUNE_PROBE_ORDER = 15
 
 
 class OlapError(RuntimeError):

@@ -74,10 +74,13 @@ std::vector<Candidate> candidates(const olap_ctx* ctx, const olap_starjoin_query
     x.knob[OLAP_TUNE_BLOCK_THREADS] = 512;
     c.push_back(x);
   }
-  // ... and with consecutive L2 probes issued together (one round trip).
+  // ... and with consecutive L2 probes issued together (one round trip),
+  // also with the int8-staged dimensions probed last.
   for (size_t i = 0; i < n4; ++i) {
     Candidate x = c[i];
     x.knob[OLAP_TUNE_MERGE_PROBES] = 1;
+    c.push_back(x);
+    x.knob[OLAP_TUNE_PROBE_ORDER] = 1;
     c.push_back(x);
   }
   return c;
@@ -121,7 +124,7 @@ int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q, int64_t 
   for (int k : {OLAP_TUNE_BLOCK_THREADS, OLAP_TUNE_BLOCKS_PER_SM, OLAP_TUNE_SMEM_DIM_BYTES,
                 OLAP_TUNE_SMEM_ACC_BYTES, OLAP_TUNE_UNROLL, OLAP_TUNE_PROBE_BITS,
                 OLAP_TUNE_SMEM_BITS_BYTES, OLAP_TUNE_ASYNC_LOADS, OLAP_TUNE_COMPACT,
-                OLAP_TUNE_SMEM_NIB_BYTES, OLAP_TUNE_MERGE_PROBES})
+                OLAP_TUNE_SMEM_NIB_BYTES, OLAP_TUNE_MERGE_PROBES, OLAP_TUNE_PROBE_ORDER})
     saved[k] = 0;
   cudaEvent_t e0, e1;
   OLAP_CUDA_TRY(ctx, cudaEventCreate(&e0));

@@ -83,6 +83,7 @@ enum {
   TUNE_SMEM_NIB_BYTES = OLAP_TUNE_SMEM_NIB_BYTES,
   TUNE_HOST_INPLACE = OLAP_TUNE_HOST_INPLACE,
   TUNE_MERGE_PROBES = OLAP_TUNE_MERGE_PROBES,
+  TUNE_PROBE_ORDER = OLAP_TUNE_PROBE_ORDER,
 };
 
 int set_error(olap_ctx* ctx, int status, const std::string& msg);

@@ -856,8 +856,11 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   int out = 0;
   int64_t soff = 0;
   // Probe order: shared-memory int8, shared-memory 4-bit codes, shared-memory
-  // bitmaps, then the rest.
-  const int pass_kind[4] = {1, 4, 2, 0};
+  // bitmaps, then the rest; with TUNE_PROBE_ORDER = 1 the shared-memory int8
+  // dimensions go last (a dimension that filters nothing, such as the
+  // headline's date, is then looked up only for the rows that survive).
+  const bool int8_last = tune_or(ctx, TUNE_PROBE_ORDER, 2) == 1;
+  const int pass_kind[4] = {int8_last ? 4 : 1, int8_last ? 2 : 4, int8_last ? 0 : 2, int8_last ? 1 : 0};
   for (int pass = 0; pass < 4; ++pass) {
     for (int j = 0; j < nd; ++j) {
       const int kj = kind[j] == 3 ? 0 : kind[j];

@@ -195,6 +195,10 @@ def test_dimvec_len_pads_like_reference(ctx):
     {_lib.TUNE_MERGE_PROBES: 1},                          # consecutive L2 probes issued together
     {_lib.TUNE_MERGE_PROBES: 1, _lib.TUNE_SMEM_DIM_BYTES: 1, _lib.TUNE_SMEM_ACC_BYTES: 1},
     {_lib.TUNE_MERGE_PROBES: 1, _lib.TUNE_SMEM_NIB_BYTES: 16 * 1024, _lib.TUNE_UNROLL: 2},
+    {_lib.TUNE_PROBE_ORDER: 1},                           # int8-staged dimensions probed last
+    {_lib.TUNE_PROBE_ORDER: 1, _lib.TUNE_MERGE_PROBES: 1, _lib.TUNE_SMEM_NIB_BYTES: 200 * 1024},
+    {_lib.TUNE_PROBE_ORDER: 1, _lib.TUNE_COMPACT: 2, _lib.TUNE_SMEM_BITS_BYTES: 64 * 1024},
+    {_lib.TUNE_PROBE_ORDER: 1, _lib.TUNE_ASYNC_LOADS: 2, _lib.TUNE_SMEM_NIB_BYTES: 16 * 1024},
     {_lib.TUNE_SMEM_NIB_BYTES: 200 * 1024},               # 4-bit codes staged in smem
     {_lib.TUNE_SMEM_NIB_BYTES: 16 * 1024, _lib.TUNE_SMEM_BITS_BYTES: 64 * 1024, _lib.TUNE_BLOCK_THREADS: 1024},
     {_lib.TUNE_SMEM_NIB_BYTES: 200 * 1024, _lib.TUNE_SMEM_DIM_BYTES: 1, _lib.TUNE_UNROLL: 2},

@@ -229,11 +229,12 @@ def run_batched(a) -> None:
         eng.run(qs, s.fk, s.m1, s.m2, out=out, totals=tot)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for qs in batches:
-        eng.run(qs, s.fk, s.m1, s.m2, out=out, totals=tot)
-    e1.record()
-    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        e0.record()
+        for qs in batches:
+            eng.run(qs, s.fk, s.m1, s.m2, out=out, totals=tot)
+        e1.record()
+        torch.cuda.synchronize()
     b_ms = e0.elapsed_time(e1) / len(batches)
     # one launch per query (dimension vectors + plain star-join), same queries
     vec_bufs = [torch.empty(n, dtype=torch.int8, device="cuda") for n in DIM_SIZES]
@@ -254,7 +255,7 @@ def run_batched(a) -> None:
     line = {"metric": "batched star-join queries/sec", "value": a.queries / (b_ms / 1e3), "unit": "queries/s",
             "n_gpus": 1, "steps": len(batches), "warmup": a.warmup, "ms_per_batch": b_ms,
             "plain_ms_per_batch": p_ms, "plain_queries_per_s": a.queries / (p_ms / 1e3),
-            "speedup_vs_one_launch_per_query": p_ms / b_ms, "higher_is_better": True,
+            "speedup_vs_one_launch_per_query": p_ms / b_ms, "higher_is_better": True, "clocks": clk.summary(),
             "config": {"workload": f"{a.queries} star-join queries per batch over the shared {a.rows:,}-row table "
                                    "(joint selectivity log-uniform [1e-4, 0.3], 1-3 group tables of 25/25/40/7, "
                                    "fact range 5-100%), one persistent launch per batch replayed as a CUDA graph",
@@ -388,6 +389,7 @@ def run_operators(a) -> None:
         return d
 
     res = []
+    clk = ClockSampler(0).__enter__()  # sampled over every operator's timing
     col = gen(n, 100, 0, (1 << 20) - 1)
     cols4 = [gen(n, 101 + c, -1000, 1000) for c in range(4)]
     ids = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -472,9 +474,11 @@ def run_operators(a) -> None:
         ok = k == int((ec > 0).sum()) and torch.equal(gs, es) and torch.equal(gc, ec)
         res.append(entry("hash group-by SUM/COUNT", ms, 8 * n, ok, groups=G))
         del keys, ok_, os_, oc_
+    clk.__exit__(None, None, None)
     line = {"metric": "operator rows/sec and HBM GB/s vs peak", "value": min(r["frac_of_peak"] for r in res),
             "unit": "min fraction of peak over the operators", "n_gpus": 1, "rows": n, "operators": res,
             "peak_GBs": peak, "peak_source": peak_src, "all_checked": all(r["checked"] for r in res),
+            "clocks": clk.summary(),
             "config": {"workload": f"operator set at {n:,} int32 rows (select at 0.001/0.01/0.1/0.5, gather of 4 "
                                    "columns, hash join 2^24 build / uniform and Zipf(1.0) probes at 50% match, "
                                    "hash group-by at 16/4096/2^20/2^22 groups)"},

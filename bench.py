@@ -519,7 +519,7 @@ def run_hostscan(a) -> None:
                 dims.append(c)
             row = {"pass_rates": list(sele)}
             outs = []
-            for mode, knob in (("inplace", 1), ("copy", 2)):
+            for mode, knob in (("inplace", 0), ("copy", 2)):  # 0: the default call
                 ctx.set_tuning(_lib.TUNE_HOST_INPLACE, knob)
 
                 def call():
@@ -735,7 +735,7 @@ def e2e_host(a, s, ctx, aggs, world, knobs) -> dict:
 
     def measure(mode):
         nonlocal ref
-        hctx.set_tuning(_lib.TUNE_HOST_INPLACE, 1 if mode == "inplace" else 2)
+        hctx.set_tuning(_lib.TUNE_HOST_INPLACE, 0 if mode == "inplace" else 2)  # 0: the default call
         out = run()
         if ref is None:
             ref = out
@@ -762,10 +762,11 @@ def e2e_host(a, s, ctx, aggs, world, knobs) -> dict:
     hctx.close()
     chunk = 1 << 22
     launches = {"inplace": 1 + s.dimvec_nums, "copy": (n + chunk - 1) // chunk}
-    paths = {"inplace": "olap_starjoin_groupsum_host with OLAP_TUNE_HOST_INPLACE=1: one kernel reads the pinned "
+    paths = {"inplace": "olap_starjoin_groupsum_host, default plan for pinned columns: one kernel reads the pinned "
                         "host columns in place over PCIe, the most selective dimension's keys whole and every "
                         "later column only for rows still alive (32-byte sectors counted on the device)",
-             "copy": "olap_starjoin_groupsum_host, pinned host columns, chunked H2D copies overlapped with the scan"}
+             "copy": "olap_starjoin_groupsum_host with OLAP_TUNE_HOST_INPLACE=2: pinned host columns, chunked H2D "
+                     "copies overlapped with the scan"}
     return {"value": n * world / dt, "unit": "rows/s", "h2d_bytes_per_step": h2d,
             # group sums, totals, the dropped-row count (+ the dimensions' pass counts in place)
             "d2h_bytes_per_step": 8 * 2 * G + 16 + 8 + (32 if a.e2e_mode == "inplace" else 0),

@@ -1125,7 +1125,9 @@ int starjoin_host(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   OLAP_REQUIRE(ctx, rows == 0 || !need_m1 || q->m1, "M1 column required by the aggregate");
   OLAP_REQUIRE(ctx, rows == 0 || !need_m2 || q->m2, "M2 column required by the aggregate");
 
-  if (tune_or(ctx, TUNE_HOST_INPLACE, 2) == 1 && rows > 0) {
+  // Pinned columns are read in place unless TUNE_HOST_INPLACE = 2 asks for
+  // the chunked copies (whose dropped-row count covers every key).
+  if (tune_or(ctx, TUNE_HOST_INPLACE, 1) == 1 && rows > 0) {
     bool handled = false;
     const int s = starjoin_host_inplace(ctx, q, group_sums, totals, &handled);
     if (handled) return s;

@@ -1,6 +1,7 @@
-"""GPU parity tests of the in-place host scan (OLAP_TUNE_HOST_INPLACE = 1):
-olap_starjoin_groupsum_host reading pinned host columns where they are, the
-most selective dimension first.  Sums and totals must equal the oracle's bit
+"""GPU parity tests of the in-place host scan (the default of
+olap_starjoin_groupsum_host for pinned columns, OLAP_TUNE_HOST_INPLACE = 1):
+the host call reading pinned host columns where they are, the most
+selective dimension first.  Sums and totals must equal the oracle's bit
 for bit; the dropped-row count must equal the count of the keys the scan
 reads (restated below in numpy); pageable or differently aligned columns
 must fall back to the chunked copies with the oracle's exact count."""

@@ -235,7 +235,7 @@ def test_host_entry_point_matches_device(ctx):
     finally:
         ctx.set_tuning(_lib.TUNE_HOST_CHUNK_ROWS, 0)
     assert np.array_equal(h_gs, o_gs) and np.array_equal(h_tot, o_tot)
-    # pinned host buffers take the direct-DMA path
+    # pinned host buffers are read in place (the default for pinned columns)
     pin = [torch.from_numpy(f).pin_memory() for f in fks]
     pm1, pm2 = torch.from_numpy(m1).pin_memory(), torch.from_numpy(m2).pin_memory()
     h_gs2, h_tot2 = olapcore.starjoin_groupsum(dvs, [p.numpy() for p in pin], factor, pm1.numpy(),

@@ -176,3 +176,26 @@ def test_inplace_falls_back_to_copies(inplace):
     st, dropped, gs, tot = run_host(ctx, dv, cols[:4], factor, cols[4], cols[5], G, aggs, (0, n))
     assert dropped == o_err and np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
     assert ctx.take_host_bytes() == n * 4 * 6 + sum(len(d) for d in dv)
+
+
+def test_copies_forced_for_pinned_columns(ctx):
+    """OLAP_TUNE_HOST_INPLACE = 2: pinned columns take the chunked copies,
+    with the oracle's exact dropped-row count and every byte copied."""
+    n = 300_001
+    dv, fk, m1, m2 = random_star(17, n, SIZES, SELE, GROUPS, key_lo=-2, key_hi_extra=3)
+    factor = [int(np.prod(GROUPS[j + 1:])) for j in range(4)]
+    G = int(np.prod(GROUPS))
+    aggs = (AGG_M1, AGG_M1_TIMES_M2)
+    hold = [pinned(f) for f in fk] + [pinned(m1), pinned(m2)]
+    o_gs, o_tot, o_err = oracle.starjoin(dv, fk, factor, m1, m2, G, aggs=aggs)
+    ctx.set_tuning(_lib.TUNE_HOST_INPLACE, 2)
+    ctx.take_host_bytes()
+    try:
+        st, dropped, gs, tot = run_host(ctx, dv, [h[1] for h in hold[:4]], factor, hold[4][1], hold[5][1], G,
+                                        aggs, (0, n))
+        moved = ctx.take_host_bytes()
+    finally:
+        ctx.set_tuning(_lib.TUNE_HOST_INPLACE, 0)
+    assert st == _lib.OLAP_ERR_RANGE and dropped == o_err > 0
+    assert np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
+    assert moved == n * 4 * 6 + sum(len(d) for d in dv)

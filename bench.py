@@ -519,7 +519,7 @@ def run_hostscan(a) -> None:
                 dims.append(c)
             row = {"pass_rates": list(sele)}
             outs = []
-            for mode, knob in (("inplace", 0), ("copy", 2)):  # 0: the default call
+            for mode, knob in (("inplace", 3), ("copy", 2)):  # each path forced
                 ctx.set_tuning(_lib.TUNE_HOST_INPLACE, knob)
 
                 def call():

@@ -76,7 +76,9 @@ extern "C" {
 #define OLAP_TUNE_COMPACT 11        /* star-join: 2 compacts survivors per warp before global probes, 1 off */
 #define OLAP_TUNE_SMEM_NIB_BYTES 12 /* bytes of 4-bit code vectors staged in smem (default 0)        */
 #define OLAP_TUNE_HOST_INPLACE 13   /* _host star-join over pinned columns: 1 reads them in place
-                                       (late materialisation over PCIe; default), 2 chunked copies */
+                                       (late materialisation over PCIe) when the filters promise to
+                                       read at most 85 % of the bytes (default), 2 chunked copies,
+                                       3 in place always */
 #define OLAP_TUNE_MERGE_PROBES 14   /* star-join: 1 probes consecutive L2 int8 dimensions together, 2 off */
 #define OLAP_TUNE_PROBE_ORDER 15    /* star-join: 1 probes the dimensions staged as int8 last, 2 first */
 
@@ -154,12 +156,13 @@ OLAP_API int olap_starjoin_launch_count(olap_ctx* ctx, const olap_starjoin_query
 
 /* Host pointers; synchronous.  The fact columns are streamed through the GPU
  * in pinned chunks with copies overlapped with the scan.  When every column
- * is in pinned (device-mapped) host memory at one 16-byte phase, one kernel
- * reads the columns in place instead (unless OLAP_TUNE_HOST_INPLACE = 2): the
- * foreign keys of the dimension that drops the most rows first, each later
- * column only for the rows still alive (late materialisation over PCIe); its
- * dropped-row count then covers the keys it read, while the sums are the
- * same.  A dimvec_len[j] of
+ * is in pinned (device-mapped) host memory at one 16-byte phase and the
+ * dimensions' pass fractions promise to read at most 85 % of the columns'
+ * bytes, one kernel reads the columns in place instead (OLAP_TUNE_HOST_INPLACE
+ * 2 forces the copies, 3 the in-place read): the foreign keys of the
+ * dimension that drops the most rows first, each later column only for the
+ * rows still alive (late materialisation over PCIe); its dropped-row count
+ * then covers the keys it read, while the sums are the same.  A dimvec_len[j] of
  * 0 means "unknown": the library then copies dimvec[j][0 .. max fk] (the
  * bytes the reference itself would read).  Returns OLAP_ERR_RANGE (results
  * still written) when rows were dropped. */

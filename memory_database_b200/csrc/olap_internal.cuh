@@ -128,10 +128,12 @@ int starjoin_device(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_
 // copies the query's host dimension vectors into `ar` (a dimvec_len of 0 is
 // resolved from the largest key) and points dq at the copies.
 int stage_host_dims(olap_ctx* ctx, const olap_starjoin_query* q, Arena& ar, olap_starjoin_query* dq);
-// In-place scan of pinned host columns; *handled is false (and nothing ran)
-// when a column is not device-mapped or the columns' 16-byte phases differ.
-int starjoin_host_inplace(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_sums,
-                          int64_t* totals, bool* handled);
+// In-place scan of pinned host columns (dq: the query with its dimension
+// vectors staged in `ar`); *handled is false (and nothing ran) when a column
+// is not device-mapped, the columns' 16-byte phases differ, or the
+// dimensions' pass fractions promise too little saving over the copies.
+int starjoin_host_inplace(olap_ctx* ctx, const olap_starjoin_query* q, const olap_starjoin_query& dq, Arena& ar,
+                          int64_t* group_sums, int64_t* totals, bool* handled);
 
 inline int64_t tune_or(const olap_ctx* c, int knob, int64_t dflt) {
   return c->tune[knob] > 0 ? c->tune[knob] : dflt;

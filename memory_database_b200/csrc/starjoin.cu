@@ -1125,17 +1125,19 @@ int starjoin_host(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   OLAP_REQUIRE(ctx, rows == 0 || !need_m1 || q->m1, "M1 column required by the aggregate");
   OLAP_REQUIRE(ctx, rows == 0 || !need_m2 || q->m2, "M2 column required by the aggregate");
 
-  // Pinned columns are read in place unless TUNE_HOST_INPLACE = 2 asks for
-  // the chunked copies (whose dropped-row count covers every key).
-  if (tune_or(ctx, TUNE_HOST_INPLACE, 1) == 1 && rows > 0) {
-    bool handled = false;
-    const int s = starjoin_host_inplace(ctx, q, group_sums, totals, &handled);
-    if (handled) return s;
-  }
   Arena ar(ctx);
   olap_starjoin_query dq = *q;
   const int sd = stage_host_dims(ctx, q, ar, &dq);
   if (sd != OLAP_OK) return sd;
+  // Pinned columns are read in place (1: when that reads fewer bytes, the
+  // default; 3: always) unless TUNE_HOST_INPLACE = 2 asks for the chunked
+  // copies (whose dropped-row count covers every key).
+  const int64_t inplace = tune_or(ctx, TUNE_HOST_INPLACE, 1);
+  if ((inplace == 1 || inplace == 3) && rows > 0) {
+    bool handled = false;
+    const int s = starjoin_host_inplace(ctx, q, dq, ar, group_sums, totals, &handled);
+    if (handled) return s;
+  }
   const int64_t nacc = q->group_nums * q->n_aggs;
   int64_t* dsum = group_sums ? ar.take<int64_t>(static_cast<size_t>(nacc)) : nullptr;
   int64_t* dtot = ar.take<int64_t>(2);

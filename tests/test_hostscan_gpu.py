@@ -1,5 +1,6 @@
 """GPU parity tests of the in-place host scan (the default of
-olap_starjoin_groupsum_host for pinned columns, OLAP_TUNE_HOST_INPLACE = 1):
+olap_starjoin_groupsum_host for pinned columns when it reads fewer bytes;
+OLAP_TUNE_HOST_INPLACE = 3 forces it):
 the host call reading pinned host columns where they are, the most
 selective dimension first.  Sums and totals must equal the oracle's bit
 for bit; the dropped-row count must equal the count of the keys the scan
@@ -82,7 +83,7 @@ def run_host(ctx, dvs, fks, factors, m1, m2, G, aggs, row_range):
 
 @pytest.fixture
 def inplace(ctx):
-    ctx.set_tuning(_lib.TUNE_HOST_INPLACE, 1)
+    ctx.set_tuning(_lib.TUNE_HOST_INPLACE, 3)  # in place whatever the filters
     ctx.take_host_bytes()
     yield ctx
     ctx.set_tuning(_lib.TUNE_HOST_INPLACE, 0)
@@ -199,3 +200,26 @@ def test_copies_forced_for_pinned_columns(ctx):
     assert st == _lib.OLAP_ERR_RANGE and dropped == o_err > 0
     assert np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
     assert moved == n * 4 * 6 + sum(len(d) for d in dv)
+
+
+def test_default_takes_copies_when_nothing_is_filtered(ctx):
+    """The default reads in place only when the filters save bytes: with
+    every dimension entry passing, the call copies the columns (every byte
+    moved once), and with the headline's filters it reads a third of them."""
+    n = 400_003
+    sele = [1.0, 1.0, 1.0, 1.0]
+    dv, fk, m1, m2 = random_star(23, n, SIZES, sele, GROUPS)
+    factor = [int(np.prod(GROUPS[j + 1:])) for j in range(4)]
+    G = int(np.prod(GROUPS))
+    hold = [pinned(f) for f in fk] + [pinned(m1), pinned(m2)]
+    cols = [h[1] for h in hold]
+    o_gs, o_tot, _ = oracle.starjoin(dv, fk, factor, m1, m2, G)
+    ctx.take_host_bytes()
+    st, dropped, gs, tot = run_host(ctx, dv, cols[:4], factor, cols[4], cols[5], G, (AGG_M1_PLUS_M2,), (0, n))
+    assert st == 0 and np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
+    assert ctx.take_host_bytes() == n * 4 * 6 + sum(len(d) for d in dv)
+    dv2, _, _, _ = random_star(23, 1, SIZES, SELE, GROUPS)
+    o_gs, o_tot, _ = oracle.starjoin(dv2, fk, factor, m1, m2, G)
+    st, dropped, gs, tot = run_host(ctx, dv2, cols[:4], factor, cols[4], cols[5], G, (AGG_M1_PLUS_M2,), (0, n))
+    assert st == 0 and np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
+    assert ctx.take_host_bytes() < 0.5 * n * 4 * 6

@@ -1,7 +1,8 @@
 """Regenerate the golden fixtures of the OLAP-core star-join.
 
-Run in a container that holds the reference tree (read-only) at
-/root/reference; the GPU tests and the bench read only the JSON written here.
+Run where the reference tree is present (read only; its location is
+$OLAP_REFERENCE_TREE); the GPU tests and the bench read only the JSON
+written here.
 
 * ``olapcore_queries.json`` — the ten query parameterisations of the
   reference's ``OLAPcore.sh`` (lines 3-12), parsed from that script, each
@@ -18,6 +19,7 @@ Usage:  python tests/golden/make_golden.py
 from __future__ import annotations
 
 import json
+import os
 import re
 import sys
 from pathlib import Path
@@ -28,7 +30,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 import oracle  # noqa: E402  (test infrastructure)
 
-REF = Path("/root/reference")
+REF = Path(os.environ.get("OLAP_REFERENCE_TREE", "/root/reference"))
 OUT = Path(__file__).resolve().parent
 FLAGS = ["d-sele", "d-bitmap", "d-groups", "s-sele", "s-bitmap", "s-groups", "p-sele",
          "p-bitmap", "p-groups", "c-sele", "c-bitmap", "c-groups", "sqlnum"]

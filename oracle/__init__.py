@@ -9,6 +9,7 @@ only where it was built.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -17,7 +18,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_OLAPCORE_SO = HERE / "_ref" / "libref_olapcore.so"
-REFERENCE_TREE = Path("/root/reference")
+# where the reference tree is read from when it is present (OLAP_REFERENCE_TREE)
+REFERENCE_TREE = Path(os.environ.get("OLAP_REFERENCE_TREE", "/root/reference"))
 
 _vp, _i64, _i32 = C.c_void_p, C.c_int64, C.c_int32
 
@@ -29,7 +31,7 @@ def build(with_reference: bool | None = None) -> None:
         with_reference = REFERENCE_TREE.exists()
     if with_reference:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE), f"OLAP_REFERENCE_TREE={REFERENCE_TREE}", *targets], check=True)
 
 
 def _load_oracle() -> C.CDLL:
@@ -39,9 +41,23 @@ def _load_oracle() -> C.CDLL:
     lib.oracle_plan.argtypes = [_vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_int), C.POINTER(_i64)]
     lib.oracle_starjoin.argtypes = [C.c_int, _vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp, C.c_int,
                                     _vp, _i64, _vp, _vp, C.POINTER(_i64)]
+    lib.oracle_starjoin_mt.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp, C.c_int,
+                                       _vp, _i64, _vp, _vp, C.POINTER(_i64)]
+    lib.oracle_starjoin_mt.restype = C.c_int
+    lib.oracle_hashjoin_sum_mt.argtypes = [C.c_int, _vp, _vp, _i64, _vp, _i64, C.POINTER(_i64)]
+    lib.oracle_hashjoin_sum_mt.restype = _i64
+    lib.oracle_gen_uniform_i32.argtypes = [_vp, _i64, C.c_uint64, C.c_uint64, _i32, _i32, C.c_int]
+    lib.oracle_gen_uniform_i32.restype = C.c_int
+    lib.oracle_gen_dimvec.argtypes = [_vp, _i64, C.c_uint64, C.c_uint64, C.c_double, _i32, C.c_int]
+    lib.oracle_gen_dimvec.restype = C.c_int
+    lib.oracle_gen_zipf_i32.argtypes = [_vp, _i64, C.c_uint64, C.c_uint64, _i64, C.c_double, C.c_int]
+    lib.oracle_gen_zipf_i32.restype = C.c_int
     lib.oracle_size_of_table.argtypes = [C.c_int, C.c_double]
     lib.oracle_size_of_table.restype = C.c_int
     lib.oracle_gen_olapcore_compat.argtypes = [C.c_double, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    lib.oracle_gen_olapcore_compat.restype = C.c_int
+    lib.oracle_glibc_rand_stream.argtypes = [C.c_uint32, _i64, _vp]
+    lib.oracle_glibc_rand_stream.restype = C.c_int
     lib.oracle_select_rowids.argtypes = [_vp, _i64, _i32, C.c_int, _vp, _i64, _vp, C.POINTER(_i64)]
     lib.oracle_select_rowids.restype = _i64
     lib.oracle_select_bitmap.argtypes = [_vp, _i64, _i32, C.c_int, _vp]
@@ -86,25 +102,57 @@ def ref_available() -> bool:
     return REF_OLAPCORE_SO.exists()
 
 
+def host_has_x86_64_v4() -> bool:
+    """Whether this host's CPU has the AVX-512 features of x86-64-v4."""
+    try:
+        flags = set()
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("flags"):
+                flags = set(line.split(":", 1)[1].split())
+                break
+        return {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags
+    except OSError:
+        return False
+
+
+_REF_V4: C.CDLL | None = None
+
+
+def ref_lib_for_host() -> tuple[C.CDLL, str]:
+    """The reference's OLAPcore built for this host's CPU: the x86-64-v4
+    (AVX-512) build where the CPU has it, else the x86-64-v3 one.  Returns
+    (library, build flags)."""
+    global _REF_V4
+    v4 = HERE / "_ref" / "libref_olapcore_v4.so"
+    if host_has_x86_64_v4() and v4.exists():
+        if _REF_V4 is None:
+            _REF_V4 = _bind_ref_olapcore(C.CDLL(str(v4)))
+        return _REF_V4, "-O3 -march=x86-64-v4"
+    return ref_lib(), "-O3 -march=x86-64-v3"
+
+
 def ref_lib() -> C.CDLL:
     """The reference's own OLAPcore functions (built from its sources)."""
     global _REF
     if _REF is None:
         if not REF_OLAPCORE_SO.exists():
             raise FileNotFoundError(f"{REF_OLAPCORE_SO} not built (needs the reference tree)")
-        lib = C.CDLL(str(REF_OLAPCORE_SO))
-        fan = [_vp, _vp, _vp, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, C.c_int]
-        for name in ("ref_OLAPcore_rowwise", "ref_OLAPcore_vwm_dv", "ref_OLAPcore_vwm_sv",
-                     "ref_OLAPcore_cwm_dv"):
-            getattr(lib, name).argtypes = fan
-            getattr(lib, name).restype = C.c_int
-        lib.ref_OLAPcore_cwm_sv.argtypes = fan[:-1] + [_vp, C.c_int]
-        lib.ref_OLAPcore_cwm_sv.restype = C.c_int
-        lib.ref_vwm_sv_groups.argtypes = [_vp, _vp, _vp, C.c_int, _vp, _i64, _i64, _vp, _vp, _vp]
-        lib.ref_row_groups.argtypes = [_vp, _vp, _vp, C.c_int, _vp, _i64, _vp, _vp, _vp]
-        lib.ref_gen_data_olapcore.argtypes = [C.c_double, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
-        _REF = lib
+        _REF = _bind_ref_olapcore(C.CDLL(str(REF_OLAPCORE_SO)))
     return _REF
+
+
+def _bind_ref_olapcore(lib: C.CDLL) -> C.CDLL:
+    fan = [_vp, _vp, _vp, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, C.c_int]
+    for name in ("ref_OLAPcore_rowwise", "ref_OLAPcore_vwm_dv", "ref_OLAPcore_vwm_sv",
+                 "ref_OLAPcore_cwm_dv"):
+        getattr(lib, name).argtypes = fan
+        getattr(lib, name).restype = C.c_int
+    lib.ref_OLAPcore_cwm_sv.argtypes = fan[:-1] + [_vp, C.c_int]
+    lib.ref_OLAPcore_cwm_sv.restype = C.c_int
+    lib.ref_vwm_sv_groups.argtypes = [_vp, _vp, _vp, C.c_int, _vp, _i64, _i64, _vp, _vp, _vp]
+    lib.ref_row_groups.argtypes = [_vp, _vp, _vp, C.c_int, _vp, _i64, _vp, _vp, _vp]
+    lib.ref_gen_data_olapcore.argtypes = [C.c_double, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    return lib
 
 
 def _p(a: np.ndarray) -> int:
@@ -131,8 +179,9 @@ def plan(sele, bitmap, groups):
 
 
 def starjoin(dimvecs, fks, factors, m1, m2, group_nums, aggs=(0,), row_range=None,
-             dim_lens=None, want_groups=True):
-    """Oracle star-join over dimensions in probe order.
+             dim_lens=None, want_groups=True, nthreads=1):
+    """Oracle star-join over dimensions in probe order (row ranges over
+    ``nthreads`` host threads when it is above 1; same result).
 
     Returns (group_sums[n_aggs, group_nums] int64 or None, totals[n_aggs], range_errors)."""
     lib = oracle_lib()
@@ -149,27 +198,107 @@ def starjoin(dimvecs, fks, factors, m1, m2, group_nums, aggs=(0,), row_range=Non
     gs = np.zeros((len(aggs), group_nums), np.int64) if want_groups else None
     tot = np.zeros(len(aggs), np.int64)
     err = _i64()
-    lib.oracle_starjoin(nd, _ptr_array(dv), _p(lens), _ptr_array(fk), _p(fac), rb, re,
-                        None if m1a is None else _p(m1a), None if m2a is None else _p(m2a),
-                        len(aggs), _p(ag), group_nums, None if gs is None else _p(gs), _p(tot),
-                        C.byref(err))
+    args = (nd, _ptr_array(dv), _p(lens), _ptr_array(fk), _p(fac), rb, re,
+            None if m1a is None else _p(m1a), None if m2a is None else _p(m2a),
+            len(aggs), _p(ag), group_nums, None if gs is None else _p(gs), _p(tot), C.byref(err))
+    if nthreads > 1:
+        assert lib.oracle_starjoin_mt(int(nthreads), *args) == 0
+    else:
+        lib.oracle_starjoin(*args)
     return gs, tot, err.value
+
+
+# ---- the benchmark's seeded tables (host copies of the library's generators) ----
+
+def gen_uniform_i32(n, seed, stream, lo, hi, nthreads=0):
+    out = np.empty(max(n, 1), np.int32)
+    assert oracle_lib().oracle_gen_uniform_i32(_p(out), n, seed, stream, lo, hi, _threads(nthreads)) == 0
+    return out[:n]
+
+
+def gen_dimvec(n, seed, stream, sele, groups, nthreads=0):
+    out = np.empty(max(n, 1), np.int8)
+    assert oracle_lib().oracle_gen_dimvec(_p(out), n, seed, stream, float(sele), int(groups),
+                                          _threads(nthreads)) == 0
+    return out[:n]
+
+
+def gen_zipf_i32(n, seed, stream, n_keys, s, nthreads=0):
+    out = np.empty(max(n, 1), np.int32)
+    assert oracle_lib().oracle_gen_zipf_i32(_p(out), n, seed, stream, n_keys, float(s), _threads(nthreads)) == 0
+    return out[:n]
+
+
+def _threads(n):
+    import os
+    return int(n) if n and n > 0 else (os.cpu_count() or 1)
+
+
+class StarTables:
+    """A star schema in host memory (numpy), with the reference main's plan."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+    @property
+    def probe_dims(self):
+        return [self.dimvec[t] for t in self.orders]
+
+    @property
+    def probe_fks(self):
+        return [self.fk[t] for t in self.orders]
+
+
+def star_schema(n_rows, dim_sizes, sele, groups, bitmap=(1, 1, 1, 1), m_range=(1, 10_000), fk_dist="uniform",
+                zipf_s=0.8, seed=42, fact_seed=None, nthreads=0):
+    """The benchmark's star schema, bit-identical to the tables the GPU
+    library generates for the same arguments (streams: foreign keys of table
+    t -> 10 + t, M1 -> 20, M2 -> 21, dimension vector of table t -> 30 + t;
+    ``fact_seed``, default ``seed``, seeds the fact columns)."""
+    fseed = seed if fact_seed is None else fact_seed
+    dimvec, fk = [], []
+    for t in range(4):
+        g = max(1, int(groups[t])) if bitmap[t] else 1
+        dimvec.append(gen_dimvec(dim_sizes[t], seed, 30 + t, sele[t], g, nthreads))
+        if fk_dist == "zipf":
+            fk.append(gen_zipf_i32(n_rows, fseed, 10 + t, dim_sizes[t], zipf_s, nthreads))
+        else:
+            fk.append(gen_uniform_i32(n_rows, fseed, 10 + t, 0, dim_sizes[t] - 1, nthreads))
+    m1 = gen_uniform_i32(n_rows, fseed, 20, m_range[0], m_range[1], nthreads)
+    m2 = gen_uniform_i32(n_rows, fseed, 21, m_range[0], m_range[1], nthreads)
+    orders, factor, nd, gn = plan(sele, bitmap, groups)
+    return StarTables(n_rows=n_rows, dim_sizes=tuple(dim_sizes), dimvec=dimvec, fk=fk, m1=m1, m2=m2,
+                      orders=orders, factor=factor, dimvec_nums=nd, group_nums=gn)
 
 
 def size_of_table(table: int, sf: float) -> int:
     return int(oracle_lib().oracle_size_of_table(table, sf))
 
 
-def gen_olapcore_compat(sf, sele, bitmap, groups, use_reference=False):
+def glibc_rand_stream(seed: int, n: int) -> np.ndarray:
+    """The first n values of glibc's rand() after srand(seed), restated."""
+    out = np.zeros(max(n, 1), np.int32)
+    assert oracle_lib().oracle_glibc_rand_stream(int(seed), int(n), _p(out)) == 0
+    return out[:n]
+
+
+def gen_olapcore_compat(sf, sele, bitmap, groups, use_reference=False, measures=True, fk_out=None):
     """The reference's OLAPcore dataset (glibc rand() from its default seed).
 
-    Returns (dimvecs[4] with size+1 bytes each, fks[4], m1, m2)."""
+    Returns (dimvecs[4] with size+1 bytes each, fks[4], m1, m2); m1 and m2
+    (constant 5) are None when ``measures`` is false.  ``fk_out``: four
+    int32 arrays of the table's row count to fill instead of new ones."""
     sizes = [size_of_table(t, sf) for t in range(4)]
     n = size_of_table(4, sf)
     dv = [np.zeros(s + 1, np.int8) for s in sizes]
-    fk = [np.zeros(n, np.int32) for _ in range(4)]
-    m1 = np.zeros(n, np.int32)
-    m2 = np.zeros(n, np.int32)
+    if fk_out is not None:
+        assert len(fk_out) == 4 and all(f.dtype == np.int32 and len(f) == n and f.flags["C_CONTIGUOUS"]
+                                        for f in fk_out)
+        fk = list(fk_out)
+    else:
+        fk = [np.empty(n, np.int32) for _ in range(4)]
+    m1 = np.zeros(n, np.int32) if measures or use_reference else None
+    m2 = np.zeros(n, np.int32) if measures or use_reference else None
     s = np.ascontiguousarray(sele, dtype=np.float64)
     b = np.ascontiguousarray(bitmap, dtype=np.int32)
     g = np.ascontiguousarray(groups, dtype=np.int32)
@@ -177,8 +306,10 @@ def gen_olapcore_compat(sf, sele, bitmap, groups, use_reference=False):
         ref_lib().ref_gen_data_olapcore(float(sf), _p(s), _p(b), _p(g), _ptr_array(dv),
                                         _ptr_array(fk), _p(m1), _p(m2))
     else:
-        oracle_lib().oracle_gen_olapcore_compat(float(sf), _p(s), _p(b), _p(g), _ptr_array(dv),
-                                                _ptr_array(fk), _p(m1), _p(m2))
+        rc = oracle_lib().oracle_gen_olapcore_compat(float(sf), _p(s), _p(b), _p(g), _ptr_array(dv),
+                                                     _ptr_array(fk), None if m1 is None else _p(m1),
+                                                     None if m2 is None else _p(m2))
+        assert rc == 0
     return dv, fk, m1, m2
 
 
@@ -248,6 +379,16 @@ def hashjoin(rk, rp, sk, want_pairs=False):
                                      None if rows is None else _p(rows), None if pay is None else _p(pay))
     if want_pairs:
         return s, m.value, rows[: m.value], pay[: m.value]
+    return s, m.value
+
+
+def hashjoin_sum(rk, rp, sk, nthreads=1):
+    """(SUM of matched payloads, matches) of the hash join, the probe side
+    over ``nthreads`` host threads."""
+    rk, rp, sk = _c32(rk), _c32(rp), _c32(sk)
+    m = _i64()
+    s = oracle_lib().oracle_hashjoin_sum_mt(int(nthreads), _p(rk), _p(rp), len(rk), _p(sk), len(sk), C.byref(m))
+    assert m.value >= 0
     return s, m.value
 
 

@@ -21,8 +21,11 @@
 //    Calls whose work overlaps on the GPU (different streams, or different
 //    host threads without ordering) race on the array and must be avoided.
 //  * The first call on each device looks up the array's device address with
-//    cudaGetSymbolAddress (with that device current) and caches it; make that
-//    first call before any stream capture.
+//    cudaGetSymbolAddress (with that device current) and caches it for the
+//    life of the process; make that first call before any stream capture.
+//    The device must not be reset between calls (cudaDeviceReset, or a
+//    teardown of its primary context): the cached address would then belong
+//    to a context that no longer exists.
 //  * No cudaMalloc, cudaFree or other allocation of device or pinned memory is
 //    made; inputs and outputs are the caller's device pointers.
 #include <cstring>

@@ -9,6 +9,8 @@ query too large for its fixed scratch must be refused.  This file is
 collected last so that a run stopping at its first failure has already run
 every other test; it also passes on its own in a fresh process."""
 import ctypes as C
+import re
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -18,7 +20,10 @@ from memory_database_b200 import _lib, olapcore
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
-OLAP_NOALLOC_MAX_DIM_ENTRIES = 8_000_000
+# the limit as the C header states it, so that the boundary cases below
+# follow the header if it changes
+_HEADER = (Path(__file__).resolve().parents[1] / "include" / "olap_capi.h").read_text()
+OLAP_NOALLOC_MAX_DIM_ENTRIES = int(re.search(r"#define OLAP_NOALLOC_MAX_DIM_ENTRIES (\d+)", _HEADER).group(1))
 
 
 def _fn():
@@ -66,6 +71,31 @@ def test_noalloc_matches_context_entry_point_twice_in_a_row():
         torch.cuda.synchronize()
         assert torch.equal(gs, ref_gs) and torch.equal(tot, ref_tot)
         assert int(err.item()) == ref_err
+
+
+def test_noalloc_accepts_exactly_its_maximum():
+    """Dimension vectors of exactly OLAP_NOALLOC_MAX_DIM_ENTRIES entries in
+    total: their pass bitmaps, alignment padding and counters must fit the
+    static scratch, and the sums equal the context entry point's."""
+    per = OLAP_NOALLOC_MAX_DIM_ENTRIES // 4
+    sizes = [per, per, per, OLAP_NOALLOC_MAX_DIM_ENTRIES - 3 * per]
+    groups, sele = [8, 8, 8, 8], [0.5, 0.3, 0.2, 0.9]
+    orders, factor, nd, G = olapcore.plan_olapcore(sele, [1] * 4, groups)
+    dv, fk, m1, m2 = _star(9, 1_000_003, sizes, sele, groups)
+    dims, fks = [dv[t] for t in orders], [fk[t] for t in orders]
+    aggs = (olapcore.AGG_M1_PLUS_M2,)
+    with olapcore.Context(0) as ctx:
+        ref_gs, ref_tot = olapcore.starjoin_groupsum(dims, fks, factor, m1, m2, G, aggs=aggs, ctx=ctx)
+        torch.cuda.synchronize()
+        ref_err = ctx.take_range_errors()
+    q = olapcore._build_query(dims, fks, factor, m1, m2, G, aggs, 0, m1.numel(), None)
+    assert sum(q.dimvec_len[j] for j in range(4)) == OLAP_NOALLOC_MAX_DIM_ENTRIES
+    gs = torch.full((1, G), -1, dtype=torch.int64, device="cuda")
+    tot = torch.full((1,), -1, dtype=torch.int64, device="cuda")
+    err = torch.full((1,), -1, dtype=torch.int64, device="cuda")
+    assert _fn()(C.byref(q), gs.data_ptr(), tot.data_ptr(), err.data_ptr(), None) == _lib.OLAP_OK
+    torch.cuda.synchronize()
+    assert torch.equal(gs, ref_gs) and torch.equal(tot, ref_tot) and int(err.item()) == ref_err
 
 
 def test_noalloc_rejects_queries_beyond_its_scratch():

@@ -197,8 +197,11 @@ OLAP_API int olap_starjoin_autotune(olap_ctx* ctx, const olap_starjoin_query* q,
  *  - All calls share the scratch, which keeps the last call's contents; each
  *    call clears what must start at zero.  Calls that overlap on the GPU race
  *    on it: order them on one stream.
- *  - The first call on a device looks up the scratch's device address; make
- *    it before any stream capture. */
+ *  - The first call on a device looks up the scratch's device address and
+ *    keeps it for the life of the process; make it before any stream
+ *    capture.  The device must not be reset (cudaDeviceReset, or a teardown
+ *    of its primary context) between calls: the kept address would then
+ *    point into a context that no longer exists. */
 #define OLAP_NOALLOC_SCRATCH_BYTES (1 << 20)
 #define OLAP_NOALLOC_MAX_DIM_ENTRIES 8000000
 OLAP_API int olap_starjoin_groupsum_noalloc(const olap_starjoin_query* q, int64_t* group_sums,

@@ -304,15 +304,13 @@ int starjoin_host_inplace(olap_ctx* ctx, const olap_starjoin_query* q, const ola
   for (int j = 0; j < nd; ++j)
     OLAP_REQUIRE(ctx, dq.dimvec_len[j] >= 1 && dq.dimvec_len[j] <= INT32_MAX, "dimvec_len must be in [1, 2^31)");
 
-  // Probe order: ascending fraction of passing dimension entries.
+  // Probe order: ascending fraction of passing dimension entries.  Scratch
+  // taken before the decision below is given back when the call declines, so
+  // the copy path that then runs finds the arena as it was.
+  const size_t arena_mark = ar.off;
   unsigned long long* cnt = ar.take<unsigned long long>(OLAP_MAX_DIMS);
-  const int64_t nacc = q->group_nums * q->n_aggs;
-  int64_t* dsum = ar.take<int64_t>(static_cast<size_t>(nacc));
-  int64_t* dtot = ar.take<int64_t>(2);
-  if (!cnt || !dsum || !dtot) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for the in-place scan");
+  if (!cnt) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for the in-place scan");
   OLAP_CUDA_TRY(ctx, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * OLAP_MAX_DIMS, ctx->stream));
-  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(dsum, 0, sizeof(int64_t) * nacc, ctx->stream));
-  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(dtot, 0, sizeof(int64_t) * 2, ctx->stream));
   for (int j = 0; j < nd; ++j) {
     const uint32_t len = static_cast<uint32_t>(dq.dimvec_len[j]);
     const int grid = static_cast<int>(std::min<int64_t>(int64_t(ctx->sm_count) * 4, (len + 255) / 256));
@@ -340,10 +338,17 @@ int starjoin_host_inplace(olap_ctx* ctx, const olap_starjoin_query* q, const ola
     const int nm = (dm1 ? 1 : 0) + (dm2 ? 1 : 0);
     sectors += nm * (1.0 - std::pow(1.0 - alive, 8.0));
     if (tune_or(ctx, TUNE_HOST_INPLACE, 1) != 3 && sectors > kInplaceMaxShare * (nd + nm)) {
+      ar.off = arena_mark;
       *handled = false;
       return OLAP_OK;
     }
   }
+  const int64_t nacc = q->group_nums * q->n_aggs;
+  int64_t* dsum = ar.take<int64_t>(static_cast<size_t>(nacc));
+  int64_t* dtot = ar.take<int64_t>(2);
+  if (!dsum || !dtot) return set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena too small for the in-place scan");
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(dsum, 0, sizeof(int64_t) * nacc, ctx->stream));
+  OLAP_CUDA_TRY(ctx, cudaMemsetAsync(dtot, 0, sizeof(int64_t) * 2, ctx->stream));
 
   HostScanParams hp;
   std::memset(&hp, 0, sizeof(hp));

@@ -223,3 +223,26 @@ def test_default_takes_copies_when_nothing_is_filtered(ctx):
     st, dropped, gs, tot = run_host(ctx, dv2, cols[:4], factor, cols[4], cols[5], G, (AGG_M1_PLUS_M2,), (0, n))
     assert st == 0 and np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
     assert ctx.take_host_bytes() < 0.5 * n * 4 * 6
+
+
+def test_declined_inplace_scan_gives_back_its_scratch():
+    """A query whose filters keep every row makes the default call decline
+    the in-place scan and copy instead.  The scratch the in-place attempt
+    took must be returned first: with group sums of 40 MB (2,500,000 groups,
+    two aggregates) in the default 64 MiB arena, taking them twice would
+    leave no room and fail the call."""
+    n = 200_003
+    groups = [50, 50, 40, 25]
+    dv, fk, m1, m2 = random_star(29, n, SIZES, [1.0] * 4, groups)
+    factor = [int(np.prod(groups[j + 1:])) for j in range(4)]
+    G = int(np.prod(groups))
+    aggs = (AGG_M1, AGG_M1_TIMES_M2)
+    hold = [pinned(f) for f in fk] + [pinned(m1), pinned(m2)]
+    cols = [h[1] for h in hold]
+    o_gs, o_tot, o_err = oracle.starjoin(dv, fk, factor, m1, m2, G, aggs=aggs)
+    with olapcore.Context(0) as c:  # default arena
+        st, dropped, gs, tot = run_host(c, dv, cols[:4], factor, cols[4], cols[5], G, aggs, (0, n))
+        moved = c.take_host_bytes()
+    assert st == 0 and o_err == 0
+    assert np.array_equal(gs, o_gs) and np.array_equal(tot, o_tot)
+    assert moved == n * 4 * 6 + sum(len(d) for d in dv)  # the copies ran

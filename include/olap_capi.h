@@ -125,9 +125,15 @@ OLAP_API const char* olap_build_info(void);
  *   group_sums[a][g] += agg_a(M1[r], M2[r])
  * with j over the dimensions in probe order (dimvec[j] is the reference's
  * dimvec_array[orders[j]]).  Semantics follow OLAPcore_vwm_sv_thread
- * (cpp:509-568): measures are read at the row's own position.  A row whose fk
- * is outside [0, dimvec_len[j]) or whose g is outside [0, group_nums) is
- * dropped and counted as a range error (the reference reads out of bounds). */
+ * (cpp:509-568): measures are read at the row's own position.  Where the
+ * reference reads out of bounds, the library drops the row instead: a row
+ * with an fk outside [0, dimvec_len[j]) is never accumulated, and it counts
+ * as a range error unless one of its in-range keys meets DIM_NULL (a row
+ * that a filter drops anyway is not an error); a surviving row whose g is
+ * outside [0, group_nums) is dropped and counted too.  The count does not
+ * depend on the order the dimensions are probed in, so every entry point
+ * below (device, host in place or copied, reference layout, no-allocation)
+ * reports the same count for the same rows. */
 typedef struct olap_starjoin_query {
   int32_t dimvec_nums;                    /* participating dimensions, 0..4   */
   int32_t n_aggs;                         /* aggregates per group, 1..2       */
@@ -161,8 +167,8 @@ OLAP_API int olap_starjoin_launch_count(olap_ctx* ctx, const olap_starjoin_query
  * bytes, one kernel reads the columns in place instead (OLAP_TUNE_HOST_INPLACE
  * 2 forces the copies, 3 the in-place read): the foreign keys of the
  * dimension that drops the most rows first, each later column only for the
- * rows still alive (late materialisation over PCIe); its dropped-row count
- * then covers the keys it read, while the sums are the same.  A dimvec_len[j] of
+ * rows still alive (late materialisation over PCIe); sums and dropped-row
+ * count are the same either way.  A dimvec_len[j] of
  * 0 means "unknown": the library then copies dimvec[j][0 .. max fk] (the
  * bytes the reference itself would read).  Returns OLAP_ERR_RANGE (results
  * still written) when rows were dropped. */
@@ -213,9 +219,15 @@ OLAP_API int olap_starjoin_groupsum_noalloc(const olap_starjoin_query* q, int64_
  * table (0 customer, 1 supplier, 2 part, 3 date); orders[0..dimvec_nums)
  * names the tables in probe order and factor[j] belongs to orders[j], exactly
  * as the reference's main builds them (cpp:1964-1987).  dimvec_len may be
- * NULL (then every fk must be trusted by the caller: no range check beyond
- * 2^31).  *count receives the grand total of M1+M2 over all groups (the
- * reference's return value); group_vector (device, [group_nums]) may be NULL. */
+ * NULL, as the reference's signature has no lengths: each dimension vector
+ * is then taken to reach to the end of the device allocation that holds it
+ * (a key past that is dropped and counted, never read; a key inside the
+ * allocation but past the caller's vector reads the bytes that follow it, as
+ * the reference would), and a vector outside any device allocation is
+ * refused with OLAP_ERR_INVALID.  *count receives the grand total of M1+M2
+ * over all groups (the reference's return value); group_vector (device,
+ * [group_nums]) may be NULL.  Dropped rows are left in the context's count
+ * (olap_ctx_take_range_errors). */
 OLAP_API int olap_OLAPcore(olap_ctx* ctx, int8_t* const* dimvec_array, const int64_t* dimvec_len,
                   int32_t* const* fk_array, const int* orders, int dimvec_nums,
                   const int* factor, int64_t size_lineorder, int64_t group_nums,

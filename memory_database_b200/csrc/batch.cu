@@ -282,17 +282,21 @@ __global__ void __launch_bounds__(kBatchMaxThreads, 1) batch_scan_kernel(const B
       while (s + 1 < nseg && sseg[s + 1] <= r0 + k) ++s;
       m[k] = k < nv ? smask[s] : 0ull;
     }
-    // Keys out of range drop the row for the queries that use the table
-    // (counted once per such query, as the plain path counts them).
+    // A key out of range drops the row for the queries that use the table;
+    // the table is not probed for it, and the row counts once per such query
+    // when every other table the query uses passes it (as the plain path
+    // counts: no in-range key of the query meets its filter's null).
+    unsigned long long oobq[4] = {0ull, 0ull, 0ull, 0ull};
+    uint32_t inr = 0;  // bit 4*o + k: key[o][k] in range
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      if (!m[k]) continue;
-      unsigned long long oob = 0;
 #pragma unroll
-      for (int o = 0; o < OLAP_MAX_DIMS; ++o)
-        if (o < ntab && static_cast<uint32_t>(key[o][k]) >= tlen[o]) oob |= tuses[o];
-      bad += __popcll(m[k] & oob);
-      m[k] &= ~oob;
+      for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
+        if (o >= ntab) continue;
+        if (static_cast<uint32_t>(key[o][k]) < tlen[o]) inr |= 1u << (4 * o + k);
+        else oobq[k] |= tuses[o];
+      }
+      oobq[k] &= m[k];
     }
     // Probe the tables, smallest first, breadth-first across the 4 rows; a
     // table is probed for a row only while a live query of the row uses it.
@@ -305,12 +309,18 @@ __global__ void __launch_bounds__(kBatchMaxThreads, 1) batch_scan_kernel(const B
       ulonglong2 rec[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k)
-        rec[k] = (m[k] & ut) ? ld_record(rt + key[o][k], pol_keep) : make_ulonglong2(~0ull, 0ull);
+        rec[k] = ((m[k] & ut) && ((inr >> (4 * o + k)) & 1u)) ? ld_record(rt + key[o][k], pol_keep)
+                                                                 : make_ulonglong2(~0ull, 0ull);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         m[k] &= rec[k].x;
         gr[o][k] = static_cast<int32_t>(static_cast<uint32_t>(rec[k].y));
       }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      bad += __popcll(m[k] & oobq[k]);
+      m[k] &= ~oobq[k];
     }
     // Per-query work only for the queries left in each row's mask.
 #pragma unroll

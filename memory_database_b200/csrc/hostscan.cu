@@ -17,9 +17,10 @@
 //  * the dimension vectors are copied to the device once per call and probed
 //    through L2; group sums accumulate in shared memory (flushed once per
 //    block) or with L2 atomics.
-// The sums equal the streaming path's.  The dropped-row count covers the keys
-// that were read: a row dropped by an earlier dimension's DIM_NULL is not
-// range-checked on the later ones.
+// The sums and the dropped-row count equal the streaming path's: a row with a
+// key out of range is never accumulated, and it keeps reading its later keys
+// (it is rare) so that it counts as a range error exactly when none of its
+// in-range keys meets DIM_NULL, the rule every star-join path shares.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -130,6 +131,7 @@ __global__ void __launch_bounds__(kHostScanThreads) starjoin_hostscan_kernel(con
     const uint32_t i = in ? w0 + lane : p.nvec - 1;  // lanes past the end keep a valid address
     const int64_t at = p.vec_begin + 4ll * i;
     uint32_t alive = in ? 0xFu : 0u;
+    uint32_t oob = 0;  // rows with a key out of range: read on, never accumulated
     int64_t g[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int j = 0; j < ND; ++j) {
@@ -146,14 +148,12 @@ __global__ void __launch_bounds__(kHostScanThreads) starjoin_hostscan_kernel(con
       int32_t c[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        bool a = (alive >> r) & 1u;
-        if (a && kk[r] >= d.len) {
-          alive &= ~(1u << r);
-          ++bad;
-          a = false;
-        }
+        const bool live = (alive >> r) & 1u;
+        const bool inr = kk[r] < d.len;
+        if (live && !inr) oob |= 1u << r;
+        const bool a = live && inr;
         const uint32_t kp = a ? kk[r] : 0u;  // in bounds whether or not the load is predicated
-        c[r] = a ? ld_probe_s8(d.vec + kp, pol_keep) : OLAP_DIM_NULL;
+        c[r] = a ? ld_probe_s8(d.vec + kp, pol_keep) : (live ? 0 : OLAP_DIM_NULL);
       }
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
@@ -161,6 +161,8 @@ __global__ void __launch_bounds__(kHostScanThreads) starjoin_hostscan_kernel(con
         else g[r] += static_cast<int64_t>(c[r]) * d.factor;
       }
     }
+    bad += __popc(alive & oob);
+    alive &= ~oob;
     if (!__any_sync(kFull, alive != 0)) continue;
     const bool need = alive != 0;
     int4 x = make_int4(0, 0, 0, 0), y = make_int4(0, 0, 0, 0);
@@ -187,17 +189,22 @@ __global__ void __launch_bounds__(kHostScanThreads) starjoin_hostscan_kernel(con
   if (blockIdx.x == 0) {
     auto one = [&](int64_t r) {
       int64_t gg = 0;
+      bool oob1 = false;
 #pragma unroll
       for (int j = 0; j < ND; ++j) {
         const uint32_t k = static_cast<uint32_t>(p.dim[j].fk[r]);
         ++sec;
         if (k >= p.dim[j].len) {
-          ++bad;
-          return;
+          oob1 = true;
+          continue;
         }
         const int32_t c = p.dim[j].vec[k];
         if (c == OLAP_DIM_NULL) return;
         gg += static_cast<int64_t>(c) * p.dim[j].factor;
+      }
+      if (oob1) {
+        ++bad;
+        return;
       }
       const int32_t x = p.m1 ? p.m1[r] : 0, y = p.m2 ? p.m2[r] : 0;
       sec += (p.m1 ? 1u : 0u) + (p.m2 ? 1u : 0u);

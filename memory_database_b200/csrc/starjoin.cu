@@ -28,6 +28,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <cuda.h>
+
 #include "olap_internal.cuh"
 
 namespace olap {
@@ -378,17 +380,33 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
       const int c = r & 3;
       return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
     };
-    // Range check of every key (registers only).
-    uint32_t inb = alive;
+    // Range check of every key (registers only).  A row with a key out of
+    // range is dropped; it is a range error unless one of its in-range keys
+    // meets DIM_NULL (then a filter drops it anyway), which counts the same
+    // whatever order the dimensions are probed in.  Rare: off the hot path.
+    uint32_t oob = 0;
 #pragma unroll
     for (int r = 0; r < V; ++r) {
       bool ok = true;
 #pragma unroll
       for (int j = 0; j < ND; ++j) ok &= key(r, j) < p.dim[j].len;
-      if (!ok) inb &= ~(1u << r);
+      if (!ok) oob |= 1u << r;
     }
-    bad += __popc(alive & ~inb);
-    alive = inb;
+    oob &= alive;
+    if (oob) {
+#pragma unroll
+      for (int r = 0; r < V; ++r) {
+        if (!((oob >> r) & 1u)) continue;
+        bool filtered = false;
+#pragma unroll
+        for (int j = 0; j < ND; ++j) {
+          const uint32_t k = key(r, j);
+          if (k < p.dim[j].len && p.dim[j].vec[k] == OLAP_DIM_NULL) filtered = true;
+        }
+        bad += filtered ? 0u : 1u;
+      }
+      alive &= ~oob;
+    }
     int32_t g[V];
 #pragma unroll
     for (int r = 0; r < V; ++r) g[r] = 0;
@@ -584,8 +602,12 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
         k[j] = static_cast<uint32_t>(p.dim[j].fk[r]);
         ok &= k[j] < p.dim[j].len;
       }
-      if (!ok) {
-        ++bad;
+      if (!ok) {  // a range error unless an in-range key meets DIM_NULL
+        bool filtered = false;
+#pragma unroll
+        for (int j = 0; j < ND; ++j)
+          if (k[j] < p.dim[j].len && p.dim[j].vec[k[j]] == OLAP_DIM_NULL) filtered = true;
+        bad += filtered ? 0u : 1u;
         return;
       }
       int64_t g = 0;
@@ -651,8 +673,12 @@ __global__ void __launch_bounds__(1024, 1) starjoin_scalar_kernel(const StarPara
     }
     const int32_t x = p.need_m1 ? ld_stream_s32(p.m1 + r, pol_stream) : 0;
     const int32_t y = p.need_m2 ? ld_stream_s32(p.m2 + r, pol_stream) : 0;
-    if (!ok) {
-      ++bad;
+    if (!ok) {  // a range error unless an in-range key meets DIM_NULL
+      bool filtered = false;
+#pragma unroll
+      for (int j = 0; j < ND; ++j)
+        if (k[j] < p.dim[j].len && p.dim[j].vec[k[j]] == OLAP_DIM_NULL) filtered = true;
+      bad += filtered ? 0u : 1u;
       continue;
     }
     int64_t g = 0;
@@ -1131,7 +1157,7 @@ int starjoin_host(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   if (sd != OLAP_OK) return sd;
   // Pinned columns are read in place (1: when that reads fewer bytes, the
   // default; 3: always) unless TUNE_HOST_INPLACE = 2 asks for the chunked
-  // copies (whose dropped-row count covers every key).
+  // copies (the same sums and dropped-row count either way).
   const int64_t inplace = tune_or(ctx, TUNE_HOST_INPLACE, 1);
   if ((inplace == 1 || inplace == 3) && rows > 0) {
     bool handled = false;
@@ -1255,6 +1281,32 @@ int starjoin_host(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   return OLAP_OK;
 }
 
+// Bytes from device pointer p to the end of the device allocation holding it
+// (the driver's cuMemGetAddressRange, reached through the runtime's entry
+// point table so the library needs no link to libcuda).  False when p is not
+// in a device allocation of the current context.
+static bool device_bytes_from(const void* p, int64_t* bytes) {
+  using AddressRange = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+  static AddressRange fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &qr) == cudaSuccess &&
+        qr == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<AddressRange>(f);
+    else
+      cudaGetLastError();
+  });
+  if (!fn || !p) return false;
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  const CUdeviceptr at = reinterpret_cast<CUdeviceptr>(p);
+  if (fn(&base, &size, at) != CUDA_SUCCESS || at < base || at >= base + size) return false;
+  *bytes = static_cast<int64_t>(base + size - at);
+  return true;
+}
+
 }  // namespace olap
 
 extern "C" {
@@ -1310,7 +1362,17 @@ int olap_OLAPcore(olap_ctx* ctx, int8_t* const* dimvec_array, const int64_t* dim
     OLAP_REQUIRE(ctx, t >= 0 && t < OLAP_MAX_DIMS, "orders[] entry must name table 0..3");
     q.dimvec[j] = dimvec_array[t];
     q.fk[j] = fk_array[t];
-    q.dimvec_len[j] = dimvec_len ? dimvec_len[t] : INT32_MAX;
+    if (dimvec_len) {
+      q.dimvec_len[j] = dimvec_len[t];
+    } else {
+      // No lengths (the reference's signature has none): a vector reaches to
+      // the end of the device allocation that holds it, so a key past that
+      // is dropped and counted, never read.
+      int64_t avail = 0;
+      OLAP_REQUIRE(ctx, olap::device_bytes_from(dimvec_array[t], &avail),
+                   "dimvec_len is NULL and a dimension vector is not in a device allocation");
+      q.dimvec_len[j] = std::min<int64_t>(avail, INT32_MAX);
+    }
     q.factor[j] = factor[j];
   }
   q.m1 = M1;

@@ -1,0 +1,134 @@
+"""GPU parity at the sizes the benchmark and the reference publish.
+
+* The reference's ten OLAPcore.sh queries on its own data stream at SF=100
+  (600,000,000 fact rows, glibc rand() from its default seed): the B200
+  kernel must reproduce the grand totals the reference published
+  (GPU/plot/old.py), and for q2.1 and q4.1 the oracle's per-group sums.  The
+  other eight queries are marked slow (a minute of host-side generation
+  each).
+* The 600M-row star-join the benchmark times, with the plan the autotuner
+  picks for it and with the plan the benchmark recorded: per-group int64
+  SUM(m1) and SUM(m1*m2) equal the oracle's on the same table (regenerated
+  on the host by the oracle's copy of the generators), and SUM(M1+M2) equals
+  the int the reference's own OLAPcore_vwm_sv returns, modulo 2^32."""
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from memory_database_b200 import olapcore, workloads
+from memory_database_b200.olapcore import AGG_M1, AGG_M1_PLUS_M2, AGG_M1_TIMES_M2
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+NT = os.cpu_count() or 1
+GOLDEN = json.loads((Path(__file__).resolve().parent / "golden" / "olapcore_queries.json").read_text())
+PER_GROUP = (21, 41)  # q2.1 and q4.1: per-group sums against the oracle too
+
+
+def _qid(q):
+    return f"q{q['sqlnum'] // 10}.{q['sqlnum'] % 10}"
+
+
+@pytest.fixture(scope="module")
+def sf100_fk():
+    n = oracle.size_of_table(4, 100.0)
+    bufs = [np.empty(n, np.int32) for _ in range(4)]
+    yield bufs
+    del bufs
+
+
+@pytest.mark.parametrize("q", [pytest.param(q, id=_qid(q), marks=() if q["sqlnum"] in PER_GROUP else pytest.mark.slow)
+                               for q in GOLDEN])
+def test_published_sf100_totals(ctx, q, sf100_fk):
+    dv, fk, _, _ = oracle.gen_olapcore_compat(100.0, q["sele"], q["bitmap"], q["groups"], measures=False,
+                                              fk_out=sf100_fk)
+    n = len(fk[0])
+    assert n == 600_000_000
+    G = q["group_nums"]
+    ddv = [torch.from_numpy(d).cuda() for d in dv]
+    dfk = [torch.from_numpy(f).cuda() for f in fk]
+    m = torch.full((n,), 5, dtype=torch.int32, device="cuda")
+    gv = torch.zeros(G, dtype=torch.int64, device="cuda")
+    total = olapcore.OLAPcore_vwm_sv(ddv, dfk, q["orders"], q["dimvec_nums"], q["factor"], n, G, m, m, 48,
+                                     dimvec_len=[len(d) for d in dv], ctx=ctx, group_vector=gv)
+    assert total == q["total_sf100_published"], _qid(q)
+    assert ctx.take_range_errors() == 0
+    del dfk, m
+    if q["sqlnum"] in PER_GROUP:
+        o = q["orders"]
+        five = np.full(n, 5, np.int32)
+        gs, tot, err = oracle.starjoin([dv[t] for t in o], [fk[t] for t in o], q["factor"], five, five, G,
+                                       nthreads=NT)
+        assert err == 0 and int(tot[0]) == total
+        assert np.array_equal(gv.cpu().numpy(), gs[0])
+    torch.cuda.empty_cache()
+
+
+DIM_SIZES = (3_000_000, 200_000, 1_400_000, 2_556)
+SELE, GROUPS = (0.5, 0.2, 0.1, 1.0), (8, 8, 8, 8)
+# The plan the benchmark recorded for this workload (OLAP_TUNE_* knob: value).
+BENCHED_PLAN = {0: 1024, 3: 1, 6: 2, 12: 230400, 14: 1, 15: 1}
+
+
+@pytest.fixture(scope="module")
+def headline():
+    n = 600_000_000
+    ctx = olapcore.Context(0, scratch_bytes=512 << 20)
+    s = workloads.make_star_schema(ctx, n, DIM_SIZES, SELE, GROUPS, seed=42)
+    h = oracle.star_schema(n, DIM_SIZES, SELE, GROUPS, seed=42)
+    aggs = (AGG_M1, AGG_M1_TIMES_M2)
+    o_gs, o_tot, o_err = oracle.starjoin(h.probe_dims, h.probe_fks, h.factor, h.m1, h.m2, h.group_nums,
+                                         aggs=aggs, nthreads=NT)
+    yield ctx, s, h, (o_gs, o_tot, o_err)
+    del s
+    ctx.close()
+    torch.cuda.empty_cache()
+
+
+def _run(ctx, s, aggs):
+    gs, tot = olapcore.starjoin_groupsum(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, s.group_nums,
+                                         aggs=aggs, dimvec_lens=s.probe_lens, ctx=ctx)
+    torch.cuda.synchronize()
+    return gs.cpu().numpy(), tot.cpu().numpy(), ctx.take_range_errors()
+
+
+@pytest.mark.parametrize("plan", ["autotuned", "benched"])
+def test_headline_600M_plan_matches_oracle(headline, plan):
+    ctx, s, h, (o_gs, o_tot, o_err) = headline
+    assert o_err == 0
+    aggs = (AGG_M1, AGG_M1_TIMES_M2)
+    for k in range(16):
+        ctx.set_tuning(k, 0)
+    if plan == "autotuned":
+        olapcore.autotune(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, s.group_nums, aggs=aggs,
+                          dimvec_lens=s.probe_lens, ctx=ctx)
+    else:
+        for k, v in BENCHED_PLAN.items():
+            ctx.set_tuning(k, v)
+    gs, tot, err = _run(ctx, s, aggs)
+    assert err == 0
+    assert np.array_equal(tot, o_tot)
+    assert np.array_equal(gs, o_gs)
+
+
+def test_headline_600M_reference_int_return(headline):
+    """SUM(M1+M2) over the same 600M rows: the reference's OLAPcore_vwm_sv
+    (its own source, all host threads) returns it modulo 2^32 as an int."""
+    if not oracle.ref_available():
+        pytest.skip("the reference was not built here")
+    ctx, s, h, _ = headline
+    for k in range(16):
+        ctx.set_tuning(k, 0)
+    gs, tot, err = _run(ctx, s, (AGG_M1_PLUS_M2,))
+    assert err == 0
+    ref = oracle.ref_lib()
+    o = np.array(h.orders, np.int32)
+    f = np.array(h.factor, np.int32)
+    r = ref.ref_OLAPcore_vwm_sv(oracle._ptr_array(h.dimvec), oracle._ptr_array(h.fk), oracle._p(o), h.dimvec_nums,
+                                oracle._p(f), h.n_rows, h.group_nums, oracle._p(h.m1), oracle._p(h.m2), NT)
+    assert (int(tot[0]) - r) % (1 << 32) == 0

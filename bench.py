@@ -53,7 +53,6 @@ def parse():
                     help="host call reads pinned columns in place (OLAP_TUNE_HOST_INPLACE) or copies them")
     ap.add_argument("--e2e-rows", type=int, default=0,
                     help="rows per rank of the e2e leg (0: the whole table at N=1, 150M per rank at N>1)")
-    ap.add_argument("--cpu-sample-rows", type=int, default=100_000_000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tune", type=str, default="", help="knob=value,... (olap_ctx_set_tuning)")
@@ -69,6 +68,8 @@ def parse():
     ap.add_argument("--queries", type=int, default=64)
     ap.add_argument("--batch-shape", type=str, default="",
                     help="block,slots of the batched scan (skips its autotuner), e.g. 1024,16384")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="headline line only (no batched / serving / operators / sweep sub-objects)")
     return ap.parse_args()
 
 
@@ -138,59 +139,102 @@ def measured_peak_gbs() -> tuple[float, str]:
 
 
 # ---------------------------------------------------------------------------
-# CPU: the reference's own OLAPcore on this host (bounded sample)
+# CPU: the reference's own OLAPcore on this host
 # ---------------------------------------------------------------------------
-def cpu_reference(rows: int, sele, groups, steps: int, warmup: int, seed: int = 42) -> dict:
-    """Time the reference's OLAPcore_vwm_sv (all host threads) on a sample of
-    the workload; returns the cpu_baseline dict (rows/s)."""
-    import ctypes as C
+REF_FANOUTS = ("OLAPcore_rowwise", "OLAPcore_vwm_dv", "OLAPcore_vwm_sv")
+
+
+def bench_config(a, world: int) -> dict:
+    """The workload both arms run (identical dicts, so the lines compare)."""
+    return {"workload": WORKLOAD, "rows_per_gpu": a.rows, "dim_sizes": list(DIM_SIZES), "sele": list(a.sele),
+            "groups": list(a.groups), "fk_dist": a.fk_dist, "group_nums": int(_prod(a.groups)),
+            "l2": "inputs 14.4 GB/GPU > 126 MB L2; no flush", "parallelism": f"row shards x{world}"}
+
+
+def _prod(xs) -> int:
+    p = 1
+    for x in xs:
+        p *= int(x) if int(x) else 1
+    return p
+
+
+def host_tables(a):
+    """The benchmark's table in host memory, from the oracle's copy of the
+    library's generators (bit-identical to the HBM table of rank 0)."""
+    import oracle
+    return oracle.star_schema(a.rows, DIM_SIZES, a.sele, a.groups, fk_dist=a.fk_dist, seed=42)
+
+
+def reference_cpu(h, steps: int, warmup: int) -> dict:
+    """Time the reference's own OLAPcore_rowwise, OLAPcore_vwm_dv and
+    OLAPcore_vwm_sv (test_multi_compute_operator.cpp:973,1052,1258, compiled
+    from its sources) on the host table ``h`` with every host thread; the
+    fastest is the baseline.  Their int returns are SUM(M1+M2) modulo 2^32
+    (rowwise's only when the measures are constant: it reads M1[i] with the
+    thread-local index, :360).  Without the compiled reference, the oracle's
+    restatement is timed instead (kind "port")."""
     import numpy as np
     import oracle
-    from memory_database_b200 import workloads
     cores = os.cpu_count() or 1
-    s = workloads.host_star_schema(rows, DIM_SIZES, sele, groups, seed=seed)
-    kind = "reference" if oracle.ref_available() else "port"
-    nd, G = s.dimvec_nums, s.group_nums
-    o = np.array(s.orders + [0] * (4 - nd), np.int32)
-    f = np.array(s.factor + [0] * (4 - nd), np.int32)
-    if kind == "reference":
-        ref = oracle.ref_lib()
-        dva, fka = oracle._ptr_array(s.dimvec), oracle._ptr_array(s.fk)
+    n, nd, G = h.n_rows, h.dimvec_nums, h.group_nums
+    if oracle.ref_available():
+        ref, flags = oracle.ref_lib_for_host()
+        o = np.array(h.orders + [0] * (4 - nd), np.int32)
+        f = np.array(h.factor + [0] * (4 - nd), np.int32)
+        dva, fka = oracle._ptr_array(h.dimvec), oracle._ptr_array(h.fk)
+        variants = {}
+        for name in REF_FANOUTS:
+            fn = getattr(ref, "ref_" + name)
 
-        def run():
-            return ref.ref_OLAPcore_vwm_sv(dva, fka, oracle._p(o), nd, oracle._p(f), rows, G,
-                                           oracle._p(s.m1), oracle._p(s.m2), cores)
-        threads = cores
-        what = "OLAPcore_vwm_sv (reference source, -O3 -march=x86-64-v3)"
-    else:
-        def run():
-            return oracle.starjoin(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G)
-        threads = 1
-        what = "oracle restatement (single thread)"
+            def run():
+                return fn(dva, fka, oracle._p(o), nd, oracle._p(f), n, G, oracle._p(h.m1), oracle._p(h.m2), cores)
+            r = 0
+            for _ in range(warmup):
+                r = run()
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                r = run()
+            dt = (time.perf_counter() - t0) / steps
+            variants[name] = {"ms": dt * 1e3, "rows_per_s": n / dt, "int_return_mod_2^32": int(r) & 0xFFFFFFFF}
+        best = min(variants, key=lambda k: variants[k]["ms"])
+        return {"kind": "reference", "cores": cores, "ms": variants[best]["ms"], "value": n / (variants[best]["ms"] / 1e3),
+                "best": best, "variants": variants, "build": flags,
+                "sum_m1_plus_m2_mod_2^32": variants["OLAPcore_vwm_sv"]["int_return_mod_2^32"],
+                "sample": f"all {n:,} rows of the workload; fastest of {', '.join(REF_FANOUTS)} "
+                          f"(reference source, {flags}, {cores} threads), {steps} timed runs after {warmup} warm-up"}
+    dims, fks = h.probe_dims, h.probe_fks
+    out = None
     for _ in range(warmup):
-        run()
+        out = oracle.starjoin(dims, fks, h.factor, h.m1, h.m2, G, want_groups=False, nthreads=cores)
     t0 = time.perf_counter()
     for _ in range(steps):
-        run()
+        out = oracle.starjoin(dims, fks, h.factor, h.m1, h.m2, G, want_groups=False, nthreads=cores)
     dt = (time.perf_counter() - t0) / steps
-    return {"value": rows / dt, "unit": "rows/s", "cores": threads, "kind": kind,
-            "sample": f"{rows:,} rows of the same workload ({what}), {steps} timed runs after {warmup} warm-up",
-            "ms_per_step": dt * 1e3}
+    return {"kind": "port", "cores": cores, "ms": dt * 1e3, "value": n / dt, "best": "oracle restatement",
+            "sum_m1_plus_m2_mod_2^32": int(out[1][0]) & 0xFFFFFFFF,
+            "sample": f"all {n:,} rows of the workload; the oracle's restatement of OLAPcore_vwm_sv "
+                      f"({cores} threads), {steps} timed runs after {warmup} warm-up"}
 
 
 def run_reference_arm(a) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    rows = min(a.rows, a.cpu_sample_rows)
-    cb = cpu_reference(rows, a.sele, a.groups, max(1, a.steps), max(1, a.warmup))
+    world = int(os.environ.get("WORLD_SIZE", str(a.gpus)))
+    h = host_tables(a)
+    cb = reference_cpu(h, max(1, a.steps), max(1, a.warmup))
     line = {
         "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "rows/s",
-        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": cb["ms_per_step"],
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": cb["ms"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-        "data": "synthetic (seeded counter-based generator)",
-        "config": {"workload": WORKLOAD, "rows_timed_per_step": rows},
-        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "data": "synthetic (seeded counter-based generator, the oracle's host copy of the library's)",
+        "config": bench_config(a, world),
+        "aggregate": "SUM(M1+M2) per group in uint32 counters (the reference's only aggregate)",
+        "rows_timed_per_step": h.n_rows,
+        "reference_variants": cb.get("variants"),
+        "check": {"sum_m1_plus_m2_mod_2^32": cb["sum_m1_plus_m2_mod_2^32"]},
+        "cpu_baseline": {"value": cb["value"], "unit": "rows/s", "cores": cb["cores"], "kind": cb["kind"],
+                         "sample": cb["sample"]},
         "e2e": {"value": cb["value"], "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -200,6 +244,10 @@ def run_reference_arm(a) -> None:
 # GPU arm
 # ---------------------------------------------------------------------------
 def run_batched(a) -> None:
+    print(json.dumps(batched_result(a)), flush=True)
+
+
+def batched_result(a) -> dict:
     """Batched configuration: Q star-join queries (own predicates, 1-3 group
     tables, 5-100% fact ranges) over the shared 600M-row table, one persistent
     launch per batch replayed as a CUDA graph, against one launch per query."""
@@ -251,11 +299,20 @@ def run_batched(a) -> None:
     e1.record()
     torch.cuda.synchronize()
     p_ms = e0.elapsed_time(e1)
+    # check (untimed): every query of the first batch equals the query run alone
+    bo, bt, offs = eng.run(qs0, s.fk, s.m1, s.m2, out=out, totals=tot)
+    checked = True
+    for i, q in enumerate(qs0):
+        batch.run_plain(ctx, dims, q, s.fk, s.m1, s.m2, vec_buffers=vec_bufs, out=pg[:, : q.group_nums],
+                        totals_out=pt)
+        checked &= bool(torch.equal(pg[0, : q.group_nums], bo[offs[i]: offs[i] + q.group_nums])
+                        and torch.equal(pt[0], bt[i]))
     rows_scanned = sum(q.row_end - q.row_begin for q in qs0)
     line = {"metric": "batched star-join queries/sec", "value": a.queries / (b_ms / 1e3), "unit": "queries/s",
             "n_gpus": 1, "steps": len(batches), "warmup": a.warmup, "ms_per_batch": b_ms,
             "plain_ms_per_batch": p_ms, "plain_queries_per_s": a.queries / (p_ms / 1e3),
             "speedup_vs_one_launch_per_query": p_ms / b_ms, "higher_is_better": True, "clocks": clk.summary(),
+            "checked": checked,
             "config": {"workload": f"{a.queries} star-join queries per batch over the shared {a.rows:,}-row table "
                                    "(joint selectivity log-uniform [1e-4, 0.3], 1-3 group tables of 25/25/40/7, "
                                    "fact range 5-100%), one persistent launch per batch replayed as a CUDA graph",
@@ -264,12 +321,16 @@ def run_batched(a) -> None:
                                         "chosen_by": "--batch-shape" if a.batch_shape
                                         else "olap_batch_autotune on a 64Mi-row sample"}},
             "data": "synthetic (seeded counter-based generator, generated in HBM)"}
-    print(json.dumps(line), flush=True)
     eng.close()
     ctx.close()
+    return line
 
 
 def run_serving(a) -> None:
+    print(json.dumps(serving_result(a)), flush=True)
+
+
+def serving_result(a) -> dict:
     """Serving configuration: Poisson arrivals at each rate of --rates, 70%
     star-joins of the batched configuration over the 600M-row table and 30%
     Q5 chains over SF~10-sized tables, served with continuous batching and
@@ -312,6 +373,7 @@ def run_serving(a) -> None:
     torch.cuda.synchronize()
     q5_batch_ms = e0.elapsed_time(e1) / 5
     per_rate = []
+    checked = True
     for rate in a.rates:
         n = max(50, int(rate * a.serve_seconds))
         reqs = S.poisson_requests(np.random.default_rng(int(rate)), rate, n, star, q5q)
@@ -320,6 +382,10 @@ def run_serving(a) -> None:
             nb = batched.batches
             rp = plain.serve(S.reset(reqs))
         sb, sp = S.summarize(rb, nb), S.summarize(rp)
+        byid = {r.rid: r for r in rp}
+        same = all(r.status == "ok" and byid[r.rid].status == "ok" and _same_result(r.result, byid[r.rid].result)
+                   for r in rb)
+        checked = checked and same
         per_rate.append({"offered_qps": rate, "requests": n,
                          "batched": {"qps": sb.qps, "p50_ms": sb.p50_ms, "p99_ms": sb.p99_ms,
                                      "mean_batch": sb.mean_batch, "by_kind": sb.by_kind},
@@ -328,6 +394,7 @@ def run_serving(a) -> None:
         batched.batches = 0
     top = per_rate[-1]
     line = {"metric": "serving queries/sec with p50/p99 latency", "value": top["batched"]["qps"],
+            "checked": checked,
             "unit": "queries/s", "n_gpus": 1, "higher_is_better": True,
             "p50_ms": top["batched"]["p50_ms"], "p99_ms": top["batched"]["p99_ms"],
             "plain_qps": top["plain"]["qps"], "plain_p50_ms": top["plain"]["p50_ms"],
@@ -340,10 +407,25 @@ def run_serving(a) -> None:
                                    "continuous batching (<=64 per launch, 2 in flight per lane) vs one launch "
                                    "per query; latency = arrival to result on the host"},
             "data": "synthetic (seeded counter-based generator, generated in HBM)"}
-    print(json.dumps(line), flush=True)
+    batched.engine.close()
+    for c in batched.contexts:
+        c.close()
+    ctx.close()
+    return line
+
+
+def _same_result(x, y) -> bool:
+    import numpy as np
+    if isinstance(x, (tuple, list)):
+        return len(x) == len(y) and all(_same_result(u, v) for u, v in zip(x, y))
+    return bool(np.array_equal(np.asarray(x), np.asarray(y)))
 
 
 def run_operators(a) -> None:
+    print(json.dumps(operators_result(a)), flush=True)
+
+
+def operators_result(a) -> dict:
     """Operator configuration at --op-rows int32 rows: select (col < t) to row
     ids at four selectivities, gather of 4 columns by those ids, hash join
     (2^24 unique build keys; probe keys uniform or Zipf(1.0) over them, half
@@ -483,7 +565,8 @@ def run_operators(a) -> None:
                                    "columns, hash join 2^24 build / uniform and Zipf(1.0) probes at 50% match, "
                                    "hash group-by at 16/4096/2^20/2^22 groups)"},
             "data": "synthetic (seeded counter-based generator, generated in HBM)"}
-    print(json.dumps(line), flush=True)
+    ctx.close()
+    return line
 
 
 def run_hostscan(a) -> None:
@@ -664,16 +747,28 @@ def main() -> None:
         except Exception:
             traffic = None
 
+    # The timed query's result, and SUM(M1+M2) on the same table, the
+    # reference's own aggregate (its int return is that modulo 2^32): both
+    # untimed, for the parity check of the CPU-baseline leg.
+    gs_h = tot_h = None
+    if world == 1:
+        gs_h, tot_h = gs.cpu().numpy(), tot.cpu().numpy()
+    _, tot_pm = olapcore.starjoin_groupsum(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G,
+                                           aggs=(olapcore.AGG_M1_PLUS_M2,), dimvec_lens=s.probe_lens,
+                                           want_groups=False, ctx=ctx)
+    sum_pm = int(tot_pm.cpu()[0])
+    range_errors = ctx.take_range_errors()
+
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": a.steps,
         "warmup": max(3, a.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic (seeded counter-based generator, generated in HBM)",
-        "config": {"workload": WORKLOAD, "rows_per_gpu": a.rows, "dim_sizes": list(DIM_SIZES),
-                   "sele": a.sele, "groups": a.groups, "fk_dist": a.fk_dist,
-                   "group_nums": G, "l2": "inputs 14.4 GB/GPU > 126 MB L2; no flush",
-                   "plan": plan or "automatic",
-                   "parallelism": f"row shards x{world}" + (", NCCL all-reduce of group vector" if world > 1 else "")},
+        "config": bench_config(a, world),
+        "aggregate": "SUM(m1) and SUM(m1*m2) per group, int64",
+        "plan": plan or "automatic",
+        "exchange": "NCCL all-reduce of the int64 group vector" if world > 1 else None,
+        "check": {"sum_m1_plus_m2_mod_2^32": sum_pm & 0xFFFFFFFF, "range_errors": range_errors},
         "hbm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
@@ -691,17 +786,144 @@ def main() -> None:
         line["gpu_launches"] = a.steps * per_query + line["e2e"].pop("_launches") * (
             1 if a.e2e_mode == "inplace" else per_query)
     if rank == 0 and world == 1 and not a.no_cpu:
-        try:
-            cb = cpu_reference(min(a.rows, a.cpu_sample_rows), a.sele, a.groups, 3, 1)
-            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
-        except Exception as e:  # the baseline is reported, never the target
-            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        line["cpu_baseline"], line["parity"] = cpu_leg(a, gs_h, tot_h, sum_pm)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    if rank == 0 and world == 1 and not a.no_secondary:
+        del s, gs, tot
+        torch.cuda.empty_cache()
+        line["secondary"] = secondary_results(a, ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def secondary_results(a, ctx) -> dict:
+    """Compact, time-bounded lines of the other configurations, measured in
+    the same run on the same GPU (each with its own clock record): the
+    batched launch (64 queries) against one launch per query, serving at one
+    offered rate, the operator set at 2^28 rows, and three points of the
+    star-join sweep.  Each sub-run checks its results (batched and serving
+    against the same queries run alone or one launch each, operators against
+    a torch restatement on the device)."""
+    import copy
+    import torch
+    out = {}
+    b = copy.copy(a)
+    b.steps = min(a.steps, 10)
+    b.warmup = min(a.warmup, 3)
+    try:
+        r = batched_result(b)
+        out["batched"] = {k: r[k] for k in ("value", "unit", "ms_per_batch", "plain_ms_per_batch",
+                                            "plain_queries_per_s", "speedup_vs_one_launch_per_query",
+                                            "steps", "clocks", "checked")}
+        out["batched"]["queries_per_batch"] = a.queries
+        out["batched"]["launch_shape"] = r["config"]["launch_shape"]
+    except Exception as e:
+        out["batched"] = {"error": str(e)[:300]}
+    torch.cuda.empty_cache()
+    try:
+        b.rates = [2000.0]
+        b.serve_seconds = 2.0
+        r = serving_result(b)
+        pr = r["per_rate"][0]
+        out["serving"] = {"offered_qps": pr["offered_qps"], "requests": pr["requests"],
+                          "qps": pr["batched"]["qps"], "p50_ms": pr["batched"]["p50_ms"],
+                          "p99_ms": pr["batched"]["p99_ms"], "mean_batch": pr["batched"]["mean_batch"],
+                          "plain_qps": pr["plain"]["qps"], "plain_p50_ms": pr["plain"]["p50_ms"],
+                          "plain_p99_ms": pr["plain"]["p99_ms"], "clocks": pr["clocks"],
+                          "checked": r.get("checked"), "mix": "70% star-joins, 30% Q5 chains"}
+    except Exception as e:
+        out["serving"] = {"error": str(e)[:300]}
+    torch.cuda.empty_cache()
+    try:
+        r = operators_result(b)
+        out["operators"] = {"rows": r["rows"], "all_checked": r["all_checked"], "peak_GBs": r["peak_GBs"],
+                            "clocks": r["clocks"],
+                            "ops": [{k: v for k, v in o.items() if k in ("op", "ms", "alg_GBs", "frac_of_peak",
+                                                                         "selectivity", "keys", "groups", "checked")}
+                                    for o in r["operators"]]}
+    except Exception as e:
+        out["operators"] = {"error": str(e)[:300]}
+    torch.cuda.empty_cache()
+    out["sweep"] = []
+    for name, sele, groups, dist in (("zipf0.8", a.sele, a.groups, "zipf"),
+                                     ("joint_sel_0.52", [0.85] * 4, a.groups, "uniform"),
+                                     ("groups_2^20", a.sele, [32] * 4, "uniform")):
+        try:
+            out["sweep"].append(sweep_point(a, ctx, name, sele, groups, dist))
+        except Exception as e:
+            out["sweep"].append({"point": name, "error": str(e)[:300]})
+        torch.cuda.empty_cache()
+    return out
+
+
+def sweep_point(a, ctx, name, sele, groups, fk_dist) -> dict:
+    """One star-join point of the sweep over the full 600M-row table: the
+    autotuned plan, 10 timed launches (CUDA events on the context stream)."""
+    import torch
+    from memory_database_b200 import olapcore, workloads
+    s = workloads.make_star_schema(ctx, a.rows, DIM_SIZES, sele, groups, fk_dist=fk_dist, seed=42)
+    aggs = (olapcore.AGG_M1, olapcore.AGG_M1_TIMES_M2)
+    G = s.group_nums
+    for k in range(16):
+        ctx.set_tuning(k, 0)
+    knobs, _ = olapcore.autotune(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,
+                                 dimvec_lens=s.probe_lens, ctx=ctx)
+    gs = torch.empty((2, G), dtype=torch.int64, device="cuda")
+    tot = torch.empty((2,), dtype=torch.int64, device="cuda")
+
+    def step():
+        olapcore.starjoin_groupsum(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,
+                                   dimvec_lens=s.probe_lens, ctx=ctx, out=gs, totals_out=tot)
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    steps = 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        e0.record()
+        for _ in range(steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    peak, _ = measured_peak_gbs()
+    gbs = a.rows * s.bytes_per_row(2) / (ms / 1e3) / 1e9
+    joint = 1.0
+    for x in sele:
+        joint *= x
+    for k in range(16):
+        ctx.set_tuning(k, 0)
+    return {"point": name, "fk_dist": fk_dist, "sele": list(sele), "joint_selectivity": joint,
+            "group_nums": G, "ms": ms, "rows_per_s": a.rows / (ms / 1e3), "alg_GBs": gbs,
+            "frac_of_peak": gbs / peak, "range_errors": ctx.take_range_errors(),
+            "plan": {str(k): v for k, v in enumerate(knobs) if v}, "clocks": clk.summary()}
+
+
+def cpu_leg(a, gs_h, tot_h, sum_pm):
+    """The CPU baseline (the reference's own fan-outs on the same table in
+    host memory, every host thread) and, as the checker, the oracle's
+    per-group sums of that table against the timed query's result."""
+    import numpy as np
+    import oracle
+    from memory_database_b200 import olapcore
+    try:
+        h = host_tables(a)
+        cb = reference_cpu(h, 3, 1)
+        o_gs, o_tot, o_err = oracle.starjoin(h.probe_dims, h.probe_fks, h.factor, h.m1, h.m2, h.group_nums,
+                                             aggs=(olapcore.AGG_M1, olapcore.AGG_M1_TIMES_M2), nthreads=cb["cores"])
+        parity = {"rows": h.n_rows, "oracle": "oracle_starjoin (restated OLAPcore_vwm_sv, int64)",
+                  "groups_equal": bool(np.array_equal(gs_h, o_gs)), "totals_equal": bool(np.array_equal(tot_h, o_tot)),
+                  "oracle_range_errors": int(o_err),
+                  "sum_m1_plus_m2_equal_to_reference_mod_2^32": (sum_pm & 0xFFFFFFFF) == cb["sum_m1_plus_m2_mod_2^32"],
+                  "reference_check_from": cb["best"] if cb["kind"] == "port" else "OLAPcore_vwm_sv"}
+        base = {"value": cb["value"], "unit": "rows/s", "cores": cb["cores"], "kind": cb["kind"],
+                "sample": cb["sample"], "variants": cb.get("variants")}
+        return base, parity
+    except Exception as e:  # the baseline is reported, never the target
+        return {"value": None, "error": str(e)[:200]}, {"error": str(e)[:200]}
 
 
 def e2e_host(a, s, ctx, aggs, world, knobs) -> dict:

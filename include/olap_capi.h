@@ -326,6 +326,15 @@ OLAP_API int olap_selalgo(olap_ctx* ctx, int32_t condition, int64_t n, const int
  * proalgo_cwm_lm_* (project/test_project_option.cpp:34-864). */
 OLAP_API int olap_project_pairs(olap_ctx* ctx, int32_t condition, int64_t n, const int32_t* Ra,
                                 const int32_t* Rc, int32_t* out_a, int32_t* out_c, int64_t* d_count);
+/* proalgo_rowwise over a row store (project/test_project_option.cpp:34-147,
+ * rows of struct row_store_min / row_store_max, include/metadata.h:251-262):
+ * the pairs (Ra, Rc) of the rows r < n with Ra <= condition and Rc <=
+ * condition, in row order, where Ra and Rc are the int32 fields at byte
+ * offsets off_a and off_c of each row_bytes-long row (rows, row_bytes and
+ * both offsets 4-byte aligned).  Device pointers; *d_count gets the count. */
+OLAP_API int olap_project_pairs_rows(olap_ctx* ctx, int32_t condition, int64_t n, const void* rows,
+                                     int64_t row_bytes, int64_t off_a, int64_t off_c, int32_t* out_a,
+                                     int32_t* out_c, int64_t* d_count);
 /* Late materialisation: outs[c][i] = cols[c][rowids[i]] for 1..8 int32
  * columns of col_len rows (a row id outside [0, col_len) gives 0 and is
  * counted as a range error). */
@@ -351,6 +360,21 @@ OLAP_API int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32
 OLAP_API int olap_hashjoin_probe(olap_ctx* ctx, const uint64_t* table, int64_t capacity,
                                  const int32_t* keys, int64_t n, int64_t* d_sum, int64_t* d_matches,
                                  int32_t* out_rows, int32_t* out_payload);
+/* Blocked Bloom filter of the build keys, kept beside the table (no
+ * counterpart in the reference): `words` 64-bit words, a power of two
+ * (olap_hashjoin_filter_words(n_build) gives about 8 bits per key: 16 MB for
+ * 2^24 keys, which stays in L2).  A probe through the filter skips the table
+ * for the keys that cannot match (all but about 2-4 % of them), so a probe
+ * side whose keys often miss reads far less of the table.  Asynchronous. */
+OLAP_API int64_t olap_hashjoin_filter_words(int64_t n_build);
+OLAP_API int olap_hashjoin_build_filter(olap_ctx* ctx, const int32_t* keys, int64_t n, uint64_t* filter,
+                                        int64_t words);
+/* olap_hashjoin_probe through the filter built from the same build keys
+ * (filter NULL: no filter); the same results. */
+OLAP_API int olap_hashjoin_probe_filtered(olap_ctx* ctx, const uint64_t* table, int64_t capacity,
+                                          const uint64_t* filter, int64_t words, const int32_t* keys, int64_t n,
+                                          int64_t* d_sum, int64_t* d_matches, int32_t* out_rows,
+                                          int32_t* out_payload);
 /* build(relation_t*, int* vector) (join:30-36): vector[key] = payload (last
  * row wins); keys outside [0, vector_len) are counted as range errors.
  * Entries not built are left as they are. */
@@ -391,6 +415,20 @@ OLAP_API int olap_agg_fixed(olap_ctx* ctx, int64_t n, const int32_t* price, cons
  * differs from a sequential CPU sum only by rounding). */
 OLAP_API int olap_agg_f64(olap_ctx* ctx, int64_t n, const double* tax, const double* qty,
                           const double* price, double* d_sum);
+
+/* ---- device buffers for host-memory callers ---------------------------------
+ * No counterpart in the reference, whose operators take host arrays: the C++
+ * drop-in header (olap_reference_api.hpp) moves a host caller's arrays
+ * through these (allocate, copy in, run the device entry point, copy out).
+ * Copies are synchronous on the context's stream. */
+OLAP_API int olap_buffer_alloc(olap_ctx* ctx, size_t bytes, void** dev);
+OLAP_API int olap_buffer_free(olap_ctx* ctx, void* dev);
+OLAP_API int olap_copy_h2d(olap_ctx* ctx, void* dev, const void* host, size_t bytes);
+OLAP_API int olap_copy_d2h(olap_ctx* ctx, void* host, const void* dev, size_t bytes);
+/* Largest value of a device int32 column into *h_max (INT32_MIN when n is
+ * 0); synchronous.  Sizes the arrays the reference indexes by key without
+ * passing their length (dimension vectors, join vectors). */
+OLAP_API int olap_max_i32(olap_ctx* ctx, const int32_t* col, int64_t n, int32_t* h_max);
 
 /* ---- dimension-vector builder and batched multi-query star-join -------------
  * Dimension tables as attributes: per dimension row an int32 filter attribute

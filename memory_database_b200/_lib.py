@@ -149,10 +149,19 @@ def _load() -> C.CDLL:
         "olap_select_bitmap": (C.c_int, [vp, vp, i64, i32, C.c_int, vp]),
         "olap_selalgo": (C.c_int, [vp, i32, i64, vp, vp, vp, vp, vp, vp]),
         "olap_project_pairs": (C.c_int, [vp, i32, i64, vp, vp, vp, vp, vp]),
+        "olap_project_pairs_rows": (C.c_int, [vp, i32, i64, vp, i64, i64, i64, vp, vp, vp]),
         "olap_gather_i32": (C.c_int, [vp, vp, i64, C.c_int, vp, i64, vp]),
+        "olap_buffer_alloc": (C.c_int, [vp, C.c_size_t, C.POINTER(vp)]),
+        "olap_buffer_free": (C.c_int, [vp, vp]),
+        "olap_copy_h2d": (C.c_int, [vp, vp, vp, C.c_size_t]),
+        "olap_copy_d2h": (C.c_int, [vp, vp, vp, C.c_size_t]),
+        "olap_max_i32": (C.c_int, [vp, vp, i64, C.POINTER(i32)]),
         "olap_hashtable_capacity": (i64, [i64]),
         "olap_hashjoin_build": (C.c_int, [vp, vp, vp, i64, vp, i64]),
         "olap_hashjoin_probe": (C.c_int, [vp, vp, i64, vp, i64, vp, vp, vp, vp]),
+        "olap_hashjoin_filter_words": (i64, [i64]),
+        "olap_hashjoin_build_filter": (C.c_int, [vp, vp, i64, vp, i64]),
+        "olap_hashjoin_probe_filtered": (C.c_int, [vp, vp, i64, vp, i64, vp, i64, vp, vp, vp, vp]),
         "olap_vecjoin_build": (C.c_int, [vp, vp, vp, i64, vp, i64]),
         "olap_vecjoin_probe": (C.c_int, [vp, vp, i64, vp, i64, vp]),
         "olap_group_vector": (C.c_int, [vp, i64, vp, vp, vp, i64, vp, vp, vp]),

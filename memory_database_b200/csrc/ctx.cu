@@ -20,6 +20,16 @@ int check_cuda(olap_ctx* ctx, cudaError_t e, const char* what) {
   return set_error(ctx, st, m);
 }
 
+// Largest value of a column: per-warp maxima, one atomicMax per warp.
+__global__ void max_i32_kernel(const int32_t* __restrict__ col, int64_t n, int* out) {
+  int m = INT32_MIN;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    m = max(m, __ldg(col + i));
+  m = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0 && m != INT32_MIN) atomicMax(out, m);
+}
+
 }  // namespace olap
 
 extern "C" {
@@ -201,6 +211,66 @@ int olap_plan_olapcore(const double sele[4], const int bitmap[4], const int grou
   }
   *dimvec_nums = nd;
   *group_nums = g;
+  return OLAP_OK;
+}
+
+int olap_buffer_alloc(olap_ctx* ctx, size_t bytes, void** dev) {
+  if (!ctx || !dev) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  *dev = nullptr;
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_CUDA_TRY(ctx, cudaMalloc(dev, bytes ? bytes : 1));
+  return OLAP_OK;
+}
+
+int olap_buffer_free(olap_ctx* ctx, void* dev) {
+  if (!ctx) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!dev) return OLAP_OK;
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  OLAP_CUDA_TRY(ctx, cudaFree(dev));
+  return OLAP_OK;
+}
+
+int olap_copy_h2d(olap_ctx* ctx, void* dev, const void* host, size_t bytes) {
+  if (!ctx || (bytes && (!dev || !host))) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!bytes) return OLAP_OK;
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return OLAP_OK;
+}
+
+int olap_copy_d2h(olap_ctx* ctx, void* host, const void* dev, size_t bytes) {
+  if (!ctx || (bytes && (!dev || !host))) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!bytes) return OLAP_OK;
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return OLAP_OK;
+}
+
+int olap_max_i32(olap_ctx* ctx, const int32_t* col, int64_t n, int32_t* h_max) {
+  if (!ctx || !h_max || n < 0 || (n > 0 && !col)) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  *h_max = INT32_MIN;
+  if (n == 0) return OLAP_OK;
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  olap::Arena ar(ctx);
+  int* d = ar.take<int>(1);
+  if (!d) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
+  const int init = INT32_MIN;
+  OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(d, &init, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  const int64_t blocks = std::min<int64_t>(int64_t(ctx->sm_count) * 4, (n + 255) / 256);
+  olap::max_i32_kernel<<<static_cast<unsigned>(blocks), 256, 0, ctx->stream>>>(col, n, d);
+  OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  int v = INT32_MIN;
+  OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(&v, d, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  *h_max = v;
   return OLAP_OK;
 }
 

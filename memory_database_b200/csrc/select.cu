@@ -135,6 +135,47 @@ struct ProjectOp {
   }
 };
 
+// Rows of a row store (an array of structs, row_bytes apart): the pair (Ra,
+// Rc) read as int32 at byte offsets off_a and off_c of each row, for the rows
+// where both are <= c (proalgo_rowwise over row_store_min / row_store_max,
+// project/test_project_option.cpp:34-147).  Rows are not 16-byte vectors, so
+// every group takes the per-row loads.
+struct ProjectRowsOp {
+  static constexpr int kGroups = kCompactGroups;
+  const unsigned char* rows;
+  int64_t row_bytes;
+  int32_t off_a, off_c;
+  int32_t* out_a;
+  int32_t* out_c;
+  int32_t cond;
+  int4 a[kCompactGroups], c[kCompactGroups];
+
+  __device__ __forceinline__ bool vec_ok() const { return false; }
+  __device__ __forceinline__ void prefetch(int, int64_t) {}
+  template <bool kFull>
+  __device__ __forceinline__ uint32_t flags(int u, int64_t first, int nv) {
+    int32_t x[4] = {0, 0, 0, 0}, y[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k >= nv) continue;
+      const unsigned char* r = rows + (first + k) * row_bytes;
+      x[k] = __ldg(reinterpret_cast<const int32_t*>(r + off_a));
+      y[k] = __ldg(reinterpret_cast<const int32_t*>(r + off_c));
+    }
+    a[u] = make_int4(x[0], x[1], x[2], x[3]);
+    c[u] = make_int4(y[0], y[1], y[2], y[3]);
+    uint32_t m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < nv) m |= static_cast<uint32_t>(x[k] <= cond && y[k] <= cond) << k;
+    return m;
+  }
+  __device__ __forceinline__ void emit(int u, int k, int64_t, int64_t pos) {
+    out_a[pos] = lane4(a[u], k);
+    out_c[pos] = lane4(c[u], k);
+  }
+};
+
 // One 32-bit word of the bitmap per warp step: lane l tests row 32w + l.
 __global__ void select_bitmap_kernel(const int32_t* __restrict__ col, int64_t n, int32_t val, int cmp,
                                      uint32_t* __restrict__ bits) {
@@ -370,6 +411,30 @@ int olap_project_pairs(olap_ctx* ctx, int32_t condition, int64_t n, const int32_
   op.out_c = out_c;
   op.cond = condition;
   op.vec = olap::al16(Ra) && olap::al16(Rc);
+  return olap::run_compaction(ctx, op, n, d_count);
+}
+
+int olap_project_pairs_rows(olap_ctx* ctx, int32_t condition, int64_t n, const void* rows, int64_t row_bytes,
+                            int64_t off_a, int64_t off_c, int32_t* out_a, int32_t* out_c, int64_t* d_count) {
+  if (!ctx) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  OLAP_REQUIRE(ctx, n >= 0 && n <= INT32_MAX, "n must be in [0, 2^31)");
+  OLAP_REQUIRE(ctx, n == 0 || (rows && out_a && out_c), "null rows or output");
+  OLAP_REQUIRE(ctx, row_bytes >= 4 && row_bytes % 4 == 0, "row_bytes must be a positive multiple of 4");
+  OLAP_REQUIRE(ctx, off_a >= 0 && off_c >= 0 && off_a % 4 == 0 && off_c % 4 == 0 && off_a + 4 <= row_bytes &&
+                        off_c + 4 <= row_bytes,
+               "field offsets must be 4-byte aligned and inside the row");
+  OLAP_REQUIRE(ctx, (reinterpret_cast<uintptr_t>(rows) & 3) == 0, "rows must be 4-byte aligned");
+  olap::ProjectRowsOp op;
+  std::memset(&op, 0, sizeof(op));
+  op.rows = static_cast<const unsigned char*>(rows);
+  op.row_bytes = row_bytes;
+  op.off_a = static_cast<int32_t>(off_a);
+  op.off_c = static_cast<int32_t>(off_c);
+  op.out_a = out_a;
+  op.out_c = out_c;
+  op.cond = condition;
   return olap::run_compaction(ctx, op, n, d_count);
 }
 

@@ -20,7 +20,7 @@ from .olapcore import Context, default_context, _ptr, _nelem
 __all__ = [
     "CMP_LE", "CMP_LT",
     "select_rowids", "select_bitmap", "sel_lt_T_fsel_independent_val_branching", "selalgo_rowwise",
-    "proalgo_rowwise", "gather",
+    "proalgo_rowwise", "proalgo_rowwise_rows", "gather",
     "HashTable", "vecjoin_build", "vecjoin_probe",
     "vector_group", "hashtable_group", "group_hash",
     "aggalgo_fixed", "aggalgo_f64",
@@ -109,6 +109,26 @@ def proalgo_rowwise(condition: int, size_R: int, Ra, Rc, ctx: Context | None = N
     return k, oa[:k], oc[:k]
 
 
+def proalgo_rowwise_rows(condition: int, size_R: int, rows, row_bytes: int, off_a: int = 0,
+                         off_c: int | None = None, ctx: Context | None = None):
+    """project/test_project_option.cpp:34-147 over a row store: ``rows`` is a
+    CUDA tensor holding size_R rows of ``row_bytes`` bytes (the reference's
+    row_store_min is 60 bytes with Ra at 0 and Rc at 56, row_store_max 72
+    bytes with Rc at 68); returns ``(count, out_a, out_c)`` for the rows with
+    Ra <= condition and Rc <= condition, in row order."""
+    torch = _torch()
+    c = _ctx(ctx)
+    n = int(size_R)
+    oc_off = int(row_bytes) - 4 if off_c is None else int(off_c)
+    oa = torch.empty(max(n, 1), dtype=torch.int32, device=rows.device)
+    oc = torch.empty(max(n, 1), dtype=torch.int32, device=rows.device)
+    cnt = _i64(rows.device)
+    check(lib.olap_project_pairs_rows(c.handle, int(condition), n, _ptr(rows), int(row_bytes), int(off_a), oc_off,
+                                      _ptr(oa), _ptr(oc), _ptr(cnt)), c.handle)
+    k = int(cnt.item())
+    return k, oa[:k], oc[:k]
+
+
 def gather(rowids, cols: Sequence, ctx: Context | None = None):
     """Late materialisation: ``[col[rowids] for col in cols]`` (1..8 int32 columns)."""
     torch = _torch()
@@ -125,26 +145,35 @@ def gather(rowids, cols: Sequence, ctx: Context | None = None):
 
 class HashTable:
     """Open-addressing build table of ``build(relation_t*, unordered_map&)``
-    (join/test_join_option.cpp:44-50); ``probe`` mirrors ``probe`` (:90-96)."""
+    (join/test_join_option.cpp:44-50); ``probe`` mirrors ``probe`` (:90-96).
+    With ``bloom`` (the default) a blocked Bloom filter of the build keys is
+    kept beside the table and probes go through it (same results; probe keys
+    that cannot match skip the table)."""
 
-    def __init__(self, n_build: int, device="cuda", ctx: Context | None = None):
+    def __init__(self, n_build: int, device="cuda", ctx: Context | None = None, bloom: bool = True):
         torch = _torch()
         self.capacity = int(lib.olap_hashtable_capacity(int(n_build)))
         self.table = torch.empty(self.capacity, dtype=torch.int64, device=device)
+        self.words = int(lib.olap_hashjoin_filter_words(int(n_build))) if bloom else 0
+        self.filter = torch.empty(self.words, dtype=torch.int64, device=device) if bloom else None
         self.ctx = ctx
 
     def build(self, keys, payload) -> "HashTable":
         c = _ctx(self.ctx)
         check(lib.olap_hashjoin_build(c.handle, _ptr(keys), _ptr(payload), _nelem(keys), _ptr(self.table),
                                       self.capacity), c.handle)
+        if self.filter is not None:
+            check(lib.olap_hashjoin_build_filter(c.handle, _ptr(keys), _nelem(keys), _ptr(self.filter), self.words),
+                  c.handle)
         return self
 
     def probe(self, keys) -> tuple[int, int]:
         """``(SUM of matched payloads, matches)``."""
         c = _ctx(self.ctx)
         s, m = _i64(keys.device), _i64(keys.device)
-        check(lib.olap_hashjoin_probe(c.handle, _ptr(self.table), self.capacity, _ptr(keys), _nelem(keys),
-                                      _ptr(s), _ptr(m), None, None), c.handle)
+        check(lib.olap_hashjoin_probe_filtered(c.handle, _ptr(self.table), self.capacity, _ptr(self.filter),
+                                               self.words, _ptr(keys), _nelem(keys), _ptr(s), _ptr(m), None, None),
+              c.handle)
         return int(s.item()), int(m.item())
 
     def probe_pairs(self, keys):
@@ -155,8 +184,9 @@ class HashTable:
         rows = torch.empty(max(n, 1), dtype=torch.int32, device=keys.device)
         pay = torch.empty(max(n, 1), dtype=torch.int32, device=keys.device)
         m = _i64(keys.device)
-        check(lib.olap_hashjoin_probe(c.handle, _ptr(self.table), self.capacity, _ptr(keys), n, None,
-                                      _ptr(m), _ptr(rows), _ptr(pay)), c.handle)
+        check(lib.olap_hashjoin_probe_filtered(c.handle, _ptr(self.table), self.capacity, _ptr(self.filter),
+                                               self.words, _ptr(keys), n, None, _ptr(m), _ptr(rows), _ptr(pay)),
+              c.handle)
         k = int(m.item())
         return rows[:k], pay[:k]
 

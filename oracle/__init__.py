@@ -434,7 +434,7 @@ def starjoin_cwm_sv(dimvecs, lens, fks, n):
 
 def ref_module(name: str) -> C.CDLL:
     """The reference's own operator module (select, join, group, aggregation,
-    starjoin) compiled from its sources into oracle/_ref."""
+    starjoin, project) compiled from its sources into oracle/_ref."""
     path = HERE / "_ref" / f"libref_{name}.so"
     if not path.exists():
         raise FileNotFoundError(f"{path} not built (needs the reference tree)")
@@ -455,6 +455,12 @@ def ref_module(name: str) -> C.CDLL:
     elif name == "aggregation":
         lib.ref_aggalgo_rowwise.argtypes = [C.c_int, _vp, _vp, _vp]
         lib.ref_aggalgo_rowwise.restype = C.c_double
+    elif name == "project":
+        for fn in ("ref_proalgo_cwm_lm_ifv", "ref_proalgo_cwm_em"):
+            getattr(lib, fn).argtypes = [C.c_int, C.c_int, _vp, _vp, _vp, _vp]
+            getattr(lib, fn).restype = C.c_int
+        lib.ref_proalgo_rowwise.argtypes = [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp]
+        lib.ref_proalgo_rowwise.restype = C.c_int
     elif name == "starjoin":
         lib.ref_starjoin_rowwise.argtypes = [C.c_int] + [_vp] * 8
         lib.ref_starjoin_cwm_sv.argtypes = [C.c_int] + [_vp] * 9

@@ -1,5 +1,5 @@
 // C-linkage bridges over the reference's operator modules (select, join,
-// group, aggregation, starjoin), one shared object per module.
+// group, aggregation, starjoin, project), one shared object per module.
 //
 // TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file once per
 // module with -DREF_MODULE_<NAME> and that module's directory on the include
@@ -92,6 +92,47 @@ int ref_starjoin_cwm_sv(int n, const int8_t* dc, const int8_t* ds, const int8_t*
                         int* result) {
   for (int i = 0; i < n; ++i) result[i] = 0;
   return starjoinalgo_cwm_sv(n, dc, ds, dp, dd, fc, fs, fp, fd, result);
+}
+}
+#elif defined(REF_MODULE_PROJECT)
+#include "test_project_option.cpp"
+extern "C" {
+// proalgo_rowwise over the module's own row stores (project/test_project_option
+// .cpp:62-90 and :120-147, the static row_min / row_max arrays it declares at
+// :20-21): the columns are written into the rows' Ra and Rc fields first, the
+// pairs come back as two int arrays.  which: 0 row_store_min, 1
+// row_store_max; n at most 2^26 (the arrays' length).
+int ref_proalgo_rowwise(int which, int cond, int n, const int* Ra, const int* Rc, int* out_a, int* out_c) {
+  fixed_arrays res;
+  res.pos_value1 = out_a;
+  res.value2 = out_c;
+  if (which == 0) {
+    for (int i = 0; i < n; ++i) {
+      row_min[i].Ra = Ra[i];
+      row_min[i].Rc = Rc[i];
+    }
+    return proalgo_rowwise(cond, n, row_min, res);
+  }
+  for (int i = 0; i < n; ++i) {
+    row_max[i].Ra = Ra[i];
+    row_max[i].Rc = Rc[i];
+  }
+  return proalgo_rowwise(cond, n, row_max, res);
+}
+// proalgo_cwm_lm_ifv (:527-595), late materialisation over the columns.
+int ref_proalgo_cwm_lm_ifv(int cond, int n, const int* Ra, const int* Rc, int* out_a, int* out_c) {
+  std::vector<int> pos1(n > 0 ? n : 1), pos2(n > 0 ? n : 1);
+  fixed_arrays res;
+  res.pos_value1 = out_a;
+  res.value2 = out_c;
+  return proalgo_cwm_lm_ifv(cond, n, Ra, Rc, pos1.data(), pos2.data(), res, 0);
+}
+// proalgo_cwm_em (:190-232), early materialisation, with pre_size 0.
+int ref_proalgo_cwm_em(int cond, int n, const int* Ra, const int* Rc, int* out_a, int* out_c) {
+  fixed_arrays res;
+  res.pos_value1 = out_a;
+  res.value2 = out_c;
+  return proalgo_cwm_em(cond, n, Ra, Rc, res, 0);
 }
 }
 #endif

@@ -90,6 +90,25 @@ def test_selalgo_and_project(ctx):
     assert np.array_equal(host(oa), ea) and np.array_equal(host(oc), ec)
 
 
+@pytest.mark.parametrize("row_bytes,rb_bytes", [(60, 52), (72, 64)])
+@pytest.mark.parametrize("n", [0, 1, 5, 4097, 1_000_003])
+def test_project_row_store(ctx, row_bytes, rb_bytes, n):
+    """proalgo_rowwise over the reference's row stores (row_store_min: Ra,
+    char Rb[52], Rc; row_store_max: Rb[64]): the pairs equal the oracle's."""
+    rng = np.random.default_rng(n + row_bytes)
+    dt = np.dtype([("Ra", "<i4"), ("Rb", f"V{rb_bytes}"), ("Rc", "<i4")])
+    assert dt.itemsize == row_bytes
+    rows = np.zeros(n, dt)
+    rows["Ra"] = rng.integers(1, 1001, n)
+    rows["Rc"] = rng.integers(1, 1001, n)
+    rows["Rb"] = rng.integers(0, 256, (n, rb_bytes), dtype=np.uint8).view(f"V{rb_bytes}").reshape(n)
+    d = torch.from_numpy(rows.view(np.uint8).reshape(-1).copy()).cuda()
+    for cond in (0, 1, 300, 1000):
+        k, oa, oc = ops.proalgo_rowwise_rows(cond, n, d, row_bytes, ctx=ctx)
+        ea, ec = oracle.project_pairs(cond, rows["Ra"].copy(), rows["Rc"].copy())
+        assert k == len(ea) and np.array_equal(host(oa), ea) and np.array_equal(host(oc), ec)
+
+
 def test_gather_out_of_range(ctx):
     col = np.arange(100, dtype=np.int32) * 3
     ids = np.array([0, 99, 100, -1, 50, 7, 7], np.int32)
@@ -99,9 +118,11 @@ def test_gather_out_of_range(ctx):
 
 
 @pytest.mark.parametrize("dist", ["uniform", "zipf"])
-def test_hash_join_config2_shape(ctx, dist):
+@pytest.mark.parametrize("bloom", [True, False])
+def test_hash_join_config2_shape(ctx, dist, bloom):
     """2^20-row build side of unique shuffled keys, 2^24 probe keys over the
-    build keys (uniform or Zipf(1.0)), half of them made non-matching."""
+    build keys (uniform or Zipf(1.0)), half of them made non-matching; with
+    and without the Bloom filter, and on unaligned probe keys (scalar path)."""
     rng = np.random.default_rng(9)
     R, S = 1 << 20, 1 << 24
     rk = rng.permutation(np.arange(1, R + 1)).astype(np.int32)
@@ -115,26 +136,32 @@ def test_hash_join_config2_shape(ctx, dist):
     ctx.synchronize()
     sk = rk[host(pos)]
     sk = np.where(rng.random(S) < 0.5, sk, sk + 4 * R).astype(np.int32)
-    ht = ops.HashTable(R, ctx=ctx).build(dev(rk), dev(rp))
+    ht = ops.HashTable(R, ctx=ctx, bloom=bloom).build(dev(rk), dev(rp))
     s, m = ht.probe(dev(sk))
     es, em = oracle.hashjoin(rk, rp, sk)
     assert (s, m) == (es, em)
     rows, pay = ht.probe_pairs(dev(sk[:500_000]))
     es2, em2, erows, epay = oracle.hashjoin(rk, rp, sk[:500_000], want_pairs=True)
     assert np.array_equal(host(rows), erows) and np.array_equal(host(pay), epay)
+    # unaligned probe keys
+    assert ht.probe(dev(sk[:1_000_001])[1:]) == oracle.hashjoin(rk, rp, sk[1:1_000_001])
 
 
-def test_hash_join_duplicates_and_edge_keys(ctx):
+@pytest.mark.parametrize("bloom", [True, False])
+def test_hash_join_duplicates_and_edge_keys(ctx, bloom):
     rng = np.random.default_rng(10)
     rk = rng.integers(-5000, 5000, 100_000).astype(np.int32)  # many duplicates, negatives
     rk[:3] = [np.iinfo(np.int32).min, np.iinfo(np.int32).max, 0]
     rp = np.arange(len(rk), dtype=np.int32)  # payload = row: "last row wins" visible
     sk = rng.integers(-6000, 6000, 300_001).astype(np.int32)
     sk[:2] = [np.iinfo(np.int32).min, np.iinfo(np.int32).max]
-    ht = ops.HashTable(len(rk), ctx=ctx).build(dev(rk), dev(rp))
+    ht = ops.HashTable(len(rk), ctx=ctx, bloom=bloom).build(dev(rk), dev(rp))
     assert ctx.take_range_errors() == 1  # the INT32_MIN build key
     assert ht.probe(dev(sk)) == oracle.hashjoin(rk, rp, sk)
-    empty = ops.HashTable(0, ctx=ctx).build(dev(rk[:0]), dev(rp[:0]))
+    rows, pay = ht.probe_pairs(dev(sk))
+    _, _, erows, epay = oracle.hashjoin(rk, rp, sk, want_pairs=True)
+    assert np.array_equal(host(rows), erows) and np.array_equal(host(pay), epay)
+    empty = ops.HashTable(0, ctx=ctx, bloom=bloom).build(dev(rk[:0]), dev(rp[:0]))
     assert empty.probe(dev(sk)) == (0, 0)
 
 

@@ -1,5 +1,5 @@
 """CPU tests: the oracle's operator restatements against the reference's own
-operator modules (select, join, group, aggregation, starjoin), compiled from
+operator modules (select, join, group, aggregation, starjoin, project), compiled from
 their sources into oracle/_ref.  Inputs follow the reference's generators
 (values in [1, 1000], keys 1..R shuffled, 1-based group ids)."""
 import numpy as np
@@ -137,3 +137,35 @@ def test_join_cwm_sv_matches_reference_static_vector():
     assert errs == 0 and np.array_equal(gid, gid_ref)
     gs, tot, _ = oracle.starjoin([dv[t] for t in orders], [fk[t] for t in orders], factor, m1, m2, G)
     assert int(tot[0]) == tot_ref
+
+
+@pytest.mark.parametrize("cond", [0, 1, 300, 999, 1000])
+def test_project_matches_reference(cond):
+    """oracle_project_pairs equals the reference's project module, compiled
+    from its sources: proalgo_rowwise over both of its row stores
+    (project/test_project_option.cpp:62-147, rows of row_store_min and
+    row_store_max) and proalgo_cwm_lm_ifv (:527-595).  The reference's
+    proalgo_cwm_em (:190-232) keeps the right rows and Rc values, but its
+    second pass reads value 1 back at the row id instead of the list
+    position (result.value2[cur_pos + pre_size]), so its Ra values are wrong
+    unless every row passes; the library follows the other variants."""
+    lib = _need("project")
+    rng = np.random.default_rng(cond + 11)
+    n = 1_000_003
+    ra = rng.integers(1, 1001, n).astype(np.int32)
+    rc = rng.integers(1, 1001, n).astype(np.int32)
+    ea, ec = oracle.project_pairs(cond, ra, rc)
+    p = oracle._p
+
+    def run(fn, *head):
+        oa, oc = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        k = fn(*head, cond, n, p(ra), p(rc), p(oa), p(oc))
+        return k, oa[:k], oc[:k]
+    for which in (0, 1):
+        k, oa, oc = run(lib.ref_proalgo_rowwise, which)
+        assert k == len(ea) and np.array_equal(oa, ea) and np.array_equal(oc, ec), which
+    k, oa, oc = run(lib.ref_proalgo_cwm_lm_ifv)
+    assert k == len(ea) and np.array_equal(oa, ea) and np.array_equal(oc, ec)
+    k, oa, oc = run(lib.ref_proalgo_cwm_em)
+    assert k == len(ea) and np.array_equal(oc, ec)
+    assert np.array_equal(oa, ea) == (len(ea) in (0, n))

@@ -504,11 +504,15 @@ def operators_result(a) -> dict:
     bpay = gen(nb, 110, -1000, 1000)
     cap = int(L.olap_hashtable_capacity(nb))
     table = torch.empty(cap, dtype=torch.int64, device="cuda")
+    words = int(L.olap_hashjoin_filter_words(nb))
+    bloom = torch.empty(words, dtype=torch.int64, device="cuda")
 
     def build_fn():
         _lib.check(L.olap_hashjoin_build(h, _ptr(bkeys), _ptr(bpay), nb, _ptr(table), cap), h)
+        _lib.check(L.olap_hashjoin_build_filter(h, _ptr(bkeys), nb, _ptr(bloom), words), h)
     ms = timed(build_fn, reps=3)
-    res.append(entry("hash join build (2^24 unique keys)", ms, 16 * nb, True, build_rows=nb, capacity=cap))
+    res.append(entry("hash join build (2^24 unique keys; table + Bloom filter)", ms, 16 * nb, True, build_rows=nb,
+                     capacity=cap, filter_bytes=8 * words))
     dense = torch.zeros(nb + 1, dtype=torch.int64, device="cuda")
     dense[bkeys.long()] = bpay.long()
     s_ = torch.zeros(1, dtype=torch.int64, device="cuda")
@@ -525,7 +529,8 @@ def operators_result(a) -> dict:
         del idx
 
         def probe_fn():
-            _lib.check(L.olap_hashjoin_probe(h, _ptr(table), cap, _ptr(pk), n, _ptr(s_), _ptr(m_), None, None), h)
+            _lib.check(L.olap_hashjoin_probe_filtered(h, _ptr(table), cap, _ptr(bloom), words, _ptr(pk), n, _ptr(s_),
+                                                      _ptr(m_), None, None), h)
         ms = timed(probe_fn)
         inr = pk <= nb
         exp_s = int(dense[torch.where(inr, pk, 0).long()].sum())
@@ -533,7 +538,7 @@ def operators_result(a) -> dict:
         res.append(entry("hash join probe (SUM payload, 50% match)", ms, 12 * n, ok, keys=dist,
                          matches=int(m_.item())))
         del pk, inr
-    del table, dense, bkeys, bpay, miss
+    del table, bloom, dense, bkeys, bpay, miss
     torch.cuda.empty_cache()
     vals = gen(n, 120, 1, 10000)
     for G in (16, 1 << 12, 1 << 20, 1 << 22):

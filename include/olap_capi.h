@@ -71,7 +71,8 @@ extern "C" {
 #define OLAP_TUNE_PROBE_BITS 6      /* global pass bitmaps for unstaged dims: 1 on, 2 off (default) */
 #define OLAP_TUNE_SMEM_BITS_BYTES 7 /* bytes of pass bitmaps staged in smem (default 0)          */
 #define OLAP_TUNE_GROUP_COMBINE 8   /* hash group-by warp combining of equal keys: 1 on, 2 off (default) */
-#define OLAP_TUNE_GROUP_PLAN 9      /* hash group-by: 1 per-block tables (capacity <= 8192), 2 partitioned */
+#define OLAP_TUNE_GROUP_PLAN 9      /* hash group-by: 1 per-block tables (capacity <= 8192), 2 partitioned,
+                                       3 per-block tables with two 32-bit counters per slot */
 #define OLAP_TUNE_ASYNC_LOADS 10    /* star-join: 2 prefetches fact columns by bulk async copies (TMA), 1 off */
 #define OLAP_TUNE_COMPACT 11        /* star-join: 2 compacts survivors per warp before global probes, 1 off */
 #define OLAP_TUNE_SMEM_NIB_BYTES 12 /* bytes of 4-bit code vectors staged in smem (default 0)        */
@@ -483,6 +484,14 @@ OLAP_API int olap_batch_graph_captures(olap_batch* b, int64_t* captures);
  * queries with the fewest groups accumulate there, the rest in L2).  A change
  * re-records the graphs on the next run. */
 OLAP_API int olap_batch_tune(olap_batch* b, int block, int smem_slots);
+/* Probe order of the batched scan: 0 (the default) probes the tables one
+ * after another, each only for rows that still have a live query using it;
+ * 1 reads every table's query mask in one round trip, then the group
+ * attributes of the tables a surviving query groups by (needs blocks of at
+ * most 512 threads; with larger ones the first order runs).  The autotuner
+ * tries both.  olap_batch_get_tuning reports the shape in force. */
+OLAP_API int olap_batch_set_probe(olap_batch* b, int parallel_probe);
+OLAP_API int olap_batch_get_tuning(olap_batch* b, int* block, int* smem_slots, int* parallel_probe);
 /* Times the block sizes {256, 512, 1024} x accumulator slots {0, 2048, 4096,
  * 8192, 16384} on the first sample_rows rows (0 = 64 Mi) of the fact table
  * with these queries (their ranges cut to the sample), keeps the fastest on

@@ -183,6 +183,8 @@ def _load() -> C.CDLL:
         "olap_batch_run": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, i64, C.c_int, vp, i64, vp, C.c_int]),
         "olap_batch_graph_captures": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "olap_batch_tune": (C.c_int, [vp, C.c_int, C.c_int]),
+        "olap_batch_set_probe": (C.c_int, [vp, C.c_int]),
+        "olap_batch_get_tuning": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "olap_batch_autotune": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, i64, C.c_int, vp, i64, vp, i64,
                                           C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
         "olap_debug_wait_timeout": (C.c_int, [vp, C.c_uint32]),

@@ -175,8 +175,27 @@ __device__ __forceinline__ ulonglong2 ld_record(const DimRecord* r, uint64_t pol
   return v;
 }
 
+__device__ __forceinline__ unsigned long long ld_record_mask(const DimRecord* r, uint64_t pol) {
+  unsigned long long v;
+  asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(r), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_record_grp(const DimRecord* r, uint64_t pol) {
+  int32_t v;
+  asm("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(&r->grp), "l"(pol));
+  return v;
+}
+
 // The fact pass: persistent, 4 rows per thread per step (128-bit loads).
-__global__ void __launch_bounds__(kBatchMaxThreads, 1) batch_scan_kernel(const BatchParams p) {
+// PAR = false: the tables are probed one after another, smallest first, each
+// only for the rows that still have a live query using it (up to four
+// dependent L2 round trips per step, 16-byte records).  PAR = true: every
+// used table's query mask is read in one round trip (the union of a batch's
+// predicates passes nearly every row, so the skipped probes save little),
+// then the group attributes only of the tables that a surviving query groups
+// by; more registers, so at most 512 threads per block.
+template <bool PAR>
+__global__ void __launch_bounds__(PAR ? 512 : kBatchMaxThreads, 1) batch_scan_kernel(const BatchParams p) {
   __shared__ BatchQuery sq[kMaxBatchQueries];
   __shared__ int64_t sseg[kMaxSegments];
   __shared__ unsigned long long smask[kMaxSegments];
@@ -225,6 +244,17 @@ __global__ void __launch_bounds__(kBatchMaxThreads, 1) batch_scan_kernel(const B
   }
   if (tid == 0) s_bad = 0;
   __syncthreads();
+  // queries grouping by the table at each probe position (their factor there is not 0)
+  unsigned long long tgrp[OLAP_MAX_DIMS] = {0ull, 0ull, 0ull, 0ull};
+  if (PAR) {
+    for (int q = 0; q < nq; ++q) {
+      const int4 f = s_qf[q];
+      tgrp[0] |= static_cast<unsigned long long>(f.x != 0) << q;
+      tgrp[1] |= static_cast<unsigned long long>(f.y != 0) << q;
+      tgrp[2] |= static_cast<unsigned long long>(f.z != 0) << q;
+      tgrp[3] |= static_cast<unsigned long long>(f.w != 0) << q;
+    }
+  }
   const uint64_t pol_stream = policy_evict_first();
   const uint64_t pol_keep = policy_evict_last();
   const int agg = p.agg;
@@ -286,7 +316,6 @@ __global__ void __launch_bounds__(kBatchMaxThreads, 1) batch_scan_kernel(const B
     // the table is not probed for it, and the row counts once per such query
     // when every other table the query uses passes it (as the plain path
     // counts: no in-range key of the query meets its filter's null).
-    unsigned long long oobq[4] = {0ull, 0ull, 0ull, 0ull};
     uint32_t inr = 0;  // bit 4*o + k: key[o][k] in range
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -294,33 +323,75 @@ __global__ void __launch_bounds__(kBatchMaxThreads, 1) batch_scan_kernel(const B
       for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
         if (o >= ntab) continue;
         if (static_cast<uint32_t>(key[o][k]) < tlen[o]) inr |= 1u << (4 * o + k);
-        else oobq[k] |= tuses[o];
       }
-      oobq[k] &= m[k];
     }
-    // Probe the tables, smallest first, breadth-first across the 4 rows; a
-    // table is probed for a row only while a live query of the row uses it.
+    // queries that use a table whose key of row k is out of range
+    auto oob_queries = [&](int k) -> unsigned long long {
+      unsigned long long q = 0;
+#pragma unroll
+      for (int o = 0; o < OLAP_MAX_DIMS; ++o)
+        if (o < ntab && !((inr >> (4 * o + k)) & 1u)) q |= tuses[o];
+      return q;
+    };
     int32_t gr[OLAP_MAX_DIMS][4] = {};
+    if (PAR) {
+      // every used table's query mask of the 4 rows in one round trip
+      unsigned long long tm[OLAP_MAX_DIMS][4];
 #pragma unroll
-    for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
-      if (o >= ntab) continue;
-      const unsigned long long ut = tuses[o];
-      const DimRecord* rt = p.rec[tab[o]];
-      ulonglong2 rec[4];
+      for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
+        if (o >= ntab) continue;
+        const unsigned long long ut = tuses[o];
+        const DimRecord* rt = p.rec[tab[o]];
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        rec[k] = ((m[k] & ut) && ((inr >> (4 * o + k)) & 1u)) ? ld_record(rt + key[o][k], pol_keep)
-                                                                 : make_ulonglong2(~0ull, 0ull);
+        for (int k = 0; k < 4; ++k)
+          tm[o][k] = ((m[k] & ut) && ((inr >> (4 * o + k)) & 1u)) ? ld_record_mask(rt + key[o][k], pol_keep)
+                                                                   : ~0ull;
+      }
+#pragma unroll
+      for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
+        if (o >= ntab) continue;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) m[k] &= tm[o][k];
+      }
+      // group attributes where a surviving query groups by the table (and
+      // its key is in range)
+#pragma unroll
+      for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
+        if (o >= ntab) continue;
+        const unsigned long long ug = tgrp[o];
+        const DimRecord* rt = p.rec[tab[o]];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          gr[o][k] = ((m[k] & ug) != 0ull && ((inr >> (4 * o + k)) & 1u)) ? ld_record_grp(rt + key[o][k], pol_keep)
+                                                                           : 0;
+      }
+    } else {
+      // Probe the tables, smallest first, breadth-first across the 4 rows; a
+      // table is probed for a row only while a live query of the row uses it.
+#pragma unroll
+      for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
+        if (o >= ntab) continue;
+        const unsigned long long ut = tuses[o];
+        const DimRecord* rt = p.rec[tab[o]];
+        ulonglong2 rec[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          rec[k] = ((m[k] & ut) && ((inr >> (4 * o + k)) & 1u)) ? ld_record(rt + key[o][k], pol_keep)
+                                                                   : make_ulonglong2(~0ull, 0ull);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          m[k] &= rec[k].x;
+          gr[o][k] = static_cast<int32_t>(static_cast<uint32_t>(rec[k].y));
+        }
+      }
+    }
+    if (inr != (1u << (4 * ntab)) - 1u) {  // rare: some key out of range
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        m[k] &= rec[k].x;
-        gr[o][k] = static_cast<int32_t>(static_cast<uint32_t>(rec[k].y));
+        const unsigned long long oq = k < nv ? oob_queries(k) : 0ull;
+        bad += __popcll(m[k] & oq);
+        m[k] &= ~oq;
       }
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      bad += __popcll(m[k] & oobq[k]);
-      m[k] &= ~oobq[k];
     }
     // Per-query work only for the queries left in each row's mask.
 #pragma unroll
@@ -422,6 +493,7 @@ struct olap_batch {
   int64_t attr_len[OLAP_MAX_DIMS] = {};
   int block = olap::kBatchThreads;        // scan kernel block size (olap_batch_tune / _autotune)
   int smem_slots = olap::kBatchSmemSlots; // per-block shared accumulators
+  int parallel_probe = 0;                 // 1: every table's mask in one round trip (block <= 512)
 };
 
 extern "C" {
@@ -637,12 +709,13 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
   const bool need_m2 = agg == OLAP_AGG_M1_PLUS_M2 || agg == OLAP_AGG_M2 || agg == OLAP_AGG_M1_TIMES_M2;
   OLAP_REQUIRE(ctx, n_rows == 0 || ((!need_m1 || m1) && (!need_m2 || m2)), "measure columns required");
   const size_t scan_smem = sizeof(unsigned long long) * static_cast<size_t>(b->smem_slots);
+  const bool par = b->parallel_probe != 0 && b->block <= 512;
+  void (*scan)(const olap::BatchParams) = par ? olap::batch_scan_kernel<true> : olap::batch_scan_kernel<false>;
   if (scan_smem > 48 * 1024)
-    OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::batch_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             static_cast<int>(scan_smem)));
   int bps = 1;
-  OLAP_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, olap::batch_scan_kernel, b->block,
-                                                                   scan_smem));
+  OLAP_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, scan, b->block, scan_smem));
   const unsigned grid = static_cast<unsigned>(ctx->sm_count) * static_cast<unsigned>(bps < 1 ? 1 : bps);
   // The work of one batch: descriptors H2D, zero outputs, query masks of the
   // used tables, one persistent pass over the fact table.
@@ -659,7 +732,7 @@ int olap_batch_run(olap_batch* b, const olap_batch_query* queries, int n_queries
       e = cudaGetLastError();
     }
     if (e == cudaSuccess && n_rows > 0) {
-      olap::batch_scan_kernel<<<grid, b->block, scan_smem, st>>>(p);
+      scan<<<grid, b->block, scan_smem, st>>>(p);
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
@@ -718,6 +791,22 @@ int olap_batch_tune(olap_batch* b, int block, int smem_slots) {
   return OLAP_OK;
 }
 
+int olap_batch_set_probe(olap_batch* b, int parallel_probe) {
+  if (!b || (parallel_probe != 0 && parallel_probe != 1)) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(b->ctx->mu);
+  b->parallel_probe = parallel_probe;
+  return OLAP_OK;
+}
+
+int olap_batch_get_tuning(olap_batch* b, int* block, int* smem_slots, int* parallel_probe) {
+  if (!b) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(b->ctx->mu);
+  if (block) *block = b->block;
+  if (smem_slots) *smem_slots = b->smem_slots;
+  if (parallel_probe) *parallel_probe = (b->parallel_probe && b->block <= 512) ? 1 : 0;
+  return OLAP_OK;
+}
+
 int olap_batch_autotune(olap_batch* b, const olap_batch_query* queries, int n_queries,
                         const int32_t* const* fk, const int32_t* m1, const int32_t* m2, int64_t n_rows,
                         int agg, int64_t* out, int64_t out_slots, int64_t* totals, int64_t sample_rows,
@@ -743,13 +832,16 @@ int olap_batch_autotune(olap_batch* b, const olap_batch_query* queries, int n_qu
   cudaMemcpyAsync(&errs_before, &ctx->counters->range_errors, sizeof(errs_before), cudaMemcpyDeviceToHost,
                   ctx->stream);
   cudaStreamSynchronize(ctx->stream);
-  const int saved_block = b->block, saved_slots = b->smem_slots;
+  const int saved_block = b->block, saved_slots = b->smem_slots, saved_probe = b->parallel_probe;
   double best = 1e30;
-  int bb = saved_block, bs = saved_slots;
+  int bb = saved_block, bs = saved_slots, bp = saved_probe;
+  for (int probe : {0, 1})
   for (int block : {256, 512, 1024}) {
+    if (probe && block > 512) continue;
     for (int slots : {0, 2048, 4096, 8192, 16384}) {
       b->block = block;
       b->smem_slots = slots;
+      b->parallel_probe = probe;
       float ms = 0.f, best_c = 1e30f;
       bool ok = true;
       for (int rep = 0; rep < 3 && ok; ++rep) {
@@ -768,6 +860,7 @@ int olap_batch_autotune(olap_batch* b, const olap_batch_query* queries, int n_qu
         best = best_c;
         bb = block;
         bs = slots;
+        bp = probe;
       }
     }
   }
@@ -780,10 +873,12 @@ int olap_batch_autotune(olap_batch* b, const olap_batch_query* queries, int n_qu
   if (best >= 1e29) {
     b->block = saved_block;
     b->smem_slots = saved_slots;
+    b->parallel_probe = saved_probe;
     return olap::set_error(ctx, OLAP_ERR_CUDA, "no batch autotune candidate ran");
   }
   b->block = bb;
   b->smem_slots = bs;
+  b->parallel_probe = bp;
   if (best_block) *best_block = bb;
   if (best_slots) *best_slots = bs;
   if (best_ms) *best_ms = best;

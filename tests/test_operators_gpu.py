@@ -299,6 +299,8 @@ def _group_expect(keys, vals, vals2):
 
 @pytest.mark.parametrize("dist,G,n,two", [
     ("zipf", 300, 2_000_001, True),        # shared-table plan, skewed
+    ("uniform", 1, (1 << 24) + 5, True),   # one key: its per-block count crosses the flush threshold
+    ("uniform", 3, (1 << 24) + 7, False),
     ("uniform", 5000, 1_000_003, True),    # partitioned plan, few groups per partition
     ("zipf", 1 << 16, 3_000_001, False),   # partitioned plan, skewed
     ("wide", 1 << 18, 2_000_003, True),    # partitioned plan, keys over the whole int32 range
@@ -316,7 +318,8 @@ def test_group_hash_plans(ctx, dist, G, n, two):
     vals = rng.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32)  # extremes of the value split
     vals2 = rng.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32) if two else None
     ek, es, ec = _group_expect(keys, vals, vals2)
-    for combine, plan in ((2, 0), (1, 0), (2, 2)):  # combining off (default) / on; forced partitioned plan
+    # combining off (default) / on; forced partitioned plan; 16-byte shared tables
+    for combine, plan in ((2, 0), (1, 0), (2, 2), (2, 3)):
         ctx.set_tuning(_lib.TUNE_GROUP_COMBINE, combine)
         ctx.set_tuning(_lib.TUNE_GROUP_PLAN, plan)
         k, s, c = ops.group_hash(dev(keys), dev(vals), dev(vals2) if two else None, max_groups=G, ctx=ctx)

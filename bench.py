@@ -318,6 +318,7 @@ def batched_result(a) -> dict:
                                    "fact range 5-100%), one persistent launch per batch replayed as a CUDA graph",
                        "fact_rows_covered_per_batch": rows_scanned,
                        "launch_shape": {"block_threads": tuned_block, "shared_accumulator_slots": tuned_slots,
+                                        "parallel_probe": eng.tuning()[2],
                                         "chosen_by": "--batch-shape" if a.batch_shape
                                         else "olap_batch_autotune on a 64Mi-row sample"}},
             "data": "synthetic (seeded counter-based generator, generated in HBM)"}

@@ -130,9 +130,19 @@ class BatchEngine:
         check(lib.olap_batch_graph_captures(self._h, C.byref(n)), self.ctx.handle)
         return n.value
 
-    def tune(self, block: int, smem_slots: int) -> None:
-        """Launch shape of the scan (threads per block, shared accumulators)."""
+    def tune(self, block: int, smem_slots: int, parallel_probe: int | None = None) -> None:
+        """Launch shape of the scan (threads per block, shared accumulators,
+        optionally the probe order: 1 reads every table's mask in one round
+        trip)."""
         check(lib.olap_batch_tune(self._h, int(block), int(smem_slots)), self.ctx.handle)
+        if parallel_probe is not None:
+            check(lib.olap_batch_set_probe(self._h, int(parallel_probe)), self.ctx.handle)
+
+    def tuning(self) -> tuple[int, int, int]:
+        """(block, smem_slots, parallel_probe) in force."""
+        b, s, p = C.c_int(), C.c_int(), C.c_int()
+        check(lib.olap_batch_get_tuning(self._h, C.byref(b), C.byref(s), C.byref(p)), self.ctx.handle)
+        return b.value, s.value, p.value
 
     def autotune(self, queries: list[Query], fk, m1, m2, agg: int = AGG_M1_PLUS_M2, sample_rows: int = 0):
         """Times the candidate launch shapes on a sample of the fact table with

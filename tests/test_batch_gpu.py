@@ -98,21 +98,29 @@ def test_batch_plain_path_matches_oracle(ctx, setup):
     assert np.array_equal(gs.cpu().numpy(), ogs) and np.array_equal(tot.cpu().numpy(), otot)
 
 
-def test_batch_counts_out_of_range_keys_like_the_plain_path(ctx, setup):
+@pytest.mark.parametrize("probe", [0, 1])
+def test_batch_counts_out_of_range_keys_like_the_plain_path(ctx, setup, probe):
     dims, fk, m1, m2, n = setup
     bad = [f.clone() for f in fk]
     bad[1][::1000] = SIZES[1] + 3   # keys past the supplier table
     bad[3][5::777] = -1
     rng = np.random.default_rng(6)
     qs = batch.random_queries(rng, 16, n, GROUPS)
-    _check_batch(ctx, (dims, bad, m1, m2, n), qs, olapcore.AGG_M1_PLUS_M2, use_graph=True)
+    eng = batch.BatchEngine(ctx, dims, max_queries=64)
+    eng.tune(512, 4096, probe)
+    _check_batch(ctx, (dims, bad, m1, m2, n), qs, olapcore.AGG_M1_PLUS_M2, use_graph=True, eng=eng)
 
 
-@pytest.mark.parametrize("block,slots", [(256, 0), (1024, 16384), (128, 2048), (768, 24576)])
-def test_launch_shapes_do_not_change_results(ctx, setup, block, slots):
+@pytest.mark.parametrize("probe", [0, 1])
+@pytest.mark.parametrize("block,slots", [(256, 0), (1024, 16384), (128, 2048), (768, 24576), (512, 4096)])
+def test_launch_shapes_do_not_change_results(ctx, setup, block, slots, probe):
+    """Every launch shape and both probe orders (all tables' masks in one
+    round trip runs for blocks of at most 512 threads) give the results of
+    the queries run alone."""
     rng = np.random.default_rng(block + slots)
     eng = batch.BatchEngine(ctx, setup[0], max_queries=64)
-    eng.tune(block, slots)
+    eng.tune(block, slots, probe)
+    assert eng.tuning() == (block, slots, probe if block <= 512 else 0)
     for nq in (64, 5):
         qs = batch.random_queries(rng, nq, setup[4], GROUPS)
         _check_batch(ctx, setup, qs, olapcore.AGG_M1_PLUS_M2, use_graph=True, eng=eng)

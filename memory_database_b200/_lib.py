@@ -51,6 +51,7 @@ TUNE_SMEM_NIB_BYTES = 12
 TUNE_HOST_INPLACE = 13
 TUNE_MERGE_PROBES = 14
 TUNE_PROBE_ORDER = 15
+TUNE_JOIN_BUILD = 16
 
 
 class OlapError(RuntimeError):

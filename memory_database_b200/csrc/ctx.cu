@@ -139,7 +139,7 @@ int olap_ctx_synchronize(olap_ctx* ctx) {
 }
 
 int olap_ctx_set_tuning(olap_ctx* ctx, int knob, int64_t value) {
-  if (!ctx || knob < 0 || knob >= 16 || value < 0) return OLAP_ERR_INVALID;
+  if (!ctx || knob < 0 || knob >= OLAP_TUNE_KNOBS || value < 0) return OLAP_ERR_INVALID;
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->tune[knob] = value;
   return OLAP_OK;

@@ -946,9 +946,8 @@ __global__ void agg_f64_final_kernel(const double* __restrict__ partial, int nb,
   }
 }
 
-// The context's grow-only buffer, at least `bytes` long (the caller's stream
-// is synchronised before a smaller buffer is replaced).
-static char* big_scratch(olap_ctx* ctx, size_t bytes) {
+// The context's grow-only buffer (declared in olap_internal.cuh).
+char* big_scratch(olap_ctx* ctx, size_t bytes) {
   if (bytes <= ctx->big_bytes) return ctx->big;
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return nullptr;
   if (ctx->big) cudaFree(ctx->big);

@@ -143,6 +143,138 @@ __global__ void hash_finish_kernel(uint64_t* __restrict__ slots, int64_t cap, co
   }
 }
 
+// ---- partitioned build ------------------------------------------------------
+// A table larger than L2 takes one random DRAM sector per CAS.  For such
+// tables the build rows are first scattered by the region of the table their
+// home slot falls in (regions of kBuildRegionSlots slots, 32 MB, which L2
+// holds), then inserted one region at a time, so the CAS traffic of a region
+// stays in L2 and each sector of the table crosses DRAM about once each way.
+// Linear probing may run past a region's end; that only costs locality.  The
+// finishing pass (row -> payload) runs once over the whole table afterwards.
+constexpr int64_t kBuildRegionSlots = int64_t(1) << 22;
+constexpr int kBuildPartThreads = 512;
+
+struct BuildPlan {
+  int64_t n;
+  int64_t per;         // rows per block of the histogram and scatter passes
+  int32_t n_blocks;
+  int32_t n_regions;   // P, a power of two
+  int32_t region_shift;
+  uint64_t mask;       // capacity - 1
+};
+
+__device__ __forceinline__ uint32_t build_region(int32_t k, const BuildPlan& bp) {
+  return static_cast<uint32_t>((hash32(static_cast<uint32_t>(k)) & bp.mask) >> bp.region_shift);
+}
+
+__global__ void __launch_bounds__(kBuildPartThreads) build_hist_kernel(BuildPlan bp, const int32_t* __restrict__ keys,
+                                                                      unsigned int* __restrict__ hist,
+                                                                      unsigned long long* range_err) {
+  extern __shared__ unsigned int s_cnt[];
+  for (int p = threadIdx.x; p < bp.n_regions; p += blockDim.x) s_cnt[p] = 0;
+  __syncthreads();
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * bp.per;
+  const int64_t e = b + bp.per < bp.n ? b + bp.per : bp.n;
+  unsigned int bad = 0;
+  for (int64_t r = b + threadIdx.x; r < e; r += blockDim.x) {
+    const int32_t k = keys[r];
+    if (k == INT32_MIN) {
+      ++bad;
+      continue;
+    }
+    atomicAdd(&s_cnt[build_region(k, bp)], 1u);
+  }
+  if (bad) atomicAdd(range_err, static_cast<unsigned long long>(bad));
+  __syncthreads();
+  for (int p = threadIdx.x; p < bp.n_regions; p += blockDim.x)
+    hist[static_cast<int64_t>(blockIdx.x) * bp.n_regions + p] = s_cnt[p];
+}
+
+// Region-major offsets: offs[b * P + p] = start of block b's run in region p;
+// region_begin[p] (and [P] = all rows).  One block.
+__global__ void __launch_bounds__(1024) build_scan_kernel(BuildPlan bp, const unsigned int* __restrict__ hist,
+                                                          unsigned long long* __restrict__ offs,
+                                                          long long* __restrict__ region_begin) {
+  __shared__ long long s_tot[2048];
+  __shared__ long long s_run[1024];
+  const int P = bp.n_regions, B = bp.n_blocks;
+  for (int p = threadIdx.x; p < P; p += blockDim.x) {
+    long long t = 0;
+    for (int b = 0; b < B; ++b) t += hist[static_cast<int64_t>(b) * P + p];
+    s_tot[p] = t;
+  }
+  __syncthreads();
+  // exclusive scan of the region totals (each thread a run of regions)
+  const int per = (P + blockDim.x - 1) / blockDim.x;
+  const int lo = threadIdx.x * per, hi = lo + per < P ? lo + per : P;
+  long long mine = 0;
+  for (int p = lo; p < hi; ++p) mine += s_tot[p];
+  s_run[threadIdx.x] = mine;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const long long y = threadIdx.x >= o ? s_run[threadIdx.x - o] : 0;
+    __syncthreads();
+    s_run[threadIdx.x] += y;
+    __syncthreads();
+  }
+  long long run = s_run[threadIdx.x] - mine;
+  for (int p = lo; p < hi; ++p) {
+    region_begin[p] = run;
+    long long c = run;
+    for (int b = 0; b < B; ++b) {
+      offs[static_cast<int64_t>(b) * P + p] = static_cast<unsigned long long>(c);
+      c += hist[static_cast<int64_t>(b) * P + p];
+    }
+    run += s_tot[p];
+  }
+  if (threadIdx.x == blockDim.x - 1) region_begin[P] = s_run[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kBuildPartThreads) build_scatter_kernel(BuildPlan bp,
+                                                                         const int32_t* __restrict__ keys,
+                                                                         const unsigned long long* __restrict__ offs,
+                                                                         uint64_t* __restrict__ tuples) {
+  extern __shared__ unsigned long long s_cur[];
+  for (int p = threadIdx.x; p < bp.n_regions; p += blockDim.x)
+    s_cur[p] = offs[static_cast<int64_t>(blockIdx.x) * bp.n_regions + p];
+  __syncthreads();
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * bp.per;
+  const int64_t e = b + bp.per < bp.n ? b + bp.per : bp.n;
+  for (int64_t r = b + threadIdx.x; r < e; r += blockDim.x) {
+    const int32_t k = keys[r];
+    if (k == INT32_MIN) continue;
+    const unsigned long long pos = atomicAdd(&s_cur[build_region(k, bp)], 1ull);
+    tuples[pos] = (static_cast<uint64_t>(static_cast<uint32_t>(k)) << 32) | static_cast<uint32_t>(r);
+  }
+}
+
+// Inserts region p's rows (tuples [region_begin[p], region_begin[p+1])).
+__global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const long long* __restrict__ region_begin,
+                                    int p, uint64_t* __restrict__ slots, uint64_t mask,
+                                    unsigned long long* overflow) {
+  const int64_t b = region_begin[p], e = region_begin[p + 1];
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = b + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < e; i += stride) {
+    const uint64_t mine = tuples[i];
+    const uint32_t k = static_cast<uint32_t>(mine >> 32);
+    uint64_t h = hash32(k) & mask;
+    bool done = false;
+    for (uint64_t step = 0; step <= mask && !done; ++step) {
+      unsigned long long* s = reinterpret_cast<unsigned long long*>(slots + h);
+      const unsigned long long prev = atomicCAS(s, kEmptySlot, mine);
+      if (prev == kEmptySlot) {
+        done = true;
+      } else if ((prev >> 32) == k) {
+        atomicMax(s, mine);  // same key: keeps the largest row
+        done = true;
+      } else {
+        h = (h + 1) & mask;
+      }
+    }
+    if (!done) atomicAdd(overflow, 1ull);
+  }
+}
+
 // Probe: SUM of matched payloads and the match count; optionally the matches
 // (probe row, payload) compacted in probe-row order by the caller's second
 // pass (see ProbeOp).
@@ -411,7 +543,43 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
   if (!overflow) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
   OLAP_CUDA_TRY(ctx, cudaMemsetAsync(overflow, 0, sizeof(*overflow), ctx->stream));
   olap::fill_u64_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, olap::kEmptySlot);
-  if (n) {
+  // Tables larger than one region are built region by region, unless
+  // OLAP_TUNE_JOIN_BUILD = 2 asks for the direct build.
+  const bool partitioned = capacity > olap::kBuildRegionSlots && n >= (int64_t(1) << 16) &&
+                           ctx->tune[olap::TUNE_JOIN_BUILD] != 2;
+  if (n && partitioned) {
+    olap::BuildPlan bp;
+    bp.n = n;
+    bp.mask = static_cast<uint64_t>(capacity - 1);
+    bp.n_regions = static_cast<int32_t>(capacity / olap::kBuildRegionSlots);
+    int lg_cap = 0;
+    while ((int64_t(1) << lg_cap) < capacity) ++lg_cap;
+    int lg_p = 0;
+    while ((1 << lg_p) < bp.n_regions) ++lg_p;
+    bp.region_shift = lg_cap - lg_p;
+    bp.n_blocks = ctx->sm_count * 2;
+    bp.per = (n + bp.n_blocks - 1) / bp.n_blocks;
+    OLAP_REQUIRE(ctx, bp.n_regions <= 2048, "hash table capacity above 2^33 slots");
+    const size_t hist_bytes = sizeof(unsigned int) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
+    const size_t offs_bytes = sizeof(unsigned long long) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
+    const size_t begin_bytes = sizeof(long long) * (bp.n_regions + 1);
+    const size_t tup_off = (hist_bytes + offs_bytes + begin_bytes + 255) & ~size_t(255);
+    char* mem = olap::big_scratch(ctx, tup_off + sizeof(uint64_t) * static_cast<size_t>(n));
+    if (!mem) return olap::set_error(ctx, OLAP_ERR_NOMEM, "device memory for the build partitions");
+    auto* hist = reinterpret_cast<unsigned int*>(mem);
+    auto* offs = reinterpret_cast<unsigned long long*>(mem + ((hist_bytes + 7) & ~size_t(7)));
+    auto* rbegin = reinterpret_cast<long long*>(reinterpret_cast<char*>(offs) + offs_bytes);
+    auto* tuples = reinterpret_cast<uint64_t*>(mem + tup_off);
+    const size_t hsm = sizeof(unsigned int) * bp.n_regions, csm = sizeof(unsigned long long) * bp.n_regions;
+    olap::build_hist_kernel<<<bp.n_blocks, olap::kBuildPartThreads, hsm, ctx->stream>>>(
+        bp, keys, hist, &ctx->counters->range_errors);
+    olap::build_scan_kernel<<<1, 1024, 0, ctx->stream>>>(bp, hist, offs, rbegin);
+    olap::build_scatter_kernel<<<bp.n_blocks, olap::kBuildPartThreads, csm, ctx->stream>>>(bp, keys, offs, tuples);
+    const unsigned ig = static_cast<unsigned>(ctx->sm_count) * 8;
+    for (int p = 0; p < bp.n_regions; ++p)
+      olap::build_insert_kernel<<<ig, 256, 0, ctx->stream>>>(tuples, rbegin, p, table, bp.mask, overflow);
+    olap::hash_finish_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, payload);
+  } else if (n) {
     olap::hash_build_kernel<<<olap::grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(
         keys, n, table, static_cast<uint64_t>(capacity - 1), &ctx->counters->range_errors, overflow);
     olap::hash_finish_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, payload);

@@ -58,7 +58,7 @@ struct olap_ctx {
   int64_t host_bytes = 0;
 
   // Tuning knobs (0 = automatic); set by olap_ctx_set_tuning.
-  int64_t tune[16] = {0};
+  int64_t tune[OLAP_TUNE_KNOBS] = {0};
 
   std::mutex mu;               // serialises calls that share this context
   std::string last_error;
@@ -84,6 +84,7 @@ enum {
   TUNE_HOST_INPLACE = OLAP_TUNE_HOST_INPLACE,
   TUNE_MERGE_PROBES = OLAP_TUNE_MERGE_PROBES,
   TUNE_PROBE_ORDER = OLAP_TUNE_PROBE_ORDER,
+  TUNE_JOIN_BUILD = OLAP_TUNE_JOIN_BUILD,
 };
 
 int set_error(olap_ctx* ctx, int status, const std::string& msg);
@@ -128,6 +129,10 @@ int starjoin_device(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_
 // copies the query's host dimension vectors into `ar` (a dimvec_len of 0 is
 // resolved from the largest key) and points dq at the copies.
 int stage_host_dims(olap_ctx* ctx, const olap_starjoin_query* q, Arena& ar, olap_starjoin_query* dq);
+// The context's grow-only device buffer, at least `bytes` long (the context's
+// stream is synchronised before a smaller buffer is replaced); null when the
+// allocation fails.  Used by calls whose scratch grows with their rows.
+char* big_scratch(olap_ctx* ctx, size_t bytes);
 // In-place scan of pinned host columns (dq: the query with its dimension
 // vectors staged in `ar`); *handled is false (and nothing ran) when a column
 // is not device-mapped, the columns' 16-byte phases differ, or the

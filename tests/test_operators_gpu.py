@@ -348,3 +348,28 @@ def test_bounded_device_wait_reports_timeout_and_context_survives(ctx):
     assert st == _lib.OLAP_ERR_TIMEOUT
     col = np.arange(100_000, dtype=np.int32)
     assert np.array_equal(host(ops.select_rowids(dev(col), 99, ctx=ctx)), np.arange(100, dtype=np.int32))
+
+
+@pytest.mark.parametrize("mode", [0, 2])
+def test_hash_join_region_build(ctx, mode):
+    """A build side whose table is larger than one 32 MB region (2^22 rows:
+    2^23 slots, 64 MB) is built region by region by default (mode 0) or
+    directly (OLAP_TUNE_JOIN_BUILD = 2): duplicate keys keep their last row,
+    the reserved key is counted, and probes equal the oracle's either way."""
+    rng = np.random.default_rng(31)
+    n = 1 << 22
+    rk = rng.integers(-(1 << 23), 1 << 23, n).astype(np.int32)  # about 1/4 duplicates, negatives
+    rk[::100_003] = np.iinfo(np.int32).min
+    rp = np.arange(n, dtype=np.int32) ^ 0x5A5A5A5A
+    sk = rng.integers(-(1 << 23), 1 << 23, 1 << 23).astype(np.int32)
+    ctx.set_tuning(_lib.TUNE_JOIN_BUILD, mode)
+    try:
+        ht = ops.HashTable(n, ctx=ctx).build(dev(rk), dev(rp))
+    finally:
+        ctx.set_tuning(_lib.TUNE_JOIN_BUILD, 0)
+    assert ht.capacity == 1 << 23
+    assert ctx.take_range_errors() == int((rk == np.iinfo(np.int32).min).sum())
+    assert ht.probe(dev(sk)) == oracle.hashjoin(rk, rp, sk)
+    rows, pay = ht.probe_pairs(dev(sk[:300_000]))
+    _, _, erows, epay = oracle.hashjoin(rk, rp, sk[:300_000], want_pairs=True)
+    assert np.array_equal(host(rows), erows) and np.array_equal(host(pay), epay)

@@ -443,6 +443,9 @@ def operators_result(a) -> dict:
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx = olapcore.Context(0, stream=stream)
+    for kv in filter(None, a.tune.split(",")):
+        k, v = kv.split("=")
+        ctx.set_tuning(int(k), int(v))
     h = ctx.handle
     n = a.op_rows
     peak, peak_src = measured_peak_gbs()
@@ -684,7 +687,7 @@ def main() -> None:
     # Plan choice for this query shape: the library's autotuner times its
     # candidate plans on a 64Mi-row sample of this rank's table (untimed).
     if a.tune:
-        knobs = [0] * 16
+        knobs = [0] * 17
         for kv in filter(None, a.tune.split(",")):
             k, v = kv.split("=")
             knobs[int(k)] = int(v)
@@ -694,7 +697,7 @@ def main() -> None:
     plan = {name: knobs[k] for k, name in enumerate(
         ["block_threads", "blocks_per_sm", "smem_dim_bytes", "smem_acc_bytes", "host_chunk_rows",
          "rows_per_thread_mode", "probe_bits", "smem_bits_bytes", "group_combine", "group_plan", "async_loads", "compact",
-         "smem_nib_bytes", "host_inplace", "merge_probes", "probe_order"]) if knobs[k]}
+         "smem_nib_bytes", "host_inplace", "merge_probes", "probe_order", "join_build"]) if knobs[k]}
 
     # kernels per query with this plan (the star-join and its staging prepasses)
     per_query = olapcore.launch_count(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,

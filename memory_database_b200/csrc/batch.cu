@@ -169,12 +169,14 @@ __global__ void __launch_bounds__(256) batch_records_kernel(const BatchParams p,
   }
 }
 
+// Record loads.  They are asm without `volatile`, which the compiler may
+// execute where their guard does not hold, so the callers pass the record of
+// key 0 (every table has at least one) in place of a key out of range.
 __device__ __forceinline__ ulonglong2 ld_record(const DimRecord* r, uint64_t pol) {
   ulonglong2 v;
   asm("ld.global.nc.L2::cache_hint.v2.u64 {%0,%1}, [%2], %3;" : "=l"(v.x), "=l"(v.y) : "l"(r), "l"(pol));
   return v;
 }
-
 __device__ __forceinline__ unsigned long long ld_record_mask(const DimRecord* r, uint64_t pol) {
   unsigned long long v;
   asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(r), "l"(pol));
@@ -343,9 +345,10 @@ __global__ void __launch_bounds__(PAR ? 512 : kBatchMaxThreads, 1) batch_scan_ke
         const unsigned long long ut = tuses[o];
         const DimRecord* rt = p.rec[tab[o]];
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-          tm[o][k] = ((m[k] & ut) && ((inr >> (4 * o + k)) & 1u)) ? ld_record_mask(rt + key[o][k], pol_keep)
-                                                                   : ~0ull;
+        for (int k = 0; k < 4; ++k) {
+          const bool in = (inr >> (4 * o + k)) & 1u;
+          tm[o][k] = ((m[k] & ut) && in) ? ld_record_mask(rt + (in ? key[o][k] : 0), pol_keep) : ~0ull;
+        }
       }
 #pragma unroll
       for (int o = 0; o < OLAP_MAX_DIMS; ++o) {
@@ -361,9 +364,10 @@ __global__ void __launch_bounds__(PAR ? 512 : kBatchMaxThreads, 1) batch_scan_ke
         const unsigned long long ug = tgrp[o];
         const DimRecord* rt = p.rec[tab[o]];
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-          gr[o][k] = ((m[k] & ug) != 0ull && ((inr >> (4 * o + k)) & 1u)) ? ld_record_grp(rt + key[o][k], pol_keep)
-                                                                           : 0;
+        for (int k = 0; k < 4; ++k) {
+          const bool in = (inr >> (4 * o + k)) & 1u;
+          gr[o][k] = ((m[k] & ug) != 0ull && in) ? ld_record_grp(rt + (in ? key[o][k] : 0), pol_keep) : 0;
+        }
       }
     } else {
       // Probe the tables, smallest first, breadth-first across the 4 rows; a
@@ -375,9 +379,11 @@ __global__ void __launch_bounds__(PAR ? 512 : kBatchMaxThreads, 1) batch_scan_ke
         const DimRecord* rt = p.rec[tab[o]];
         ulonglong2 rec[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-          rec[k] = ((m[k] & ut) && ((inr >> (4 * o + k)) & 1u)) ? ld_record(rt + key[o][k], pol_keep)
-                                                                   : make_ulonglong2(~0ull, 0ull);
+        for (int k = 0; k < 4; ++k) {
+          const bool in = (inr >> (4 * o + k)) & 1u;
+          rec[k] = ((m[k] & ut) && in) ? ld_record(rt + (in ? key[o][k] : 0), pol_keep)
+                                       : make_ulonglong2(~0ull, 0ull);
+        }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           m[k] &= rec[k].x;

@@ -242,6 +242,7 @@ template <class F>
 __device__ __forceinline__ void agg_rows(int64_t b, int64_t e, int64_t t0, int64_t stride, const int32_t* keys,
                                          const int32_t* vals, const int32_t* vals2, bool vec, F&& f) {
   const uint64_t pol = policy_evict_first();
+  const int32_t* v2 = vals2 ? vals2 : vals;  // a valid address even where the guarded load is hoisted
   const int64_t b4 = vec ? (b + 3) & ~int64_t(3) : e;  // first aligned row
   const int64_t head = b4 < e ? b4 : e;
   // head rows one by one (at most 3), then groups of 4, then the tail
@@ -265,7 +266,7 @@ __device__ __forceinline__ void agg_rows(int64_t b, int64_t e, int64_t t0, int64
       if (ok[g]) {
         k[g] = ld_stream_v4(keys + head + 4 * i, pol);
         v[g] = ld_stream_v4(vals + head + 4 * i, pol);
-        if (vals2) w[g] = ld_stream_v4(vals2 + head + 4 * i, pol);
+        if (vals2) w[g] = ld_stream_v4(v2 + head + 4 * i, pol);
       }
     }
 #pragma unroll
@@ -453,6 +454,7 @@ __global__ void __launch_bounds__(kPackThreads, 2) group_hash_pack_kernel(int64_
   const int64_t b = static_cast<int64_t>(blockIdx.x) * per;
   const int64_t e = b + per < n ? b + per : n;
   const uint64_t pol = policy_evict_first();
+  const int32_t* v2 = vals2 ? vals2 : vals;  // a valid address even where the guarded load is hoisted
   unsigned int bad = 0;
   auto spill = [&](int32_t k, int64_t v) { global_add(g, k, static_cast<uint64_t>(v), 1); };
   auto one = [&](int64_t r) {
@@ -477,7 +479,7 @@ __global__ void __launch_bounds__(kPackThreads, 2) group_hash_pack_kernel(int64_
     for (int64_t i = threadIdx.x; i < n4; i += blockDim.x) {
       const int4 kk = ld_stream_v4(keys + head + 4 * i, pol);
       const int4 a = ld_stream_v4(vals + head + 4 * i, pol);
-      const int4 c = vals2 ? ld_stream_v4(vals2 + head + 4 * i, pol) : make_int4(0, 0, 0, 0);
+      const int4 c = vals2 ? ld_stream_v4(v2 + head + 4 * i, pol) : make_int4(0, 0, 0, 0);
       const int32_t kr[4] = {kk.x, kk.y, kk.z, kk.w}, ar[4] = {a.x, a.y, a.z, a.w}, cr[4] = {c.x, c.y, c.z, c.w};
       int32_t k[4];
       int64_t v[4];

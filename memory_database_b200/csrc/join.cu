@@ -67,8 +67,12 @@ __device__ __forceinline__ uint64_t ld_keep_u64(const uint64_t* p, uint64_t pol)
 }
 
 // Keys of k4 that may be in the table: all four unless there is a filter.
+// The kernels are instantiated with and without a filter, so the unfiltered
+// ones form no filter address at all (the word loads below are asm without
+// `volatile`; a null filter behind a runtime test could still be read).
+template <bool kFilter>
 __device__ __forceinline__ uint32_t bloom_pass4(const Bloom& f, const int4 k4, uint64_t pol) {
-  if (!f.words) return 0xFu;
+  if (!kFilter) return 0xFu;
   const uint32_t k[4] = {static_cast<uint32_t>(k4.x), static_cast<uint32_t>(k4.y), static_cast<uint32_t>(k4.z),
                          static_cast<uint32_t>(k4.w)};
   uint64_t w[4];
@@ -83,8 +87,9 @@ __device__ __forceinline__ uint32_t bloom_pass4(const Bloom& f, const int4 k4, u
   return m;
 }
 
+template <bool kFilter>
 __device__ __forceinline__ bool bloom_pass(const Bloom& f, int32_t k) {
-  if (!f.words) return true;
+  if (!kFilter) return true;
   const uint64_t b = bloom_bits(static_cast<uint32_t>(k));
   return (__ldg(f.words + bloom_word(static_cast<uint32_t>(k), f.shift)) & b) == b;
 }
@@ -356,6 +361,7 @@ __device__ __forceinline__ uint32_t hash_lookup4(const uint64_t* __restrict__ sl
   return found;
 }
 
+template <bool kFilter>
 __global__ void __launch_bounds__(512) hash_probe_sum_kernel(const int32_t* __restrict__ keys, int64_t n,
                                                              const uint64_t* __restrict__ slots, uint64_t mask,
                                                              Bloom filter, int vec, unsigned long long* sum,
@@ -370,13 +376,13 @@ __global__ void __launch_bounds__(512) hash_probe_sum_kernel(const int32_t* __re
   for (int64_t i = tid; i < n4; i += stride) {
     const int4 k = ld_stream_v4(keys + 4 * i, pol);
     int32_t p[4];
-    const uint32_t f = hash_lookup4(slots, mask, k, p, bloom_pass4(filter, k, keep));
+    const uint32_t f = hash_lookup4(slots, mask, k, p, bloom_pass4<kFilter>(filter, k, keep));
     s += static_cast<int64_t>(p[0]) + p[1] + static_cast<int64_t>(p[2]) + p[3];  // 0 where absent
     c += __popc(f);
   }
   for (int64_t r = 4 * n4 + tid; r < n; r += stride) {
     int32_t p = 0;
-    if (bloom_pass(filter, keys[r]) && hash_lookup(slots, mask, keys[r], &p)) {
+    if (bloom_pass<kFilter>(filter, keys[r]) && hash_lookup(slots, mask, keys[r], &p)) {
       s += p;
       ++c;
     }
@@ -402,6 +408,7 @@ __global__ void __launch_bounds__(512) hash_probe_sum_kernel(const int32_t* __re
 }
 
 // Matches (probe row, payload) in probe-row order.
+template <bool kFilter>
 struct ProbeOp {
   static constexpr int kGroups = kCompactGroups;
   const int32_t* keys;
@@ -432,11 +439,11 @@ struct ProbeOp {
     uint32_t m = 0;
     if (nv == 4) {
       const int4 k4 = make_int4(k[0], k[1], k[2], k[3]);
-      m = hash_lookup4(slots, mask, k4, p, bloom_pass4(filter, k4, policy_evict_last()));
+      m = hash_lookup4(slots, mask, k4, p, bloom_pass4<kFilter>(filter, k4, policy_evict_last()));
     } else {
 #pragma unroll
       for (int j = 0; j < 4; ++j)
-        if (j < nv && bloom_pass(filter, k[j]) && hash_lookup(slots, mask, k[j], &p[j])) m |= 1u << j;
+        if (j < nv && bloom_pass<kFilter>(filter, k[j]) && hash_lookup(slots, mask, k[j], &p[j])) m |= 1u << j;
     }
     pay[u] = make_int4(p[0], p[1], p[2], p[3]);
     return m;
@@ -510,6 +517,28 @@ __global__ void __launch_bounds__(512) vec_probe_kernel(const int32_t* __restric
 }
 
 static bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Matched pairs of n probe keys through the order-preserving compaction.
+template <bool kFilter>
+int probe_pairs(olap_ctx* ctx, Arena& ar, const uint64_t* table, uint64_t mask, const Bloom& bloom,
+                const int32_t* keys, int64_t n, unsigned long long* total, int32_t* out_rows,
+                int32_t* out_payload) {
+  ProbeOp<kFilter> op;
+  std::memset(&op, 0, sizeof(op));
+  op.keys = keys;
+  op.slots = table;
+  op.mask = mask;
+  op.filter = bloom;
+  op.out_rows = out_rows;
+  op.out_payload = out_payload;
+  op.vec = al16(keys);
+  ScanTiles st;
+  const int rc = make_scan_tiles(ctx, ar, n, total, ctx->stream, &st, compact_tile_items<ProbeOp<kFilter>>());
+  if (rc != OLAP_OK) return rc;
+  compact_kernel<ProbeOp<kFilter>><<<compact_grid(ctx, st.n_tiles), kCompactThreads, 0, ctx->stream>>>(op, n, st);
+  OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  return OLAP_OK;
+}
 
 static unsigned grid_for(const olap_ctx* ctx, int64_t items, int threads) {
   int64_t g = (items + threads - 1) / threads;
@@ -649,30 +678,26 @@ int olap_hashjoin_probe_filtered(olap_ctx* ctx, const uint64_t* table, int64_t c
     if (!m) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
     OLAP_CUDA_TRY(ctx, cudaMemsetAsync(d_sum, 0, sizeof(int64_t), ctx->stream));
     OLAP_CUDA_TRY(ctx, cudaMemsetAsync(m, 0, sizeof(int64_t), ctx->stream));
-    if (n)
-      olap::hash_probe_sum_kernel<<<olap::grid_for(ctx, (n + 3) / 4, 512), 512, 0, ctx->stream>>>(
-          keys, n, table, mask, bloom, olap::al16(keys), reinterpret_cast<unsigned long long*>(d_sum), m);
+    if (n) {
+      const dim3 grid(olap::grid_for(ctx, (n + 3) / 4, 512));
+      auto* ds = reinterpret_cast<unsigned long long*>(d_sum);
+      if (filter)
+        olap::hash_probe_sum_kernel<true><<<grid, 512, 0, ctx->stream>>>(keys, n, table, mask, bloom,
+                                                                        olap::al16(keys), ds, m);
+      else
+        olap::hash_probe_sum_kernel<false><<<grid, 512, 0, ctx->stream>>>(keys, n, table, mask, bloom,
+                                                                         olap::al16(keys), ds, m);
+    }
     OLAP_CUDA_TRY(ctx, cudaGetLastError());
   }
   if (out_rows && out_payload) {
-    olap::ProbeOp op;
-    std::memset(&op, 0, sizeof(op));
-    op.keys = keys;
-    op.slots = table;
-    op.mask = mask;
-    op.filter = bloom;
-    op.out_rows = out_rows;
-    op.out_payload = out_payload;
-    op.vec = olap::al16(keys);
-    olap::ScanTiles st;
     unsigned long long* total = (!d_sum && d_matches) ? reinterpret_cast<unsigned long long*>(d_matches)
                                                       : ar.take<unsigned long long>(1);
     if (!total) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
-    int rc = olap::make_scan_tiles(ctx, ar, n, total, ctx->stream, &st, olap::compact_tile_items<olap::ProbeOp>());
+    const int rc = filter ? olap::probe_pairs<true>(ctx, ar, table, mask, bloom, keys, n, total, out_rows, out_payload)
+                          : olap::probe_pairs<false>(ctx, ar, table, mask, bloom, keys, n, total, out_rows,
+                                                     out_payload);
     if (rc != OLAP_OK) return rc;
-    olap::compact_kernel<olap::ProbeOp><<<olap::compact_grid(ctx, st.n_tiles), olap::kCompactThreads, 0,
-                                         ctx->stream>>>(op, n, st);
-    OLAP_CUDA_TRY(ctx, cudaGetLastError());
   }
   return OLAP_OK;
 }

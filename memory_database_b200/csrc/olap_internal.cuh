@@ -204,6 +204,41 @@ __device__ __forceinline__ int32_t ld_probe_s32(const int32_t* p, uint64_t pol) 
   return v;
 }
 
+// The loads above are asm statements without `volatile`: the compiler treats
+// them as free of side effects and may execute one where its C++ guard does
+// not hold (hoisted out of a branch or a conditional expression).  So every
+// address given to them must be valid whether or not the guard holds.  Where
+// a guard protects an address that may be invalid (a null column, a key out
+// of range, a row past the end), the `_if` forms below apply the guard as a
+// predicate inside the asm statement: however the statement is moved, the
+// load touches memory only when `pred` holds, and returns `dflt` (zeros for
+// the vector form) otherwise.
+__device__ __forceinline__ int4 ld_stream_v4_if(bool pred, const int32_t* p, uint64_t pol) {
+  int4 v;
+  asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %4, 0;\n\t"
+      "@q ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%5], %6;\n\t"
+      "@!q mov.b32 %0, 0;\n\t@!q mov.b32 %1, 0;\n\t@!q mov.b32 %2, 0;\n\t@!q mov.b32 %3, 0;\n\t}"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "r"(static_cast<uint32_t>(pred)), "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_stream_s32_if(bool pred, const int32_t* p, uint64_t pol, int32_t dflt) {
+  int32_t v;
+  asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %1, 0;\n\t"
+      "@q ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%2], %3;\n\t@!q mov.b32 %0, %4;\n\t}"
+      : "=r"(v)
+      : "r"(static_cast<uint32_t>(pred)), "l"(p), "l"(pol), "r"(dflt));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_probe_s8_if(bool pred, const int8_t* p, uint64_t pol, int32_t dflt) {
+  int32_t v;
+  asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %1, 0;\n\t"
+      "@q ld.global.nc.L2::cache_hint.s8 %0, [%2], %3;\n\t@!q mov.b32 %0, %4;\n\t}"
+      : "=r"(v)
+      : "r"(static_cast<uint32_t>(pred)), "l"(p), "l"(pol), "r"(dflt));
+  return v;
+}
+
 // Exact 64-bit accumulation into shared memory with 32-bit atomics: the low
 // word is added atomically and its carry-out is forwarded to the high word.
 // Addition mod 2^64 is commutative, so the final pair is exact whatever the

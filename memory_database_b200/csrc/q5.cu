@@ -163,13 +163,14 @@ __global__ void __launch_bounds__(512, 3) q5_lines_kernel(const int32_t* __restr
   const uint64_t keep = policy_evict_last();
   unsigned int bad = 0;
   auto one = [&](int32_t sk, int32_t ok, int32_t p, int32_t dc) {
-    if (sk < 1 || sk > n_supp || ok < 0 || ok >= n_orders) {
+    const bool in = sk >= 1 && sk <= n_supp && ok >= 0 && ok < n_orders;
+    if (!in) {
       ++bad;
       return;
     }
     const int32_t ns = snation(sk - 1);
     if (ns < 0) return;
-    const int32_t no = static_cast<int8_t>(ld_probe_s8(dim_o + ok, keep));
+    const int32_t no = static_cast<int8_t>(ld_probe_s8_if(in, dim_o + ok, keep, -2));
     if (no != ns) return;
     smem_add_u64(&s_sum[ns], static_cast<uint64_t>(static_cast<int64_t>(p) * (100 - dc)));
   };
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(512, 3) q5_lines_kernel(const int32_t* __restr
       else ns[e] = snation(sk[e] - 1);
     }
 #pragma unroll
-    for (int e = 0; e < 4; ++e) no[e] = ns[e] >= 0 ? static_cast<int8_t>(ld_probe_s8(dim_o + ok[e], keep)) : -2;
+    for (int e = 0; e < 4; ++e) no[e] = static_cast<int8_t>(ld_probe_s8_if(ns[e] >= 0, dim_o + ok[e], keep, -2));
 #pragma unroll
     for (int e = 0; e < 4; ++e)
       if (ns[e] >= 0 && no[e] == ns[e])
@@ -326,13 +327,14 @@ __global__ void __launch_bounds__(1024, 1) q5b_lines_kernel(
   const uint64_t keep = policy_evict_last();
   unsigned int bad = 0;
   auto one = [&](int32_t sk, int32_t ok, int32_t p, int32_t dc) {
-    if (sk < 1 || sk > n_supp || ok < 0 || ok >= n_orders) {
+    const bool in = sk >= 1 && sk <= n_supp && ok >= 0 && ok < n_orders;
+    if (!in) {
       ++bad;
       return;
     }
     const int32_t ns = stage_s ? s_dim[sk - 1] : dim_s[sk - 1];
     if (ns < 0) return;
-    const int32_t no = static_cast<int8_t>(ld_probe_s8(dim_o + ok, keep));
+    const int32_t no = static_cast<int8_t>(ld_probe_s8_if(in, dim_o + ok, keep, -2));
     if (no != ns) return;
     uint64_t m = s_nat[ns] & q5_date_mask(D, s_date, __ldg(o_orderdate + ok));
     const uint64_t v = static_cast<uint64_t>(static_cast<int64_t>(p) * (100 - dc));
@@ -362,7 +364,7 @@ __global__ void __launch_bounds__(1024, 1) q5b_lines_kernel(
       else ns[e] = stage_s ? s_dim[sk[e] - 1] : dim_s[sk[e] - 1];
     }
 #pragma unroll
-    for (int e = 0; e < 4; ++e) no[e] = ns[e] >= 0 ? static_cast<int8_t>(ld_probe_s8(dim_o + ok[e], keep)) : -2;
+    for (int e = 0; e < 4; ++e) no[e] = static_cast<int8_t>(ld_probe_s8_if(ns[e] >= 0, dim_o + ok[e], keep, -2));
 #pragma unroll
     for (int e = 0; e < 4; ++e) dt[e] = (ns[e] >= 0 && no[e] == ns[e]) ? __ldg(o_orderdate + ok[e]) : 0;
 #pragma unroll

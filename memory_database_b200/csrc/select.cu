@@ -186,7 +186,7 @@ __global__ void select_bitmap_kernel(const int32_t* __restrict__ col, int64_t n,
   const uint64_t pol = policy_evict_first();
   for (int64_t w = warp; w < nwords; w += nwarps) {
     const int64_t r = (w << 5) + lane;
-    const bool pass = r < n && cmp_pass(ld_stream_s32(col + r, pol), val, cmp);
+    const bool pass = r < n && cmp_pass(ld_stream_s32_if(r < n, col + r, pol, 0), val, cmp);
     const uint32_t word = __ballot_sync(0xffffffffu, pass);
     if (lane == 0) bits[w] = word;
   }

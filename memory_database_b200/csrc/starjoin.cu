@@ -361,8 +361,8 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
           alive |= 0xFu << (4 * u);
 #pragma unroll
           for (int j = 0; j < ND; ++j) kf[u][j] = ld_stream_v4(fkb[j] + 4ull * gi, pol_stream);
-          ka[u] = need_m1 ? ld_stream_v4(m1b + 4ull * gi, pol_stream) : make_int4(0, 0, 0, 0);
-          kb[u] = need_m2 ? ld_stream_v4(m2b + 4ull * gi, pol_stream) : make_int4(0, 0, 0, 0);
+          ka[u] = ld_stream_v4_if(need_m1, m1b + 4ull * gi, pol_stream);
+          kb[u] = ld_stream_v4_if(need_m2, m2b + 4ull * gi, pol_stream);
         } else {
 #pragma unroll
           for (int j = 0; j < ND; ++j) kf[u][j] = make_int4(0, 0, 0, 0);
@@ -406,6 +406,21 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
         bad += filtered ? 0u : 1u;
       }
       alive &= ~oob;
+      // keys of dropped rows to 0: every key left in registers addresses
+      // its vector, so no probe below can leave it, predicated or not
+#pragma unroll
+      for (int u = 0; u < NG; ++u) {
+        const uint32_t ob = (oob >> (4 * u)) & 0xFu;
+        if (!ob) continue;
+#pragma unroll
+        for (int j = 0; j < ND; ++j) {
+          int4& v = kf[u][j];
+          if (ob & 1u) v.x = 0;
+          if (ob & 2u) v.y = 0;
+          if (ob & 4u) v.z = 0;
+          if (ob & 8u) v.w = 0;
+        }
+      }
     }
     int32_t g[V];
 #pragma unroll
@@ -671,8 +686,8 @@ __global__ void __launch_bounds__(1024, 1) starjoin_scalar_kernel(const StarPara
       k[j] = static_cast<uint32_t>(ld_stream_s32(p.dim[j].fk + r, pol_stream));
       ok &= k[j] < p.dim[j].len;
     }
-    const int32_t x = p.need_m1 ? ld_stream_s32(p.m1 + r, pol_stream) : 0;
-    const int32_t y = p.need_m2 ? ld_stream_s32(p.m2 + r, pol_stream) : 0;
+    const int32_t x = ld_stream_s32_if(p.need_m1, p.m1 + r, pol_stream, 0);
+    const int32_t y = ld_stream_s32_if(p.need_m2, p.m2 + r, pol_stream, 0);
     if (!ok) {  // a range error unless an in-range key meets DIM_NULL
       bool filtered = false;
 #pragma unroll
@@ -697,7 +712,7 @@ __global__ void __launch_bounds__(1024, 1) starjoin_scalar_kernel(const StarPara
         } else if (d.bits) {
           if (!((__ldg(d.bits + (k[j] >> 5)) >> (k[j] & 31)) & 1u)) { live = false; break; }
         }
-        c = ld_probe_s8(d.vec + k[j], pol_keep);
+        c = ld_probe_s8_if(ok, d.vec + k[j], pol_keep, OLAP_DIM_NULL);  // ok: all keys in range here
       }
       if (c == OLAP_DIM_NULL) live = false;
       else g += static_cast<int64_t>(c) * d.factor;

@@ -694,6 +694,7 @@ def main() -> None:
     else:
         knobs, _ = olapcore.autotune(s.probe_dims, s.probe_fks, s.factor, s.m1, s.m2, G, aggs=aggs,
                                      dimvec_lens=s.probe_lens, ctx=ctx)
+        knobs = list(knobs) + [0] * (17 - len(knobs))  # the star-join knobs; join_build is not one
     plan = {name: knobs[k] for k, name in enumerate(
         ["block_threads", "blocks_per_sm", "smem_dim_bytes", "smem_acc_bytes", "host_chunk_rows",
          "rows_per_thread_mode", "probe_bits", "smem_bits_bytes", "group_combine", "group_plan", "async_loads", "compact",
@@ -819,6 +820,7 @@ def secondary_results(a, ctx) -> dict:
     import copy
     import torch
     out = {}
+    main_stream = torch.cuda.current_stream()  # the sub-runs make their own streams current
     b = copy.copy(a)
     b.steps = min(a.steps, 10)
     b.warmup = min(a.warmup, 3)
@@ -831,6 +833,7 @@ def secondary_results(a, ctx) -> dict:
         out["batched"]["launch_shape"] = r["config"]["launch_shape"]
     except Exception as e:
         out["batched"] = {"error": str(e)[:300]}
+    torch.cuda.set_stream(main_stream)
     torch.cuda.empty_cache()
     try:
         b.rates = [2000.0]
@@ -845,6 +848,7 @@ def secondary_results(a, ctx) -> dict:
                           "checked": r.get("checked"), "mix": "70% star-joins, 30% Q5 chains"}
     except Exception as e:
         out["serving"] = {"error": str(e)[:300]}
+    torch.cuda.set_stream(main_stream)
     torch.cuda.empty_cache()
     try:
         r = operators_result(b)
@@ -855,6 +859,7 @@ def secondary_results(a, ctx) -> dict:
                                     for o in r["operators"]]}
     except Exception as e:
         out["operators"] = {"error": str(e)[:300]}
+    torch.cuda.set_stream(main_stream)
     torch.cuda.empty_cache()
     out["sweep"] = []
     for name, sele, groups, dist in (("zipf0.8", a.sele, a.groups, "zipf"),
@@ -890,12 +895,15 @@ def sweep_point(a, ctx, name, sele, groups, fk_dist) -> dict:
         step()
     torch.cuda.synchronize()
     steps = 10
+    # the events go on the stream the context launches on
+    ctx_stream = torch.cuda.ExternalStream(ctx.stream_handle()) if ctx.stream_handle() else \
+        torch.cuda.default_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(0) as clk:
-        e0.record()
+        e0.record(ctx_stream)
         for _ in range(steps):
             step()
-        e1.record()
+        e1.record(ctx_stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     peak, _ = measured_peak_gbs()

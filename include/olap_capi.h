@@ -71,8 +71,9 @@ extern "C" {
 #define OLAP_TUNE_PROBE_BITS 6      /* global pass bitmaps for unstaged dims: 1 on, 2 off (default) */
 #define OLAP_TUNE_SMEM_BITS_BYTES 7 /* bytes of pass bitmaps staged in smem (default 0)          */
 #define OLAP_TUNE_GROUP_COMBINE 8   /* hash group-by warp combining of equal keys: 1 on, 2 off (default) */
-#define OLAP_TUNE_GROUP_PLAN 9      /* hash group-by: 1 per-block tables (capacity <= 8192), 2 partitioned,
-                                       3 per-block tables with two 32-bit counters per slot */
+#define OLAP_TUNE_GROUP_PLAN 9      /* hash group-by: 1 per-block tables (capacity <= 8192), rows'
+                                       updates batched, 2 partitioned, 3 per-block tables, one row's
+                                       update after another */
 #define OLAP_TUNE_ASYNC_LOADS 10    /* star-join: 2 prefetches fact columns by bulk async copies (TMA), 1 off */
 #define OLAP_TUNE_COMPACT 11        /* star-join: 2 compacts survivors per warp before global probes, 1 off */
 #define OLAP_TUNE_SMEM_NIB_BYTES 12 /* bytes of 4-bit code vectors staged in smem (default 0)        */

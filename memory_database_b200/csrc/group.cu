@@ -322,70 +322,11 @@ __global__ void __launch_bounds__(kAggThreads) group_hash_smem_kernel(int64_t n,
     if (st.key[i] != kEmptyKey) global_add(t, st.key[i], st.sum[i], st.cnt[i]);
 }
 
-// ---- packed shared tables ---------------------------------------------------
-// One 64-bit word per slot holds the slot's row count (bits 49-63) and the
-// sum of its values biased by 2^32 each (bits 0-48), so a row costs one
-// 64-bit shared atomic instead of two 32-bit ones and a carry.  A value (one
-// int32, or the sum of two) lies in [-2^32, 2^32), so a biased value is
-// below 2^33 and a count below 2^15 keeps the biased sum below 2^48.  The
-// thread whose add takes a slot's count to kPackFlush exchanges the word for
-// 0 and adds it to the global table; adds racing with it land before the
-// exchange (in the flushed word) or after it (in the fresh one), and at most
-// the block's threads can add between the two, so the count never reaches
-// 2^15.
-constexpr int kPackCountShift = 49;
-constexpr uint64_t kPackSumMask = (uint64_t(1) << kPackCountShift) - 1;
-constexpr uint64_t kPackFlush = uint64_t(1) << 14;
-constexpr int64_t kPackBias = int64_t(1) << 32;
-
-__device__ __forceinline__ uint64_t pack_row(int64_t v) {
-  return (uint64_t(1) << kPackCountShift) + static_cast<uint64_t>(v + kPackBias);
-}
-__device__ __forceinline__ void unpack(uint64_t w, uint64_t* sum, uint64_t* cnt) {
-  const uint64_t c = w >> kPackCountShift;
-  *cnt = c;
-  *sum = (w & kPackSumMask) - c * static_cast<uint64_t>(kPackBias);  // mod 2^64: the signed sum
-}
-
-struct PackAgg {
-  int32_t* key;
-  unsigned long long* acc;
-  uint32_t slots;  // a power of two >= 4
-  uint32_t nb;     // buckets of 4 slots
-};
-
-__device__ __forceinline__ PackAgg pack_agg(unsigned char* base, uint32_t slots) {
-  PackAgg t;
-  t.acc = reinterpret_cast<unsigned long long*>(base);
-  t.key = reinterpret_cast<int32_t*>(t.acc + slots);
-  t.slots = slots;
-  t.nb = slots >> 2;
-  return t;
-}
-
-__device__ __forceinline__ void pack_agg_clear(const PackAgg& t) {
-  for (uint32_t i = threadIdx.x; i < t.slots; i += blockDim.x) {
-    t.key[i] = kEmptyKey;
-    t.acc[i] = 0;
-  }
-}
-
-// One row into slot i: a 64-bit add, and the flush when the count fills.
-__device__ __forceinline__ void pack_add(const PackAgg& t, uint32_t i, uint64_t w, const HashAgg& g) {
-  const uint64_t old = atomicAdd(t.acc + i, static_cast<unsigned long long>(w));
-  if ((old >> kPackCountShift) + (w >> kPackCountShift) >= kPackFlush &&
-      (old >> kPackCountShift) < kPackFlush) {
-    const uint64_t full = atomicExch(t.acc + i, 0ull);
-    uint64_t s, c;
-    unpack(full, &s, &c);
-    global_add(g, t.key[i], s, c);
-  }
-}
-
+// ---- batched shared-table updates -------------------------------------------
 // Slot of key k in the bucket run starting at b, inserting it when absent
-// (the bucket reads are volatile: other threads insert concurrently).  -1
-// when the table has no room for k.
-__device__ __forceinline__ int pack_find_insert(const PackAgg& t, int32_t k, uint32_t b) {
+// (volatile reads: other threads insert concurrently); -1 when the table has
+// no room for k.
+__device__ __forceinline__ int smem_find_insert(const SmemAgg& t, int32_t k, uint32_t b) {
   const uint32_t nb = t.nb;
   for (uint32_t step = 0; step < nb; ++step) {
     const int4 q = lds_volatile_v4(t.key + 4 * b);
@@ -406,67 +347,102 @@ __device__ __forceinline__ int pack_find_insert(const PackAgg& t, int32_t k, uin
   return -1;
 }
 
-// Rows of a thread step (R of them): the home buckets of all R keys are read
-// first (plain shared loads, issued together: a stale read only sends a row
-// to the insert path, since keys are never removed), then each row adds to
-// the slot it found or takes the insert path.  Returns the mask of the rows
-// that found no room in the table (the caller sends them to the global one).
+// R rows (count 1 each) into the shared table, with every step of the R rows
+// issued together: the R home buckets are read first (plain loads: a stale
+// read can only miss a key, since keys are never removed, and a miss takes
+// the volatile insert path), then the R low-word adds whose old values give
+// the carries, the R count adds, and the high words where a carry or a
+// negative value needs one.  Only 32-bit shared atomics: on B200 a 64-bit
+// shared atomicAdd runs several times slower than a 32-bit one.  Returns the
+// mask of the rows that found no room (the caller adds them elsewhere).
 template <int R>
-__device__ __forceinline__ uint32_t pack_rows(const PackAgg& t, const int32_t (&k)[R], const int64_t (&v)[R],
-                                              uint32_t valid, const HashAgg& g) {
-  int4 q[R];
+__device__ __forceinline__ uint32_t smem_agg_rows(const SmemAgg& t, const int32_t (&k)[R], const int64_t (&v)[R],
+                                                  uint32_t valid) {
   uint32_t b[R];
+  int4 q[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     b[r] = mix32(static_cast<uint32_t>(k[r])) & (t.nb - 1);
     q[r] = ((valid >> r) & 1u) ? *reinterpret_cast<const int4*>(t.key + 4 * b[r]) : make_int4(0, 0, 0, 0);
   }
+  int s[R];
   uint32_t lost = 0;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    if (!((valid >> r) & 1u)) continue;
-    int slot = q[r].x == k[r] ? 0 : q[r].y == k[r] ? 1 : q[r].z == k[r] ? 2 : q[r].w == k[r] ? 3 : -1;
-    const int i = slot >= 0 ? static_cast<int>(4 * b[r]) + slot : pack_find_insert(t, k[r], b[r]);
-    if (i >= 0) pack_add(t, static_cast<uint32_t>(i), pack_row(v[r]), g);
-    else lost |= 1u << r;
+    const int j = q[r].x == k[r] ? 0 : q[r].y == k[r] ? 1 : q[r].z == k[r] ? 2 : q[r].w == k[r] ? 3 : -1;
+    s[r] = ((valid >> r) & 1u) && j >= 0 ? static_cast<int>(4 * b[r]) + j : -1;
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    if (((valid >> r) & 1u) && s[r] < 0) {
+      s[r] = smem_find_insert(t, k[r], b[r]);
+      if (s[r] < 0) lost |= 1u << r;
+    }
+  }
+  uint32_t old[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    old[r] = s[r] >= 0 ? atomicAdd(reinterpret_cast<uint32_t*>(t.sum + s[r]), static_cast<uint32_t>(v[r])) : 0u;
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    if (s[r] >= 0) atomicAdd(t.cnt + s[r], 1u);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    if (s[r] < 0) continue;
+    const uint32_t lo = static_cast<uint32_t>(v[r]);
+    const uint32_t hi = static_cast<uint32_t>(static_cast<uint64_t>(v[r]) >> 32) + ((old[r] + lo) < old[r] ? 1u : 0u);
+    if (hi) atomicAdd(reinterpret_cast<uint32_t*>(t.sum + s[r]) + 1, hi);
   }
   return lost;
 }
 
-constexpr int kPackThreads = 512;  // two blocks (2 x 96 KiB tables at 8192 slots) per SM
+constexpr int kRowsThreads = 1024;
 
-// Plan 1 with packed tables: each block aggregates a contiguous share of the
-// rows in a `slots`-slot table (12 bytes per slot), then adds its slots to
-// the global table; a row whose key finds no room goes to the global table.
-__global__ void __launch_bounds__(kPackThreads, 2) group_hash_pack_kernel(int64_t n, const int32_t* __restrict__ keys,
-                                                                          int32_t key_offset,
-                                                                          const int32_t* __restrict__ vals,
-                                                                          const int32_t* __restrict__ vals2,
-                                                                          uint32_t slots, HashAgg g,
-                                                                          unsigned long long* range_err) {
+// Plan 1 with batched updates: each block aggregates a contiguous share of
+// the rows in a `slots`-slot shared table, 4 rows per thread step with the
+// next step's columns already loading (software pipelined), then adds its
+// slots to the global table; a row whose key finds no room goes to the
+// global table directly.
+template <bool HAS2>
+__global__ void __launch_bounds__(kRowsThreads) group_hash_rows_kernel(int64_t n, const int32_t* __restrict__ keys,
+                                                                       int32_t key_offset,
+                                                                       const int32_t* __restrict__ vals,
+                                                                       const int32_t* __restrict__ vals2,
+                                                                       uint32_t slots, HashAgg g,
+                                                                       unsigned long long* range_err) {
   extern __shared__ __align__(16) unsigned char agg_smem[];
-  const PackAgg t = pack_agg(agg_smem, slots);
-  pack_agg_clear(t);
+  const SmemAgg t = smem_agg(agg_smem, slots);
+  smem_agg_clear(t);
   __syncthreads();
   const bool vec = ((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(vals) |
-                     reinterpret_cast<uintptr_t>(vals2)) & 15) == 0;
+                     (HAS2 ? reinterpret_cast<uintptr_t>(vals2) : 0)) & 15) == 0;
   const int64_t per = ((n + gridDim.x - 1) / gridDim.x + 3) & ~int64_t(3);
   const int64_t b = static_cast<int64_t>(blockIdx.x) * per;
   const int64_t e = b + per < n ? b + per : n;
   const uint64_t pol = policy_evict_first();
-  const int32_t* v2 = vals2 ? vals2 : vals;  // a valid address even where the guarded load is hoisted
   unsigned int bad = 0;
-  auto spill = [&](int32_t k, int64_t v) { global_add(g, k, static_cast<uint64_t>(v), 1); };
-  auto one = [&](int64_t r) {
-    const int32_t k = agg_key(keys[r], key_offset);
-    const int64_t v = static_cast<int64_t>(vals[r]) + (vals2 ? vals2[r] : 0);
-    if (k == kEmptyKey) {
-      ++bad;
-      return;
+  auto rows = [&](const int4 kk, const int4 a, const int4 c, uint32_t valid) {
+    const int32_t kr[4] = {kk.x, kk.y, kk.z, kk.w}, ar[4] = {a.x, a.y, a.z, a.w}, cr[4] = {c.x, c.y, c.z, c.w};
+    int32_t k[4];
+    int64_t v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      k[u] = agg_key(kr[u], key_offset);
+      v[u] = static_cast<int64_t>(ar[u]) + (HAS2 ? cr[u] : 0);
+      if (((valid >> u) & 1u) && k[u] == kEmptyKey) {  // reserved as the empty marker
+        ++bad;
+        valid &= ~(1u << u);
+      }
     }
-    const int32_t kk[1] = {k};
-    const int64_t vv[1] = {v};
-    if (pack_rows<1>(t, kk, vv, 1u, g)) spill(k, v);
+    const uint32_t lost = valid ? smem_agg_rows<4>(t, k, v, valid) : 0u;
+    if (lost) {  // rare: keys that found no room in the table
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if ((lost >> u) & 1u) global_add(g, k[u], static_cast<uint64_t>(v[u]), 1);
+    }
+  };
+  auto one = [&](int64_t r) {
+    rows(make_int4(keys[r], 0, 0, 0), make_int4(vals[r], 0, 0, 0), make_int4(HAS2 ? vals2[r] : 0, 0, 0, 0), 1u);
   };
   if (b < e) {
     const int64_t b4 = (b + 3) & ~int64_t(3);
@@ -474,45 +450,37 @@ __global__ void __launch_bounds__(kPackThreads, 2) group_hash_pack_kernel(int64_
     const int64_t n4 = (e - head) >> 2;
     // rows before the first aligned one, and all rows when unaligned: one at a time
     for (int64_t r = b + threadIdx.x; r < head; r += blockDim.x) one(r);
-    // groups of 4 aligned rows per thread step (two blocks per SM keep
-    // enough of them in flight)
-    for (int64_t i = threadIdx.x; i < n4; i += blockDim.x) {
-      const int4 kk = ld_stream_v4(keys + head + 4 * i, pol);
-      const int4 a = ld_stream_v4(vals + head + 4 * i, pol);
-      const int4 c = vals2 ? ld_stream_v4(v2 + head + 4 * i, pol) : make_int4(0, 0, 0, 0);
-      const int32_t kr[4] = {kk.x, kk.y, kk.z, kk.w}, ar[4] = {a.x, a.y, a.z, a.w}, cr[4] = {c.x, c.y, c.z, c.w};
-      int32_t k[4];
-      int64_t v[4];
-      uint32_t valid = 0xFu;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        k[u] = agg_key(kr[u], key_offset);
-        v[u] = static_cast<int64_t>(ar[u]) + cr[u];
-        if (k[u] == kEmptyKey) {
-          ++bad;
-          valid &= ~(1u << u);
-        }
+    const int32_t* kp = keys + head;
+    const int32_t* ap = vals + head;
+    const int32_t* cp = HAS2 ? vals2 + head : vals + head;
+    int64_t i = threadIdx.x;
+    int4 kk = make_int4(0, 0, 0, 0), a = kk, c = kk;
+    if (i < n4) {
+      kk = ld_stream_v4(kp + 4 * i, pol);
+      a = ld_stream_v4(ap + 4 * i, pol);
+      if (HAS2) c = ld_stream_v4(cp + 4 * i, pol);
+    }
+    for (; i < n4; i += blockDim.x) {
+      // the next step's columns load while this step's rows update the table
+      const int64_t nx = i + blockDim.x;
+      int4 kn = make_int4(0, 0, 0, 0), an = kn, cn = kn;
+      if (nx < n4) {
+        kn = ld_stream_v4(kp + 4 * nx, pol);
+        an = ld_stream_v4(ap + 4 * nx, pol);
+        if (HAS2) cn = ld_stream_v4(cp + 4 * nx, pol);
       }
-      const uint32_t lost = valid ? pack_rows<4>(t, k, v, valid, g) : 0u;
-      if (lost) {  // rare: keys that found no room in the table
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if ((lost >> u) & 1u) spill(k[u], v[u]);
-      }
+      rows(kk, a, c, 0xFu);
+      kk = kn;
+      a = an;
+      c = cn;
     }
     for (int64_t r = head + 4 * n4 + threadIdx.x; r < e; r += blockDim.x) one(r);
   }
   const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
   if ((threadIdx.x & 31) == 0 && wbad) atomicAdd(range_err, static_cast<unsigned long long>(wbad));
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) {
-    const uint64_t w = t.acc[i];
-    if (t.key[i] != kEmptyKey && w) {
-      uint64_t s, c;
-      unpack(w, &s, &c);
-      global_add(g, t.key[i], s, c);
-    }
-  }
+  for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x)
+    if (t.key[i] != kEmptyKey && t.cnt[i]) global_add(g, t.key[i], t.sum[i], t.cnt[i]);
 }
 
 // Plan 2.  Partition of a key: the top bits of its hash (the shared tables
@@ -803,6 +771,26 @@ __global__ void __launch_bounds__(kAggThreads) group_part_agg_kernel(
   unsigned int lost = 0;
   // rows of the partition, 8 per thread in flight
   for (int64_t base = b; base < e; base += 8 * static_cast<int64_t>(blockDim.x)) {
+    if (!combine) {  // two batches of 4 rows
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        int32_t k[4];
+        int64_t v[4];
+        uint32_t valid = 0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int64_t i = base + (4 * h + u) * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+          const bool ok = i < e;
+          typename PartRow<HAS2>::T x{};
+          if (ok) x = rows[i];
+          k[u] = ok ? PartRow<HAS2>::key(x) : 0;
+          v[u] = ok ? PartRow<HAS2>::val(x) : 0;
+          valid |= static_cast<uint32_t>(ok) << u;
+        }
+        if (valid) lost += __popc(smem_agg_rows<4>(st, k, v, valid));
+      }
+      continue;
+    }
     typename PartRow<HAS2>::T r[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
@@ -816,7 +804,7 @@ __global__ void __launch_bounds__(kAggThreads) group_part_agg_kernel(
       const int32_t k = ok ? PartRow<HAS2>::key(r[u]) : 0;
       int64_t gs = ok ? PartRow<HAS2>::val(r[u]) : 0;
       uint32_t gc = 1;
-      if (combine ? warp_combine(ok, k, gs, &gs, &gc) : ok)
+      if (warp_combine(ok, k, gs, &gs, &gc))
         if (!smem_agg_add(st, k, static_cast<uint64_t>(gs), gc)) ++lost;
     }
   }
@@ -1037,10 +1025,10 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
   // (measured on B200), so it is off unless the tuning knob asks for it.
   const int combine = ctx->tune[olap::TUNE_GROUP_COMBINE] == 1 ? 1 : 0;
   const int64_t plan_knob = ctx->tune[olap::TUNE_GROUP_PLAN];
-  // Knob: 1 plan 1 where it fits (packed tables), 2 plan 2 always, 3 plan 1
-  // with the 16-byte tables of two 32-bit counters; 0 the default (1).
+  // Knob: 1 plan 1 where it fits (batched table updates), 2 plan 2 always,
+  // 3 plan 1 with one row's table update after another; 0 the default (1).
   const bool plan1 = plan_knob == 2 ? false : capacity <= olap::kAggSlots;
-  const bool packed = plan_knob != 3 && combine == 0;
+  const bool batched = plan_knob != 3 && combine == 0;
   if (plan1) {
     // Plan 1: per-block shared tables of `capacity` slots, then the global
     // table (in the context's grow-only buffer) and its compaction.
@@ -1057,20 +1045,23 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
     olap::fill_i32_kernel<<<olap::grid_of(ctx, capacity, 256, 8), 256, 0, ctx->stream>>>(t.keys, capacity,
                                                                                        olap::kEmptyKey);
     const uint32_t slots = static_cast<uint32_t>(capacity);  // per-block table
-    if (n && e == cudaSuccess && packed) {
-      const size_t smem = static_cast<size_t>(slots) * 12;
-      e = cudaFuncSetAttribute(olap::group_hash_pack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem));
-      int bps = 1;
-      if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, olap::group_hash_pack_kernel, olap::kPackThreads,
-                                                          smem);
-      int64_t grid = static_cast<int64_t>(ctx->sm_count) * (bps < 1 ? 1 : bps);
-      grid = std::min<int64_t>(grid, (n + 4 * olap::kPackThreads - 1) / (4 * olap::kPackThreads));
-      if (e == cudaSuccess)
-        olap::group_hash_pack_kernel<<<static_cast<unsigned>(grid < 1 ? 1 : grid), olap::kPackThreads, smem,
-                                       ctx->stream>>>(n, keys, key_offset, vals, vals2, slots, t,
-                                                      &ctx->counters->range_errors);
+    if (n && e == cudaSuccess && batched) {
+      const size_t smem = static_cast<size_t>(slots) * 16;
+      auto launch = [&](auto kern) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        int bps = 1;
+        if (e == cudaSuccess)
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, olap::kRowsThreads, smem);
+        int64_t grid = static_cast<int64_t>(ctx->sm_count) * (bps < 1 ? 1 : bps);
+        grid = std::min<int64_t>(grid, (n + 4 * olap::kRowsThreads - 1) / (4 * olap::kRowsThreads));
+        if (e == cudaSuccess)
+          kern<<<static_cast<unsigned>(grid < 1 ? 1 : grid), olap::kRowsThreads, smem, ctx->stream>>>(
+              n, keys, key_offset, vals, vals2, slots, t, &ctx->counters->range_errors);
+      };
+      if (vals2)
+        launch(olap::group_hash_rows_kernel<true>);
+      else
+        launch(olap::group_hash_rows_kernel<false>);
     } else if (n && e == cudaSuccess) {
       const size_t smem = static_cast<size_t>(slots) * 16;
       e = cudaFuncSetAttribute(olap::group_hash_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -896,8 +896,7 @@ def sweep_point(a, ctx, name, sele, groups, fk_dist) -> dict:
     torch.cuda.synchronize()
     steps = 10
     # the events go on the stream the context launches on
-    ctx_stream = torch.cuda.ExternalStream(ctx.stream_handle()) if ctx.stream_handle() else \
-        torch.cuda.default_stream()
+    ctx_stream = torch.cuda.ExternalStream(ctx.stream_handle) if ctx.stream_handle else torch.cuda.default_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(0) as clk:
         e0.record(ctx_stream)

@@ -353,11 +353,15 @@ __device__ __forceinline__ int smem_find_insert(const SmemAgg& t, int32_t k, uin
 // the volatile insert path), then the R low-word adds whose old values give
 // the carries, the R count adds, and the high words where a carry or a
 // negative value needs one.  Only 32-bit shared atomics: on B200 a 64-bit
-// shared atomicAdd runs several times slower than a 32-bit one.  Returns the
-// mask of the rows that found no room (the caller adds them elsewhere).
+// shared atomicAdd runs several times slower than a 32-bit one.  `sync`: the
+// lanes of the warp that call together (0 when the callers are not
+// warp-uniform); they are brought back together after the insert path, whose
+// probe loop ends at a different step on each lane (left diverged, the warp
+// would run all later steps once per lane group).  Returns the mask of the
+// rows that found no room (the caller adds them elsewhere).
 template <int R>
 __device__ __forceinline__ uint32_t smem_agg_rows(const SmemAgg& t, const int32_t (&k)[R], const int64_t (&v)[R],
-                                                  uint32_t valid) {
+                                                  uint32_t valid, uint32_t sync) {
   uint32_t b[R];
   int4 q[R];
 #pragma unroll
@@ -379,6 +383,7 @@ __device__ __forceinline__ uint32_t smem_agg_rows(const SmemAgg& t, const int32_
       if (s[r] < 0) lost |= 1u << r;
     }
   }
+  if (sync) __syncwarp(sync);
   uint32_t old[R];
 #pragma unroll
   for (int r = 0; r < R; ++r)
@@ -421,7 +426,7 @@ __global__ void __launch_bounds__(kRowsThreads) group_hash_rows_kernel(int64_t n
   const int64_t e = b + per < n ? b + per : n;
   const uint64_t pol = policy_evict_first();
   unsigned int bad = 0;
-  auto rows = [&](const int4 kk, const int4 a, const int4 c, uint32_t valid) {
+  auto rows = [&](const int4 kk, const int4 a, const int4 c, uint32_t valid, uint32_t sync) {
     const int32_t kr[4] = {kk.x, kk.y, kk.z, kk.w}, ar[4] = {a.x, a.y, a.z, a.w}, cr[4] = {c.x, c.y, c.z, c.w};
     int32_t k[4];
     int64_t v[4];
@@ -434,7 +439,7 @@ __global__ void __launch_bounds__(kRowsThreads) group_hash_rows_kernel(int64_t n
         valid &= ~(1u << u);
       }
     }
-    const uint32_t lost = valid ? smem_agg_rows<4>(t, k, v, valid) : 0u;
+    const uint32_t lost = smem_agg_rows<4>(t, k, v, valid, sync);
     if (lost) {  // rare: keys that found no room in the table
 #pragma unroll
       for (int u = 0; u < 4; ++u)
@@ -442,7 +447,7 @@ __global__ void __launch_bounds__(kRowsThreads) group_hash_rows_kernel(int64_t n
     }
   };
   auto one = [&](int64_t r) {
-    rows(make_int4(keys[r], 0, 0, 0), make_int4(vals[r], 0, 0, 0), make_int4(HAS2 ? vals2[r] : 0, 0, 0, 0), 1u);
+    rows(make_int4(keys[r], 0, 0, 0), make_int4(vals[r], 0, 0, 0), make_int4(HAS2 ? vals2[r] : 0, 0, 0, 0), 1u, 0u);
   };
   if (b < e) {
     const int64_t b4 = (b + 3) & ~int64_t(3);
@@ -453,23 +458,27 @@ __global__ void __launch_bounds__(kRowsThreads) group_hash_rows_kernel(int64_t n
     const int32_t* kp = keys + head;
     const int32_t* ap = vals + head;
     const int32_t* cp = HAS2 ? vals2 + head : vals + head;
-    int64_t i = threadIdx.x;
+    // Every lane of a warp runs the same steps (a lane past the end has no
+    // rows in its last one), so the table updates can bring the warp back
+    // together.
+    const int64_t lane = threadIdx.x & 31;
+    const int64_t w0 = static_cast<int64_t>(threadIdx.x) - lane;
     int4 kk = make_int4(0, 0, 0, 0), a = kk, c = kk;
-    if (i < n4) {
-      kk = ld_stream_v4(kp + 4 * i, pol);
-      a = ld_stream_v4(ap + 4 * i, pol);
-      if (HAS2) c = ld_stream_v4(cp + 4 * i, pol);
+    if (w0 + lane < n4) {
+      kk = ld_stream_v4(kp + 4 * (w0 + lane), pol);
+      a = ld_stream_v4(ap + 4 * (w0 + lane), pol);
+      if (HAS2) c = ld_stream_v4(cp + 4 * (w0 + lane), pol);
     }
-    for (; i < n4; i += blockDim.x) {
+    for (int64_t i0 = w0; i0 < n4; i0 += blockDim.x) {
       // the next step's columns load while this step's rows update the table
-      const int64_t nx = i + blockDim.x;
+      const int64_t i = i0 + lane, nx = i + blockDim.x;
       int4 kn = make_int4(0, 0, 0, 0), an = kn, cn = kn;
       if (nx < n4) {
         kn = ld_stream_v4(kp + 4 * nx, pol);
         an = ld_stream_v4(ap + 4 * nx, pol);
         if (HAS2) cn = ld_stream_v4(cp + 4 * nx, pol);
       }
-      rows(kk, a, c, 0xFu);
+      rows(kk, a, c, i < n4 ? 0xFu : 0u, 0xffffffffu);
       kk = kn;
       a = an;
       c = cn;
@@ -787,7 +796,7 @@ __global__ void __launch_bounds__(kAggThreads) group_part_agg_kernel(
           v[u] = ok ? PartRow<HAS2>::val(x) : 0;
           valid |= static_cast<uint32_t>(ok) << u;
         }
-        if (valid) lost += __popc(smem_agg_rows<4>(st, k, v, valid));
+        lost += __popc(smem_agg_rows<4>(st, k, v, valid, 0xffffffffu));  // the loop is block-uniform
       }
       continue;
     }

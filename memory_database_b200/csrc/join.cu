@@ -172,6 +172,10 @@ __device__ __forceinline__ uint32_t build_region(int32_t k, const BuildPlan& bp)
   return static_cast<uint32_t>((hash32(static_cast<uint32_t>(k)) & bp.mask) >> bp.region_shift);
 }
 
+// The histogram and scatter passes run warp-uniform loops and aggregate a
+// warp's rows per region (match_any): one shared atomic per region present in
+// the warp instead of one per row (a table has few regions, so most rows of a
+// warp share theirs).
 __global__ void __launch_bounds__(kBuildPartThreads) build_hist_kernel(BuildPlan bp, const int32_t* __restrict__ keys,
                                                                       unsigned int* __restrict__ hist,
                                                                       unsigned long long* range_err) {
@@ -180,14 +184,16 @@ __global__ void __launch_bounds__(kBuildPartThreads) build_hist_kernel(BuildPlan
   __syncthreads();
   const int64_t b = static_cast<int64_t>(blockIdx.x) * bp.per;
   const int64_t e = b + bp.per < bp.n ? b + bp.per : bp.n;
+  const int lane = threadIdx.x & 31;
   unsigned int bad = 0;
-  for (int64_t r = b + threadIdx.x; r < e; r += blockDim.x) {
-    const int32_t k = keys[r];
-    if (k == INT32_MIN) {
-      ++bad;
-      continue;
-    }
-    atomicAdd(&s_cnt[build_region(k, bp)], 1u);
+  for (int64_t r0 = b + (threadIdx.x - lane); r0 < e; r0 += blockDim.x) {
+    const int64_t r = r0 + lane;
+    const int32_t k = r < e ? keys[r] : INT32_MIN;
+    if (r < e && k == INT32_MIN) ++bad;
+    const bool live = k != INT32_MIN;
+    const uint32_t reg = live ? build_region(k, bp) : 0xFFFFFFFFu;
+    const unsigned int m = __match_any_sync(0xffffffffu, reg);
+    if (live && lane == __ffs(m) - 1) atomicAdd(&s_cnt[reg], static_cast<unsigned int>(__popc(m)));
   }
   if (bad) atomicAdd(range_err, static_cast<unsigned long long>(bad));
   __syncthreads();
@@ -235,21 +241,35 @@ __global__ void __launch_bounds__(1024) build_scan_kernel(BuildPlan bp, const un
   if (threadIdx.x == blockDim.x - 1) region_begin[P] = s_run[threadIdx.x];
 }
 
+// Shared memory: the block's run starts (P x u64), then its positions taken
+// so far in each run (P x u32).
 __global__ void __launch_bounds__(kBuildPartThreads) build_scatter_kernel(BuildPlan bp,
                                                                          const int32_t* __restrict__ keys,
                                                                          const unsigned long long* __restrict__ offs,
                                                                          uint64_t* __restrict__ tuples) {
-  extern __shared__ unsigned long long s_cur[];
-  for (int p = threadIdx.x; p < bp.n_regions; p += blockDim.x)
-    s_cur[p] = offs[static_cast<int64_t>(blockIdx.x) * bp.n_regions + p];
+  extern __shared__ unsigned long long s_start[];
+  unsigned int* s_taken = reinterpret_cast<unsigned int*>(s_start + bp.n_regions);
+  for (int p = threadIdx.x; p < bp.n_regions; p += blockDim.x) {
+    s_start[p] = offs[static_cast<int64_t>(blockIdx.x) * bp.n_regions + p];
+    s_taken[p] = 0;
+  }
   __syncthreads();
   const int64_t b = static_cast<int64_t>(blockIdx.x) * bp.per;
   const int64_t e = b + bp.per < bp.n ? b + bp.per : bp.n;
-  for (int64_t r = b + threadIdx.x; r < e; r += blockDim.x) {
-    const int32_t k = keys[r];
-    if (k == INT32_MIN) continue;
-    const unsigned long long pos = atomicAdd(&s_cur[build_region(k, bp)], 1ull);
-    tuples[pos] = (static_cast<uint64_t>(static_cast<uint32_t>(k)) << 32) | static_cast<uint32_t>(r);
+  const int lane = threadIdx.x & 31;
+  for (int64_t r0 = b + (threadIdx.x - lane); r0 < e; r0 += blockDim.x) {
+    const int64_t r = r0 + lane;
+    const int32_t k = r < e ? keys[r] : INT32_MIN;
+    const bool live = k != INT32_MIN;
+    const uint32_t reg = live ? build_region(k, bp) : 0xFFFFFFFFu;
+    const unsigned int m = __match_any_sync(0xffffffffu, reg);
+    if (live) {
+      const int leader = __ffs(m) - 1;
+      unsigned int at = 0;
+      if (lane == leader) at = atomicAdd(&s_taken[reg], static_cast<unsigned int>(__popc(m)));
+      at = __shfl_sync(m, at, leader) + __popc(m & ((1u << lane) - 1u));
+      tuples[s_start[reg] + at] = (static_cast<uint64_t>(static_cast<uint32_t>(k)) << 32) | static_cast<uint32_t>(r);
+    }
   }
 }
 
@@ -362,10 +382,10 @@ __device__ __forceinline__ uint32_t hash_lookup4(const uint64_t* __restrict__ sl
 }
 
 template <bool kFilter>
-__global__ void __launch_bounds__(512) hash_probe_sum_kernel(const int32_t* __restrict__ keys, int64_t n,
-                                                             const uint64_t* __restrict__ slots, uint64_t mask,
-                                                             Bloom filter, int vec, unsigned long long* sum,
-                                                             unsigned long long* matches) {
+__global__ void __launch_bounds__(512, 2) hash_probe_sum_kernel(const int32_t* __restrict__ keys, int64_t n,
+                                                                const uint64_t* __restrict__ slots, uint64_t mask,
+                                                                Bloom filter, int vec, unsigned long long* sum,
+                                                                unsigned long long* matches) {
   __shared__ long long s_red[16][2];
   const uint64_t pol = policy_evict_first();
   const uint64_t keep = policy_evict_last();
@@ -599,7 +619,8 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
     auto* offs = reinterpret_cast<unsigned long long*>(mem + ((hist_bytes + 7) & ~size_t(7)));
     auto* rbegin = reinterpret_cast<long long*>(reinterpret_cast<char*>(offs) + offs_bytes);
     auto* tuples = reinterpret_cast<uint64_t*>(mem + tup_off);
-    const size_t hsm = sizeof(unsigned int) * bp.n_regions, csm = sizeof(unsigned long long) * bp.n_regions;
+    const size_t hsm = sizeof(unsigned int) * bp.n_regions;
+    const size_t csm = (sizeof(unsigned long long) + sizeof(unsigned int)) * bp.n_regions;
     olap::build_hist_kernel<<<bp.n_blocks, olap::kBuildPartThreads, hsm, ctx->stream>>>(
         bp, keys, hist, &ctx->counters->range_errors);
     olap::build_scan_kernel<<<1, 1024, 0, ctx->stream>>>(bp, hist, offs, rbegin);

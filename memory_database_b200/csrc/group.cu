@@ -125,8 +125,8 @@ __device__ __forceinline__ void global_add(const HashAgg& t, int32_t k, uint64_t
 // ---- hash group-by --------------------------------------------------------
 //
 // Two plans, chosen by the capacity (a power of two >= 2 x the distinct keys):
-//  * capacity <= kAggSlots: every block keeps a shared-memory table with
-//    `capacity` slots, so each distinct key stays in shared memory; blocks
+//  * capacity <= kAggSlots: every block keeps a shared-memory table of at
+//    least `capacity` slots, so each distinct key stays in shared memory; blocks
 //    flush their tables into the global table once, and the occupied slots
 //    are compacted into the outputs.  One read of the columns.
 //  * larger: the rows are partitioned by high bits of the key hash into P
@@ -145,8 +145,15 @@ struct SmemAgg {
   int32_t* key;
   unsigned int* cnt;
   unsigned long long* sum;
-  uint32_t slots;   // a power of two >= 4
-  uint32_t nb;      // buckets of 4 slots
+  uint32_t slots;   // a multiple of 4
+  uint32_t nb;      // buckets of 4 slots (any count, so a table can fill the shared memory)
+
+  // Home bucket of key k: the low 16 hash bits scaled to [0, nb) (plan 2's
+  // partitions take the high bits); probing wraps after the last bucket.
+  __device__ __forceinline__ uint32_t home(int32_t k) const {
+    return ((mix32(static_cast<uint32_t>(k)) & 0xFFFFu) * nb) >> 16;
+  }
+  __device__ __forceinline__ uint32_t next(uint32_t b) const { return b + 1 == nb ? 0u : b + 1; }
 };
 
 __device__ __forceinline__ SmemAgg smem_agg(unsigned char* base, uint32_t slots) {
@@ -176,15 +183,14 @@ __device__ __forceinline__ int4 lds_volatile_v4(const int32_t* p) {
 
 // Adds (s, c) to key k's slot; false when the table has no room for k.
 // Buckets of 4 slots, probed linearly: one 16-byte read finds k or the first
-// free slot of a bucket, which keeps the probe loops of a warp short at half
+// free slot of a bucket, which keeps the probe loops of a warp short at low
 // load.  Keys are never removed, so a key lives in the first bucket that had
 // a free slot when it was inserted, and a thread that loses a slot's CAS to
-// the same key uses that slot.
-__device__ __forceinline__ bool smem_agg_add(const SmemAgg& t, int32_t k, uint64_t s, uint32_t c) {
-  const uint32_t nb = t.nb;  // a power of two
-  // low hash bits: the partitions of plan 2 use the high ones
-  uint32_t b = mix32(static_cast<uint32_t>(k)) & (nb - 1);
-  for (uint32_t step = 0; step < nb; ++step) {
+// the same key uses that slot.  Returns k's slot from the bucket run starting
+// at b, inserting k when absent (volatile reads: other threads insert
+// concurrently); -1 when the table has no room for k.
+__device__ __forceinline__ int smem_find_insert(const SmemAgg& t, int32_t k, uint32_t b) {
+  for (uint32_t step = 0; step < t.nb; ++step) {
     const int4 q = lds_volatile_v4(t.key + 4 * b);
     int slot = q.x == k ? 0 : q.y == k ? 1 : q.z == k ? 2 : q.w == k ? 3 : -1;
     if (slot < 0 && (q.x == kEmptyKey || q.y == kEmptyKey || q.z == kEmptyKey || q.w == kEmptyKey)) {
@@ -198,14 +204,19 @@ __device__ __forceinline__ bool smem_agg_add(const SmemAgg& t, int32_t k, uint64
         }
       }
     }
-    if (slot >= 0) {
-      smem_add_u64(t.sum + 4 * b + slot, s);
-      atomicAdd(t.cnt + 4 * b + slot, c);
-      return true;
-    }
-    b = (b + 1) & (nb - 1);
+    if (slot >= 0) return static_cast<int>(4 * b) + slot;
+    b = t.next(b);
   }
-  return false;
+  return -1;
+}
+
+// Adds (s, c) to key k's slot; false when the table has no room for k.
+__device__ __forceinline__ bool smem_agg_add(const SmemAgg& t, int32_t k, uint64_t s, uint32_t c) {
+  const int i = smem_find_insert(t, k, t.home(k));
+  if (i < 0) return false;
+  smem_add_u64(t.sum + i, s);
+  atomicAdd(t.cnt + i, c);
+  return true;
 }
 
 // Warp combine of the rows that share a key: returns true on the lane that
@@ -323,30 +334,6 @@ __global__ void __launch_bounds__(kAggThreads) group_hash_smem_kernel(int64_t n,
 }
 
 // ---- batched shared-table updates -------------------------------------------
-// Slot of key k in the bucket run starting at b, inserting it when absent
-// (volatile reads: other threads insert concurrently); -1 when the table has
-// no room for k.
-__device__ __forceinline__ int smem_find_insert(const SmemAgg& t, int32_t k, uint32_t b) {
-  const uint32_t nb = t.nb;
-  for (uint32_t step = 0; step < nb; ++step) {
-    const int4 q = lds_volatile_v4(t.key + 4 * b);
-    int slot = q.x == k ? 0 : q.y == k ? 1 : q.z == k ? 2 : q.w == k ? 3 : -1;
-    if (slot < 0 && (q.x == kEmptyKey || q.y == kEmptyKey || q.z == kEmptyKey || q.w == kEmptyKey)) {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int32_t cur = j == 0 ? q.x : j == 1 ? q.y : j == 2 ? q.z : q.w;
-        if (slot < 0 && cur == kEmptyKey) {
-          const int32_t prev = atomicCAS(t.key + 4 * b + j, kEmptyKey, k);
-          if (prev == kEmptyKey || prev == k) slot = j;
-        }
-      }
-    }
-    if (slot >= 0) return static_cast<int>(4 * b) + slot;
-    b = (b + 1) & (nb - 1);
-  }
-  return -1;
-}
-
 // R rows (count 1 each) into the shared table, with every step of the R rows
 // issued together: the R home buckets are read first (plain loads: a stale
 // read can only miss a key, since keys are never removed, and a miss takes
@@ -366,7 +353,7 @@ __device__ __forceinline__ uint32_t smem_agg_rows(const SmemAgg& t, const int32_
   int4 q[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    b[r] = mix32(static_cast<uint32_t>(k[r])) & (t.nb - 1);
+    b[r] = t.home(k[r]);
     q[r] = ((valid >> r) & 1u) ? *reinterpret_cast<const int4*>(t.key + 4 * b[r]) : make_int4(0, 0, 0, 0);
   }
   int s[R];
@@ -1055,7 +1042,13 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
                                                                                        olap::kEmptyKey);
     const uint32_t slots = static_cast<uint32_t>(capacity);  // per-block table
     if (n && e == cudaSuccess && batched) {
-      const size_t smem = static_cast<size_t>(slots) * 16;
+      // The block tables fill the shared memory once the keys are many: at
+      // lower load fewer keys overflow their home bucket, and the lanes of a
+      // warp take the insert path less often.
+      uint32_t tslots = slots;
+      if (capacity >= 2048)
+        tslots = std::max<uint32_t>(slots, static_cast<uint32_t>(ctx->smem_optin / 16) & ~3u);
+      const size_t smem = static_cast<size_t>(tslots) * 16;
       auto launch = [&](auto kern) {
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         int bps = 1;
@@ -1065,7 +1058,7 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
         grid = std::min<int64_t>(grid, (n + 4 * olap::kRowsThreads - 1) / (4 * olap::kRowsThreads));
         if (e == cudaSuccess)
           kern<<<static_cast<unsigned>(grid < 1 ? 1 : grid), olap::kRowsThreads, smem, ctx->stream>>>(
-              n, keys, key_offset, vals, vals2, slots, t, &ctx->counters->range_errors);
+              n, keys, key_offset, vals, vals2, tslots, t, &ctx->counters->range_errors);
       };
       if (vals2)
         launch(olap::group_hash_rows_kernel<true>);

@@ -273,6 +273,67 @@ __global__ void __launch_bounds__(kBuildPartThreads) build_scatter_kernel(BuildP
   }
 }
 
+// SUM probes into a table larger than L2: the probe keys that pass the filter
+// are grouped by the table region of their home slot (the regions of the
+// region-by-region build), so the probe pass that follows walks the table one
+// L2-resident region after another instead of reading a random DRAM sector
+// per key.  Rows [b, e) of each block, 4 keys per lane (16-byte loads when
+// aligned), regions aggregated per warp as in the build passes.  KEEP = false
+// counts the keys per region, true writes them.
+template <bool kFilter, bool KEEP>
+__global__ void __launch_bounds__(kBuildPartThreads) probe_partition_kernel(
+    BuildPlan bp, const int32_t* __restrict__ keys, Bloom filter, int vec, unsigned int* __restrict__ hist,
+    const unsigned long long* __restrict__ offs, int32_t* __restrict__ out) {
+  extern __shared__ unsigned long long s_part[];
+  unsigned long long* s_start = s_part;  // KEEP: the block's run start in each region
+  unsigned int* s_cnt = reinterpret_cast<unsigned int*>(s_part + (KEEP ? bp.n_regions : 0));
+  for (int p = threadIdx.x; p < bp.n_regions; p += blockDim.x) {
+    if (KEEP) s_start[p] = offs[static_cast<int64_t>(blockIdx.x) * bp.n_regions + p];
+    s_cnt[p] = 0;
+  }
+  __syncthreads();
+  const uint64_t pol = policy_evict_first();
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * bp.per;
+  const int64_t e = b + bp.per < bp.n ? b + bp.per : bp.n;
+  const int lane = threadIdx.x & 31;
+  const int64_t step = 4 * static_cast<int64_t>(blockDim.x);
+  for (int64_t r0 = b + 4 * static_cast<int64_t>(threadIdx.x - lane); r0 < e; r0 += step) {
+    const int64_t r = r0 + 4 * lane;
+    int32_t k[4];
+    if (vec && r + 4 <= e) {
+      const int4 v = ld_stream_v4(keys + r, pol);
+      k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w;
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) k[u] = r + u < e ? keys[r + u] : 0;
+    }
+    uint32_t live = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      live |= static_cast<uint32_t>(r + u < e && bloom_pass<kFilter>(filter, k[u])) << u;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool on = (live >> u) & 1u;
+      const uint32_t reg = on ? build_region(k[u], bp) : 0xFFFFFFFFu;
+      const unsigned int m = __match_any_sync(0xffffffffu, reg);
+      if (on) {
+        const int leader = __ffs(m) - 1;
+        unsigned int at = 0;
+        if (lane == leader) at = atomicAdd(&s_cnt[reg], static_cast<unsigned int>(__popc(m)));
+        if (KEEP) {
+          at = __shfl_sync(m, at, leader) + __popc(m & ((1u << lane) - 1u));
+          out[s_start[reg] + at] = k[u];
+        }
+      }
+    }
+  }
+  if (!KEEP) {
+    __syncthreads();
+    for (int p = threadIdx.x; p < bp.n_regions; p += blockDim.x)
+      hist[static_cast<int64_t>(blockIdx.x) * bp.n_regions + p] = s_cnt[p];
+  }
+}
+
 // Inserts region p's rows (tuples [region_begin[p], region_begin[p+1])).
 __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const long long* __restrict__ region_begin,
                                     int p, uint64_t* __restrict__ slots, uint64_t mask,
@@ -385,8 +446,10 @@ template <bool kFilter>
 __global__ void __launch_bounds__(512, 2) hash_probe_sum_kernel(const int32_t* __restrict__ keys, int64_t n,
                                                                 const uint64_t* __restrict__ slots, uint64_t mask,
                                                                 Bloom filter, int vec, unsigned long long* sum,
-                                                                unsigned long long* matches) {
+                                                                unsigned long long* matches,
+                                                                const long long* n_live) {
   __shared__ long long s_red[16][2];
+  if (n_live) n = *n_live;  // keys written by an earlier pass: the count is on the device
   const uint64_t pol = policy_evict_first();
   const uint64_t keep = policy_evict_last();
   int64_t s = 0, c = 0;
@@ -567,6 +630,59 @@ static unsigned grid_for(const olap_ctx* ctx, int64_t items, int threads) {
   return static_cast<unsigned>(g < 1 ? 1 : g);
 }
 
+// Plan of the region passes over a table of `capacity` slots for n rows.
+static BuildPlan region_plan(const olap_ctx* ctx, int64_t n, int64_t capacity, int64_t align) {
+  BuildPlan bp;
+  bp.n = n;
+  bp.mask = static_cast<uint64_t>(capacity - 1);
+  bp.n_regions = static_cast<int32_t>(capacity / kBuildRegionSlots);
+  int lg_cap = 0;
+  while ((int64_t(1) << lg_cap) < capacity) ++lg_cap;
+  int lg_p = 0;
+  while ((1 << lg_p) < bp.n_regions) ++lg_p;
+  bp.region_shift = lg_cap - lg_p;
+  bp.n_blocks = ctx->sm_count * 2;
+  bp.per = ((n + bp.n_blocks - 1) / bp.n_blocks + align - 1) / align * align;
+  return bp;
+}
+
+// SUM probe of n keys with the keys grouped by table region first (counts,
+// offsets, the grouped keys in the context's grow-only buffer), then one
+// probe pass over the grouped keys, whose count stays on the device.
+template <bool kFilter>
+int probe_sum_by_region(olap_ctx* ctx, const uint64_t* table, int64_t capacity, const Bloom& bloom,
+                        const int32_t* keys, int64_t n, unsigned long long* d_sum, unsigned long long* d_matches) {
+  const BuildPlan bp = region_plan(ctx, n, capacity, 4);
+  if (bp.n_regions > 2048) return set_error(ctx, OLAP_ERR_UNSUPPORTED, "hash table capacity above 2^33 slots");
+  const size_t hist_bytes = sizeof(unsigned int) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
+  const size_t offs_bytes = sizeof(unsigned long long) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
+  const size_t begin_bytes = sizeof(long long) * (bp.n_regions + 1);
+  const size_t keys_off = (hist_bytes + 8 + offs_bytes + begin_bytes + 255) & ~size_t(255);
+  char* mem = big_scratch(ctx, keys_off + sizeof(int32_t) * static_cast<size_t>(n));
+  if (!mem) return set_error(ctx, OLAP_ERR_NOMEM, "device memory for the grouped probe keys");
+  auto* hist = reinterpret_cast<unsigned int*>(mem);
+  auto* offs = reinterpret_cast<unsigned long long*>(mem + ((hist_bytes + 7) & ~size_t(7)));
+  auto* rbegin = reinterpret_cast<long long*>(reinterpret_cast<char*>(offs) + offs_bytes);
+  auto* grouped = reinterpret_cast<int32_t*>(mem + keys_off);
+  const int vec = al16(keys);
+  const size_t hsm = sizeof(unsigned int) * bp.n_regions;
+  const size_t ssm = (sizeof(unsigned long long) + sizeof(unsigned int)) * bp.n_regions;
+  probe_partition_kernel<kFilter, false><<<bp.n_blocks, kBuildPartThreads, hsm, ctx->stream>>>(
+      bp, keys, bloom, vec, hist, nullptr, nullptr);
+  build_scan_kernel<<<1, 1024, 0, ctx->stream>>>(bp, hist, offs, rbegin);
+  probe_partition_kernel<kFilter, true><<<bp.n_blocks, kBuildPartThreads, ssm, ctx->stream>>>(
+      bp, keys, bloom, vec, nullptr, offs, grouped);
+  Bloom none;
+  none.words = nullptr;
+  none.shift = 32;
+  // keys in region order: the grid walks the grouped keys front to back, so
+  // the table regions are visited one after another
+  hash_probe_sum_kernel<false><<<grid_for(ctx, (n + 3) / 4, 512), 512, 0, ctx->stream>>>(
+      grouped, n, table, bp.mask, none, 1, d_sum, d_matches, rbegin + bp.n_regions);
+  OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  return OLAP_OK;
+}
+
 }  // namespace olap
 
 extern "C" {
@@ -597,22 +713,12 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
   const bool partitioned = capacity > olap::kBuildRegionSlots && n >= (int64_t(1) << 16) &&
                            ctx->tune[olap::TUNE_JOIN_BUILD] != 2;
   if (n && partitioned) {
-    olap::BuildPlan bp;
-    bp.n = n;
-    bp.mask = static_cast<uint64_t>(capacity - 1);
-    bp.n_regions = static_cast<int32_t>(capacity / olap::kBuildRegionSlots);
-    int lg_cap = 0;
-    while ((int64_t(1) << lg_cap) < capacity) ++lg_cap;
-    int lg_p = 0;
-    while ((1 << lg_p) < bp.n_regions) ++lg_p;
-    bp.region_shift = lg_cap - lg_p;
-    bp.n_blocks = ctx->sm_count * 2;
-    bp.per = (n + bp.n_blocks - 1) / bp.n_blocks;
+    const olap::BuildPlan bp = olap::region_plan(ctx, n, capacity, 1);
     OLAP_REQUIRE(ctx, bp.n_regions <= 2048, "hash table capacity above 2^33 slots");
     const size_t hist_bytes = sizeof(unsigned int) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
     const size_t offs_bytes = sizeof(unsigned long long) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
     const size_t begin_bytes = sizeof(long long) * (bp.n_regions + 1);
-    const size_t tup_off = (hist_bytes + offs_bytes + begin_bytes + 255) & ~size_t(255);
+    const size_t tup_off = (hist_bytes + 8 + offs_bytes + begin_bytes + 255) & ~size_t(255);
     char* mem = olap::big_scratch(ctx, tup_off + sizeof(uint64_t) * static_cast<size_t>(n));
     if (!mem) return olap::set_error(ctx, OLAP_ERR_NOMEM, "device memory for the build partitions");
     auto* hist = reinterpret_cast<unsigned int*>(mem);
@@ -699,15 +805,23 @@ int olap_hashjoin_probe_filtered(olap_ctx* ctx, const uint64_t* table, int64_t c
     if (!m) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
     OLAP_CUDA_TRY(ctx, cudaMemsetAsync(d_sum, 0, sizeof(int64_t), ctx->stream));
     OLAP_CUDA_TRY(ctx, cudaMemsetAsync(m, 0, sizeof(int64_t), ctx->stream));
-    if (n) {
+    auto* ds = reinterpret_cast<unsigned long long*>(d_sum);
+    // Many keys into a table larger than one region: partition the keys by
+    // region first, unless OLAP_TUNE_JOIN_BUILD = 2 asks for whole-table passes.
+    const bool partitioned = capacity > olap::kBuildRegionSlots && n >= (int64_t(1) << 22) &&
+                             ctx->tune[olap::TUNE_JOIN_BUILD] != 2;
+    if (n && partitioned) {
+      const int rc = filter ? olap::probe_sum_by_region<true>(ctx, table, capacity, bloom, keys, n, ds, m)
+                            : olap::probe_sum_by_region<false>(ctx, table, capacity, bloom, keys, n, ds, m);
+      if (rc != OLAP_OK) return rc;
+    } else if (n) {
       const dim3 grid(olap::grid_for(ctx, (n + 3) / 4, 512));
-      auto* ds = reinterpret_cast<unsigned long long*>(d_sum);
       if (filter)
         olap::hash_probe_sum_kernel<true><<<grid, 512, 0, ctx->stream>>>(keys, n, table, mask, bloom,
-                                                                        olap::al16(keys), ds, m);
+                                                                        olap::al16(keys), ds, m, nullptr);
       else
         olap::hash_probe_sum_kernel<false><<<grid, 512, 0, ctx->stream>>>(keys, n, table, mask, bloom,
-                                                                         olap::al16(keys), ds, m);
+                                                                         olap::al16(keys), ds, m, nullptr);
     }
     OLAP_CUDA_TRY(ctx, cudaGetLastError());
   }

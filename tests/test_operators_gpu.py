@@ -350,6 +350,31 @@ def test_bounded_device_wait_reports_timeout_and_context_survives(ctx):
     assert np.array_equal(host(ops.select_rowids(dev(col), 99, ctx=ctx)), np.arange(100, dtype=np.int32))
 
 
+@pytest.mark.parametrize("bloom", [True, False])
+@pytest.mark.parametrize("mode", [0, 2])
+def test_hash_join_region_probe(ctx, bloom, mode):
+    """SUM probes of at least 2^22 keys into a table larger than one region
+    group their keys by table region first (mode 0, the default) or probe the
+    whole table directly (OLAP_TUNE_JOIN_BUILD = 2); with and without the
+    Bloom filter, aligned and unaligned keys, a ragged count, edge keys: the
+    same (sum, matches) as the oracle."""
+    rng = np.random.default_rng(37)
+    n = (1 << 22) + 5
+    rk = rng.integers(-(1 << 23), 1 << 23, n).astype(np.int32)  # duplicates and negatives
+    rp = rng.integers(-1000, 1000, n).astype(np.int32)
+    sk = rng.integers(-(1 << 23), 1 << 23, (1 << 22) + 1001).astype(np.int32)
+    sk[:7] = [np.iinfo(np.int32).min, np.iinfo(np.int32).max, 0, -1, 1, rk[0], rk[-1]]
+    ht = ops.HashTable(n, ctx=ctx, bloom=bloom).build(dev(rk), dev(rp))
+    assert ht.capacity == 1 << 24
+    ctx.set_tuning(_lib.TUNE_JOIN_BUILD, mode)
+    try:
+        d = dev(sk)
+        assert ht.probe(d) == oracle.hashjoin(rk, rp, sk)
+        assert ht.probe(d[1:]) == oracle.hashjoin(rk, rp, sk[1:])
+    finally:
+        ctx.set_tuning(_lib.TUNE_JOIN_BUILD, 0)
+
+
 @pytest.mark.parametrize("mode", [0, 2])
 def test_hash_join_region_build(ctx, mode):
     """A build side whose table is larger than one 32 MB region (2^22 rows:

@@ -368,7 +368,8 @@ OLAP_API int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32
  * *d_matches the match count (may be NULL).  With out_rows/out_payload the
  * matches (probe row, payload) are also written in probe-row order (then
  * *d_matches, or the count of a NULL d_sum call, is their number).  A SUM
- * call (no pairs) of 2^22 keys or more into a table above 32 MB first groups
+ * call (no pairs) of 2^22 keys or more into a table above 32 MB (and up to
+ * 2^27 slots, 1 GB) first groups
  * its keys by the 32 MB region of their home slot (4 bytes per key of
  * scratch from the context's grow-only buffer), then probes the regions one
  * after another, each resident in L2; OLAP_TUNE_JOIN_BUILD = 2 probes in key

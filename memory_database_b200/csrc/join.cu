@@ -273,65 +273,111 @@ __global__ void __launch_bounds__(kBuildPartThreads) build_scatter_kernel(BuildP
   }
 }
 
-// SUM probes into a table larger than L2: the probe keys that pass the filter
-// are grouped by the table region of their home slot (the regions of the
-// region-by-region build), so the probe pass that follows walks the table one
-// L2-resident region after another instead of reading a random DRAM sector
-// per key.  Rows [b, e) of each block, 4 keys per lane (16-byte loads when
-// aligned), regions aggregated per warp as in the build passes.  KEEP = false
-// counts the keys per region, true writes them.
-template <bool kFilter, bool KEEP>
-__global__ void __launch_bounds__(kBuildPartThreads) probe_partition_kernel(
-    BuildPlan bp, const int32_t* __restrict__ keys, Bloom filter, int vec, unsigned int* __restrict__ hist,
-    const unsigned long long* __restrict__ offs, int32_t* __restrict__ out) {
-  extern __shared__ unsigned long long s_part[];
-  unsigned long long* s_start = s_part;  // KEEP: the block's run start in each region
-  unsigned int* s_cnt = reinterpret_cast<unsigned int*>(s_part + (KEEP ? bp.n_regions : 0));
-  for (int p = threadIdx.x; p < bp.n_regions; p += blockDim.x) {
-    if (KEEP) s_start[p] = offs[static_cast<int64_t>(blockIdx.x) * bp.n_regions + p];
-    s_cnt[p] = 0;
-  }
-  __syncthreads();
-  const uint64_t pol = policy_evict_first();
-  const int64_t b = static_cast<int64_t>(blockIdx.x) * bp.per;
-  const int64_t e = b + bp.per < bp.n ? b + bp.per : bp.n;
-  const int lane = threadIdx.x & 31;
-  const int64_t step = 4 * static_cast<int64_t>(blockDim.x);
-  for (int64_t r0 = b + 4 * static_cast<int64_t>(threadIdx.x - lane); r0 < e; r0 += step) {
-    const int64_t r = r0 + 4 * lane;
-    int32_t k[4];
-    if (vec && r + 4 <= e) {
-      const int4 v = ld_stream_v4(keys + r, pol);
-      k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w;
-    } else {
+// SUM probes into a table larger than L2: the probe keys are grouped by the
+// table region of their home slot (the regions of the region-by-region
+// build), so the probe pass that follows walks the table one L2-resident
+// region after another instead of reading a random DRAM sector per key.
+// A radix partition by warps: warp w takes a contiguous segment of the keys
+// (a multiple of 128: 4 keys per lane, 16-byte loads when aligned), counts
+// its keys per region with one ballot per region (lane p keeps region p's
+// count; at most 32 regions), and the scatter pass re-reads the segment and
+// writes each key at its warp's next position in its region.  Counts are
+// region-major (hist[p * W + w]), so one exclusive scan gives every warp's
+// run start.
+struct RegionPass {
+  BuildPlan bp;
+  int64_t seg;       // keys per warp
+  int32_t n_warps;   // W
+  int32_t vec;       // keys 16-byte aligned
+};
+
+__device__ __forceinline__ void region_keys(const RegionPass& rp, const int32_t* __restrict__ keys, int64_t r,
+                                            int64_t e, uint64_t pol, int32_t (&k)[4], uint32_t (&reg)[4]) {
+  if (rp.vec && r + 4 <= e) {
+    const int4 v = ld_stream_v4(keys + r, pol);
+    k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w;
+  } else {
 #pragma unroll
-      for (int u = 0; u < 4; ++u) k[u] = r + u < e ? keys[r + u] : 0;
-    }
-    uint32_t live = 0;
+    for (int u = 0; u < 4; ++u) k[u] = r + u < e ? keys[r + u] : 0;
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) reg[u] = r + u < e ? build_region(k[u], rp.bp) : 0xFFFFFFFFu;
+}
+
+__global__ void __launch_bounds__(kBuildPartThreads) region_hist_kernel(RegionPass rp, const int32_t* __restrict__ keys,
+                                                                       unsigned int* __restrict__ hist) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t b = w * rp.seg;
+  const int64_t e = b + rp.seg < rp.bp.n ? b + rp.seg : rp.bp.n;
+  const int P = rp.bp.n_regions;
+  const uint64_t pol = policy_evict_first();
+  unsigned int cnt = 0;  // lane p: the segment's keys in region p
+  for (int64_t r0 = b; r0 < e; r0 += 128) {
+    int32_t k[4];
+    uint32_t reg[4];
+    region_keys(rp, keys, r0 + 4 * lane, e, pol, k, reg);
 #pragma unroll
     for (int u = 0; u < 4; ++u)
-      live |= static_cast<uint32_t>(r + u < e && bloom_pass<kFilter>(filter, k[u])) << u;
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const bool on = (live >> u) & 1u;
-      const uint32_t reg = on ? build_region(k[u], bp) : 0xFFFFFFFFu;
-      const unsigned int m = __match_any_sync(0xffffffffu, reg);
-      if (on) {
-        const int leader = __ffs(m) - 1;
-        unsigned int at = 0;
-        if (lane == leader) at = atomicAdd(&s_cnt[reg], static_cast<unsigned int>(__popc(m)));
-        if (KEEP) {
-          at = __shfl_sync(m, at, leader) + __popc(m & ((1u << lane) - 1u));
-          out[s_start[reg] + at] = k[u];
-        }
+      for (int p = 0; p < P; ++p) {
+        const unsigned int m = __ballot_sync(0xffffffffu, reg[u] == static_cast<uint32_t>(p));
+        cnt += lane == p ? __popc(m) : 0u;
       }
-    }
   }
-  if (!KEEP) {
+  if (lane < P && w < rp.n_warps) hist[static_cast<int64_t>(lane) * rp.n_warps + w] = cnt;
+}
+
+__global__ void __launch_bounds__(kBuildPartThreads) region_scatter_kernel(RegionPass rp,
+                                                                          const int32_t* __restrict__ keys,
+                                                                          const unsigned int* __restrict__ start,
+                                                                          int32_t* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t b = w * rp.seg;
+  const int64_t e = b + rp.seg < rp.bp.n ? b + rp.seg : rp.bp.n;
+  const int P = rp.bp.n_regions;
+  const uint64_t pol = policy_evict_first();
+  const unsigned int lt = (1u << lane) - 1u;
+  // lane p: the next position of this warp's run in region p
+  unsigned int next = lane < P && w < rp.n_warps ? start[static_cast<int64_t>(lane) * rp.n_warps + w] : 0u;
+  for (int64_t r0 = b; r0 < e; r0 += 128) {
+    int32_t k[4];
+    uint32_t reg[4];
+    region_keys(rp, keys, r0 + 4 * lane, e, pol, k, reg);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      for (int p = 0; p < P; ++p) {
+        const unsigned int m = __ballot_sync(0xffffffffu, reg[u] == static_cast<uint32_t>(p));
+        const unsigned int at = __shfl_sync(0xffffffffu, next, p);
+        if (reg[u] == static_cast<uint32_t>(p)) out[at + __popc(m & lt)] = k[u];
+        next += lane == p ? __popc(m) : 0u;
+      }
+  }
+}
+
+// Exclusive scan of m counts (one block); out[m] = the total.
+__global__ void __launch_bounds__(1024) scan_counts_kernel(const unsigned int* __restrict__ in, int64_t m,
+                                                           unsigned int* __restrict__ out) {
+  __shared__ unsigned int s_run[1024];
+  const int64_t per = (m + blockDim.x - 1) / blockDim.x;
+  const int64_t lo = threadIdx.x * per, hi = lo + per < m ? lo + per : m;
+  unsigned int mine = 0;
+  for (int64_t i = lo; i < hi; ++i) mine += in[i];
+  s_run[threadIdx.x] = mine;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const unsigned int y = threadIdx.x >= o ? s_run[threadIdx.x - o] : 0u;
     __syncthreads();
-    for (int p = threadIdx.x; p < bp.n_regions; p += blockDim.x)
-      hist[static_cast<int64_t>(blockIdx.x) * bp.n_regions + p] = s_cnt[p];
+    s_run[threadIdx.x] += y;
+    __syncthreads();
   }
+  unsigned int run = s_run[threadIdx.x] - mine;
+  for (int64_t i = lo; i < hi; ++i) {
+    const unsigned int c = in[i];
+    out[i] = run;
+    run += c;
+  }
+  if (threadIdx.x == blockDim.x - 1) out[m] = s_run[threadIdx.x];
 }
 
 // Inserts region p's rows (tuples [region_begin[p], region_begin[p+1])).
@@ -446,10 +492,8 @@ template <bool kFilter>
 __global__ void __launch_bounds__(512, 2) hash_probe_sum_kernel(const int32_t* __restrict__ keys, int64_t n,
                                                                 const uint64_t* __restrict__ slots, uint64_t mask,
                                                                 Bloom filter, int vec, unsigned long long* sum,
-                                                                unsigned long long* matches,
-                                                                const long long* n_live) {
+                                                                unsigned long long* matches) {
   __shared__ long long s_red[16][2];
-  if (n_live) n = *n_live;  // keys written by an earlier pass: the count is on the device
   const uint64_t pol = policy_evict_first();
   const uint64_t keep = policy_evict_last();
   int64_t s = 0, c = 0;
@@ -647,38 +691,37 @@ static BuildPlan region_plan(const olap_ctx* ctx, int64_t n, int64_t capacity, i
 }
 
 // SUM probe of n keys with the keys grouped by table region first (counts,
-// offsets, the grouped keys in the context's grow-only buffer), then one
-// probe pass over the grouped keys, whose count stays on the device.
-template <bool kFilter>
-int probe_sum_by_region(olap_ctx* ctx, const uint64_t* table, int64_t capacity, const Bloom& bloom,
-                        const int32_t* keys, int64_t n, unsigned long long* d_sum, unsigned long long* d_matches) {
-  const BuildPlan bp = region_plan(ctx, n, capacity, 4);
-  if (bp.n_regions > 2048) return set_error(ctx, OLAP_ERR_UNSUPPORTED, "hash table capacity above 2^33 slots");
-  const size_t hist_bytes = sizeof(unsigned int) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
-  const size_t offs_bytes = sizeof(unsigned long long) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
-  const size_t begin_bytes = sizeof(long long) * (bp.n_regions + 1);
-  const size_t keys_off = (hist_bytes + 8 + offs_bytes + begin_bytes + 255) & ~size_t(255);
+// run starts and the grouped keys in the context's grow-only buffer), then
+// one probe pass over the grouped keys.  The filter is not needed there:
+// every lookup reads the L2-resident region.
+int probe_sum_by_region(olap_ctx* ctx, const uint64_t* table, int64_t capacity, const int32_t* keys, int64_t n,
+                        unsigned long long* d_sum, unsigned long long* d_matches) {
+  RegionPass rp;
+  rp.bp = region_plan(ctx, n, capacity, 4);
+  rp.vec = al16(keys);
+  const int threads = kBuildPartThreads;
+  const int64_t blocks = static_cast<int64_t>(ctx->sm_count) * (2048 / threads);
+  rp.n_warps = static_cast<int32_t>(blocks * (threads / 32));
+  rp.seg = ((n + rp.n_warps - 1) / rp.n_warps + 127) / 128 * 128;
+  const int64_t m = static_cast<int64_t>(rp.bp.n_regions) * rp.n_warps;
+  const size_t cnt_bytes = sizeof(unsigned int) * static_cast<size_t>(m);
+  const size_t start_bytes = sizeof(unsigned int) * static_cast<size_t>(m + 1);
+  const size_t keys_off = (cnt_bytes + start_bytes + 255) & ~size_t(255);
   char* mem = big_scratch(ctx, keys_off + sizeof(int32_t) * static_cast<size_t>(n));
   if (!mem) return set_error(ctx, OLAP_ERR_NOMEM, "device memory for the grouped probe keys");
   auto* hist = reinterpret_cast<unsigned int*>(mem);
-  auto* offs = reinterpret_cast<unsigned long long*>(mem + ((hist_bytes + 7) & ~size_t(7)));
-  auto* rbegin = reinterpret_cast<long long*>(reinterpret_cast<char*>(offs) + offs_bytes);
+  auto* start = reinterpret_cast<unsigned int*>(mem + cnt_bytes);
   auto* grouped = reinterpret_cast<int32_t*>(mem + keys_off);
-  const int vec = al16(keys);
-  const size_t hsm = sizeof(unsigned int) * bp.n_regions;
-  const size_t ssm = (sizeof(unsigned long long) + sizeof(unsigned int)) * bp.n_regions;
-  probe_partition_kernel<kFilter, false><<<bp.n_blocks, kBuildPartThreads, hsm, ctx->stream>>>(
-      bp, keys, bloom, vec, hist, nullptr, nullptr);
-  build_scan_kernel<<<1, 1024, 0, ctx->stream>>>(bp, hist, offs, rbegin);
-  probe_partition_kernel<kFilter, true><<<bp.n_blocks, kBuildPartThreads, ssm, ctx->stream>>>(
-      bp, keys, bloom, vec, nullptr, offs, grouped);
+  region_hist_kernel<<<static_cast<unsigned>(blocks), threads, 0, ctx->stream>>>(rp, keys, hist);
+  scan_counts_kernel<<<1, 1024, 0, ctx->stream>>>(hist, m, start);
+  region_scatter_kernel<<<static_cast<unsigned>(blocks), threads, 0, ctx->stream>>>(rp, keys, start, grouped);
   Bloom none;
   none.words = nullptr;
   none.shift = 32;
   // keys in region order: the grid walks the grouped keys front to back, so
   // the table regions are visited one after another
   hash_probe_sum_kernel<false><<<grid_for(ctx, (n + 3) / 4, 512), 512, 0, ctx->stream>>>(
-      grouped, n, table, bp.mask, none, 1, d_sum, d_matches, rbegin + bp.n_regions);
+      grouped, n, table, rp.bp.mask, none, 1, d_sum, d_matches);
   OLAP_CUDA_TRY(ctx, cudaGetLastError());
   return OLAP_OK;
 }
@@ -808,20 +851,19 @@ int olap_hashjoin_probe_filtered(olap_ctx* ctx, const uint64_t* table, int64_t c
     auto* ds = reinterpret_cast<unsigned long long*>(d_sum);
     // Many keys into a table larger than one region: partition the keys by
     // region first, unless OLAP_TUNE_JOIN_BUILD = 2 asks for whole-table passes.
-    const bool partitioned = capacity > olap::kBuildRegionSlots && n >= (int64_t(1) << 22) &&
-                             ctx->tune[olap::TUNE_JOIN_BUILD] != 2;
+    const bool partitioned = capacity > olap::kBuildRegionSlots && capacity <= 32 * olap::kBuildRegionSlots &&
+                             n >= (int64_t(1) << 22) && ctx->tune[olap::TUNE_JOIN_BUILD] != 2;
     if (n && partitioned) {
-      const int rc = filter ? olap::probe_sum_by_region<true>(ctx, table, capacity, bloom, keys, n, ds, m)
-                            : olap::probe_sum_by_region<false>(ctx, table, capacity, bloom, keys, n, ds, m);
+      const int rc = olap::probe_sum_by_region(ctx, table, capacity, keys, n, ds, m);
       if (rc != OLAP_OK) return rc;
     } else if (n) {
       const dim3 grid(olap::grid_for(ctx, (n + 3) / 4, 512));
       if (filter)
         olap::hash_probe_sum_kernel<true><<<grid, 512, 0, ctx->stream>>>(keys, n, table, mask, bloom,
-                                                                        olap::al16(keys), ds, m, nullptr);
+                                                                        olap::al16(keys), ds, m);
       else
         olap::hash_probe_sum_kernel<false><<<grid, 512, 0, ctx->stream>>>(keys, n, table, mask, bloom,
-                                                                         olap::al16(keys), ds, m, nullptr);
+                                                                         olap::al16(keys), ds, m);
     }
     OLAP_CUDA_TRY(ctx, cudaGetLastError());
   }

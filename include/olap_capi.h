@@ -83,10 +83,8 @@ extern "C" {
                                        3 in place always */
 #define OLAP_TUNE_MERGE_PROBES 14   /* star-join: 1 probes consecutive L2 int8 dimensions together, 2 off */
 #define OLAP_TUNE_PROBE_ORDER 15    /* star-join: 1 probes the dimensions staged as int8 last, 2 first */
-#define OLAP_TUNE_JOIN_BUILD 16     /* hash join over tables above 32 MB: 1 region by region (the
-                                       default: builds insert one region at a time, SUM probes of 2^22
-                                       keys or more group their keys by region first), 2 whole-table
-                                       passes (one random DRAM sector per insert or probe) */
+#define OLAP_TUNE_JOIN_BUILD 16     /* hash join build: 1 region by region (the default for tables above
+                                       32 MB), 2 direct (one random DRAM sector per insert) */
 #define OLAP_TUNE_KNOBS 17          /* knobs olap_ctx_set_tuning accepts (the autotuner sets 0..15) */
 
 typedef struct olap_ctx olap_ctx;
@@ -367,13 +365,7 @@ OLAP_API int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32
  * matched payloads (a missing key adds 0, as operator[] inserts 0) and
  * *d_matches the match count (may be NULL).  With out_rows/out_payload the
  * matches (probe row, payload) are also written in probe-row order (then
- * *d_matches, or the count of a NULL d_sum call, is their number).  A SUM
- * call (no pairs) of 2^22 keys or more into a table above 32 MB (and up to
- * 2^27 slots, 1 GB) first groups
- * its keys by the 32 MB region of their home slot (4 bytes per key of
- * scratch from the context's grow-only buffer), then probes the regions one
- * after another, each resident in L2; OLAP_TUNE_JOIN_BUILD = 2 probes in key
- * order instead.  Asynchronous. */
+ * *d_matches, or the count of a NULL d_sum call, is their number). */
 OLAP_API int olap_hashjoin_probe(olap_ctx* ctx, const uint64_t* table, int64_t capacity,
                                  const int32_t* keys, int64_t n, int64_t* d_sum, int64_t* d_matches,
                                  int32_t* out_rows, int32_t* out_payload);

@@ -273,113 +273,6 @@ __global__ void __launch_bounds__(kBuildPartThreads) build_scatter_kernel(BuildP
   }
 }
 
-// SUM probes into a table larger than L2: the probe keys are grouped by the
-// table region of their home slot (the regions of the region-by-region
-// build), so the probe pass that follows walks the table one L2-resident
-// region after another instead of reading a random DRAM sector per key.
-// A radix partition by warps: warp w takes a contiguous segment of the keys
-// (a multiple of 128: 4 keys per lane, 16-byte loads when aligned), counts
-// its keys per region with one ballot per region (lane p keeps region p's
-// count; at most 32 regions), and the scatter pass re-reads the segment and
-// writes each key at its warp's next position in its region.  Counts are
-// region-major (hist[p * W + w]), so one exclusive scan gives every warp's
-// run start.
-struct RegionPass {
-  BuildPlan bp;
-  int64_t seg;       // keys per warp
-  int32_t n_warps;   // W
-  int32_t vec;       // keys 16-byte aligned
-};
-
-__device__ __forceinline__ void region_keys(const RegionPass& rp, const int32_t* __restrict__ keys, int64_t r,
-                                            int64_t e, uint64_t pol, int32_t (&k)[4], uint32_t (&reg)[4]) {
-  if (rp.vec && r + 4 <= e) {
-    const int4 v = ld_stream_v4(keys + r, pol);
-    k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w;
-  } else {
-#pragma unroll
-    for (int u = 0; u < 4; ++u) k[u] = r + u < e ? keys[r + u] : 0;
-  }
-#pragma unroll
-  for (int u = 0; u < 4; ++u) reg[u] = r + u < e ? build_region(k[u], rp.bp) : 0xFFFFFFFFu;
-}
-
-__global__ void __launch_bounds__(kBuildPartThreads) region_hist_kernel(RegionPass rp, const int32_t* __restrict__ keys,
-                                                                       unsigned int* __restrict__ hist) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int64_t b = w * rp.seg;
-  const int64_t e = b + rp.seg < rp.bp.n ? b + rp.seg : rp.bp.n;
-  const int P = rp.bp.n_regions;
-  const uint64_t pol = policy_evict_first();
-  unsigned int cnt = 0;  // lane p: the segment's keys in region p
-  for (int64_t r0 = b; r0 < e; r0 += 128) {
-    int32_t k[4];
-    uint32_t reg[4];
-    region_keys(rp, keys, r0 + 4 * lane, e, pol, k, reg);
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-      for (int p = 0; p < P; ++p) {
-        const unsigned int m = __ballot_sync(0xffffffffu, reg[u] == static_cast<uint32_t>(p));
-        cnt += lane == p ? __popc(m) : 0u;
-      }
-  }
-  if (lane < P && w < rp.n_warps) hist[static_cast<int64_t>(lane) * rp.n_warps + w] = cnt;
-}
-
-__global__ void __launch_bounds__(kBuildPartThreads) region_scatter_kernel(RegionPass rp,
-                                                                          const int32_t* __restrict__ keys,
-                                                                          const unsigned int* __restrict__ start,
-                                                                          int32_t* __restrict__ out) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int64_t b = w * rp.seg;
-  const int64_t e = b + rp.seg < rp.bp.n ? b + rp.seg : rp.bp.n;
-  const int P = rp.bp.n_regions;
-  const uint64_t pol = policy_evict_first();
-  const unsigned int lt = (1u << lane) - 1u;
-  // lane p: the next position of this warp's run in region p
-  unsigned int next = lane < P && w < rp.n_warps ? start[static_cast<int64_t>(lane) * rp.n_warps + w] : 0u;
-  for (int64_t r0 = b; r0 < e; r0 += 128) {
-    int32_t k[4];
-    uint32_t reg[4];
-    region_keys(rp, keys, r0 + 4 * lane, e, pol, k, reg);
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-      for (int p = 0; p < P; ++p) {
-        const unsigned int m = __ballot_sync(0xffffffffu, reg[u] == static_cast<uint32_t>(p));
-        const unsigned int at = __shfl_sync(0xffffffffu, next, p);
-        if (reg[u] == static_cast<uint32_t>(p)) out[at + __popc(m & lt)] = k[u];
-        next += lane == p ? __popc(m) : 0u;
-      }
-  }
-}
-
-// Exclusive scan of m counts (one block); out[m] = the total.
-__global__ void __launch_bounds__(1024) scan_counts_kernel(const unsigned int* __restrict__ in, int64_t m,
-                                                           unsigned int* __restrict__ out) {
-  __shared__ unsigned int s_run[1024];
-  const int64_t per = (m + blockDim.x - 1) / blockDim.x;
-  const int64_t lo = threadIdx.x * per, hi = lo + per < m ? lo + per : m;
-  unsigned int mine = 0;
-  for (int64_t i = lo; i < hi; ++i) mine += in[i];
-  s_run[threadIdx.x] = mine;
-  __syncthreads();
-  for (int o = 1; o < 1024; o <<= 1) {
-    const unsigned int y = threadIdx.x >= o ? s_run[threadIdx.x - o] : 0u;
-    __syncthreads();
-    s_run[threadIdx.x] += y;
-    __syncthreads();
-  }
-  unsigned int run = s_run[threadIdx.x] - mine;
-  for (int64_t i = lo; i < hi; ++i) {
-    const unsigned int c = in[i];
-    out[i] = run;
-    run += c;
-  }
-  if (threadIdx.x == blockDim.x - 1) out[m] = s_run[threadIdx.x];
-}
-
 // Inserts region p's rows (tuples [region_begin[p], region_begin[p+1])).
 __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const long long* __restrict__ region_begin,
                                     int p, uint64_t* __restrict__ slots, uint64_t mask,
@@ -690,42 +583,6 @@ static BuildPlan region_plan(const olap_ctx* ctx, int64_t n, int64_t capacity, i
   return bp;
 }
 
-// SUM probe of n keys with the keys grouped by table region first (counts,
-// run starts and the grouped keys in the context's grow-only buffer), then
-// one probe pass over the grouped keys.  The filter is not needed there:
-// every lookup reads the L2-resident region.
-int probe_sum_by_region(olap_ctx* ctx, const uint64_t* table, int64_t capacity, const int32_t* keys, int64_t n,
-                        unsigned long long* d_sum, unsigned long long* d_matches) {
-  RegionPass rp;
-  rp.bp = region_plan(ctx, n, capacity, 4);
-  rp.vec = al16(keys);
-  const int threads = kBuildPartThreads;
-  const int64_t blocks = static_cast<int64_t>(ctx->sm_count) * (2048 / threads);
-  rp.n_warps = static_cast<int32_t>(blocks * (threads / 32));
-  rp.seg = ((n + rp.n_warps - 1) / rp.n_warps + 127) / 128 * 128;
-  const int64_t m = static_cast<int64_t>(rp.bp.n_regions) * rp.n_warps;
-  const size_t cnt_bytes = sizeof(unsigned int) * static_cast<size_t>(m);
-  const size_t start_bytes = sizeof(unsigned int) * static_cast<size_t>(m + 1);
-  const size_t keys_off = (cnt_bytes + start_bytes + 255) & ~size_t(255);
-  char* mem = big_scratch(ctx, keys_off + sizeof(int32_t) * static_cast<size_t>(n));
-  if (!mem) return set_error(ctx, OLAP_ERR_NOMEM, "device memory for the grouped probe keys");
-  auto* hist = reinterpret_cast<unsigned int*>(mem);
-  auto* start = reinterpret_cast<unsigned int*>(mem + cnt_bytes);
-  auto* grouped = reinterpret_cast<int32_t*>(mem + keys_off);
-  region_hist_kernel<<<static_cast<unsigned>(blocks), threads, 0, ctx->stream>>>(rp, keys, hist);
-  scan_counts_kernel<<<1, 1024, 0, ctx->stream>>>(hist, m, start);
-  region_scatter_kernel<<<static_cast<unsigned>(blocks), threads, 0, ctx->stream>>>(rp, keys, start, grouped);
-  Bloom none;
-  none.words = nullptr;
-  none.shift = 32;
-  // keys in region order: the grid walks the grouped keys front to back, so
-  // the table regions are visited one after another
-  hash_probe_sum_kernel<false><<<grid_for(ctx, (n + 3) / 4, 512), 512, 0, ctx->stream>>>(
-      grouped, n, table, rp.bp.mask, none, 1, d_sum, d_matches);
-  OLAP_CUDA_TRY(ctx, cudaGetLastError());
-  return OLAP_OK;
-}
-
 }  // namespace olap
 
 extern "C" {
@@ -849,14 +706,7 @@ int olap_hashjoin_probe_filtered(olap_ctx* ctx, const uint64_t* table, int64_t c
     OLAP_CUDA_TRY(ctx, cudaMemsetAsync(d_sum, 0, sizeof(int64_t), ctx->stream));
     OLAP_CUDA_TRY(ctx, cudaMemsetAsync(m, 0, sizeof(int64_t), ctx->stream));
     auto* ds = reinterpret_cast<unsigned long long*>(d_sum);
-    // Many keys into a table larger than one region: partition the keys by
-    // region first, unless OLAP_TUNE_JOIN_BUILD = 2 asks for whole-table passes.
-    const bool partitioned = capacity > olap::kBuildRegionSlots && capacity <= 32 * olap::kBuildRegionSlots &&
-                             n >= (int64_t(1) << 22) && ctx->tune[olap::TUNE_JOIN_BUILD] != 2;
-    if (n && partitioned) {
-      const int rc = olap::probe_sum_by_region(ctx, table, capacity, keys, n, ds, m);
-      if (rc != OLAP_OK) return rc;
-    } else if (n) {
+    if (n) {
       const dim3 grid(olap::grid_for(ctx, (n + 3) / 4, 512));
       if (filter)
         olap::hash_probe_sum_kernel<true><<<grid, 512, 0, ctx->stream>>>(keys, n, table, mask, bloom,

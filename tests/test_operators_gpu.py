@@ -351,13 +351,11 @@ def test_bounded_device_wait_reports_timeout_and_context_survives(ctx):
 
 
 @pytest.mark.parametrize("bloom", [True, False])
-@pytest.mark.parametrize("mode", [0, 2])
-def test_hash_join_region_probe(ctx, bloom, mode):
-    """SUM probes of at least 2^22 keys into a table larger than one region
-    group their keys by table region first (mode 0, the default) or probe the
-    whole table directly (OLAP_TUNE_JOIN_BUILD = 2); with and without the
-    Bloom filter, aligned and unaligned keys, a ragged count, edge keys: the
-    same (sum, matches) as the oracle."""
+def test_hash_join_probe_large_table(ctx, bloom):
+    """2^22 + 5 build rows (a 2^24-slot, 128 MB table: above one L2-sized
+    region) probed by 2^22 + 1001 keys, with and without the Bloom filter,
+    aligned and unaligned, a ragged count and edge keys: the same (sum,
+    matches) as the oracle."""
     rng = np.random.default_rng(37)
     n = (1 << 22) + 5
     rk = rng.integers(-(1 << 23), 1 << 23, n).astype(np.int32)  # duplicates and negatives
@@ -366,13 +364,9 @@ def test_hash_join_region_probe(ctx, bloom, mode):
     sk[:7] = [np.iinfo(np.int32).min, np.iinfo(np.int32).max, 0, -1, 1, rk[0], rk[-1]]
     ht = ops.HashTable(n, ctx=ctx, bloom=bloom).build(dev(rk), dev(rp))
     assert ht.capacity == 1 << 24
-    ctx.set_tuning(_lib.TUNE_JOIN_BUILD, mode)
-    try:
-        d = dev(sk)
-        assert ht.probe(d) == oracle.hashjoin(rk, rp, sk)
-        assert ht.probe(d[1:]) == oracle.hashjoin(rk, rp, sk[1:])
-    finally:
-        ctx.set_tuning(_lib.TUNE_JOIN_BUILD, 0)
+    d = dev(sk)
+    assert ht.probe(d) == oracle.hashjoin(rk, rp, sk)
+    assert ht.probe(d[1:]) == oracle.hashjoin(rk, rp, sk[1:])
 
 
 @pytest.mark.parametrize("mode", [0, 2])

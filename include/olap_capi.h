@@ -501,11 +501,12 @@ OLAP_API int olap_batch_tune(olap_batch* b, int block, int smem_slots);
 OLAP_API int olap_batch_set_probe(olap_batch* b, int parallel_probe);
 OLAP_API int olap_batch_get_tuning(olap_batch* b, int* block, int* smem_slots, int* parallel_probe);
 /* Times the block sizes {256, 512, 1024} x accumulator slots {0, 2048, 4096,
- * 8192, 16384} on the first sample_rows rows (0 = 64 Mi) of the fact table
- * with these queries (their ranges cut to the sample), keeps the fastest on
- * the handle and returns it (pointers may be NULL).  out/out_slots/totals as
- * for olap_batch_run; their contents afterwards are unspecified.
- * Synchronous. */
+ * 8192, 16384} x both probe orders on the first sample_rows rows (0 = 64 Mi)
+ * of the fact table with these queries (their fact ranges scaled onto the
+ * sample, so it sees the whole table's mix of live queries), keeps the
+ * fastest on the handle and returns it (pointers may be NULL).
+ * out/out_slots/totals as for olap_batch_run; their contents afterwards are
+ * unspecified.  Synchronous. */
 OLAP_API int olap_batch_autotune(olap_batch* b, const olap_batch_query* queries, int n_queries,
                                  const int32_t* const* fk, const int32_t* m1, const int32_t* m2,
                                  int64_t n_rows, int agg, int64_t* out, int64_t out_slots,

@@ -821,11 +821,17 @@ int olap_batch_autotune(olap_batch* b, const olap_batch_query* queries, int n_qu
   olap_ctx* ctx = b->ctx;
   if (sample_rows <= 0) sample_rows = int64_t(64) << 20;
   const int64_t rows = std::min(n_rows, sample_rows);
-  // The queries restricted to the sample's rows [0, rows).
+  // The queries' fact ranges scaled onto the sample's rows [0, rows), so the
+  // sample sees the same mix of live queries per row as the whole table (a
+  // prefix cut would drop the queries whose ranges start past it, and the
+  // shape that wins on fewer queries is not the one that wins on all).
   std::vector<olap_batch_query> qs(queries, queries + n_queries);
+  const double scale = n_rows > rows ? static_cast<double>(rows) / static_cast<double>(n_rows) : 1.0;
   for (auto& q : qs) {
-    q.row_begin = std::min(q.row_begin, rows);
-    q.row_end = std::min(q.row_end, rows);
+    const int64_t lo = std::min<int64_t>(rows, static_cast<int64_t>(static_cast<double>(q.row_begin) * scale));
+    const int64_t hi = std::min<int64_t>(rows, static_cast<int64_t>(static_cast<double>(q.row_end) * scale));
+    q.row_begin = std::max<int64_t>(0, lo);
+    q.row_end = std::max<int64_t>(q.row_begin, hi);
   }
   cudaEvent_t e0, e1;
   {

@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(PAR ? 512 : kBatchMaxThreads, 1) batch_scan_ke
           continue;
         }
         if (qi.y >= 0) {
-          smem_add_u64(&sacc[qi.y + g], static_cast<uint64_t>(v));
+          smem_add_split(reinterpret_cast<uint32_t*>(sacc), p.smem_slots, qi.y + g, static_cast<uint64_t>(v));
         } else {
           const int64_t base = (static_cast<int64_t>(qi.w) << 32) | static_cast<uint32_t>(qi.z);
           atomicAdd(&out[base + g], static_cast<unsigned long long>(v));
@@ -433,7 +433,8 @@ __global__ void __launch_bounds__(PAR ? 512 : kBatchMaxThreads, 1) batch_scan_ke
     const BatchQuery& Q = sq[q];
     if (Q.smem_off < 0) continue;
     for (int64_t g = tid; g < Q.group_nums; g += blockDim.x) {
-      const unsigned long long v = sacc[Q.smem_off + g];
+      const unsigned long long v = smem_split_get(reinterpret_cast<const uint32_t*>(sacc), p.smem_slots,
+                                                  Q.smem_off + g);
       if (v) atomicAdd(&out[Q.out_offset + g], v);
     }
   }

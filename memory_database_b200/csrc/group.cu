@@ -23,7 +23,6 @@
 namespace olap {
 
 constexpr int kGroupThreads = 512;
-constexpr int kSmemSlots = 2048;  // block hash table slots (32 KiB of shared memory)
 constexpr int32_t kEmptyKey = INT32_MIN;
 
 __host__ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
@@ -144,7 +143,7 @@ constexpr int kAggSlots = 8192;  // 16 B per slot: 128 KB of shared memory
 struct SmemAgg {
   int32_t* key;
   unsigned int* cnt;
-  unsigned long long* sum;
+  uint32_t* lo;     // low words of the 64-bit sums; the high words follow at lo + slots
   uint32_t slots;   // a multiple of 4
   uint32_t nb;      // buckets of 4 slots (any count, so a table can fill the shared memory)
 
@@ -154,12 +153,13 @@ struct SmemAgg {
     return ((mix32(static_cast<uint32_t>(k)) & 0xFFFFu) * nb) >> 16;
   }
   __device__ __forceinline__ uint32_t next(uint32_t b) const { return b + 1 == nb ? 0u : b + 1; }
+  __device__ __forceinline__ uint64_t sum(uint32_t i) const { return smem_split_get(lo, slots, i); }
 };
 
 __device__ __forceinline__ SmemAgg smem_agg(unsigned char* base, uint32_t slots) {
   SmemAgg t;
-  t.sum = reinterpret_cast<unsigned long long*>(base);
-  t.key = reinterpret_cast<int32_t*>(t.sum + slots);
+  t.lo = reinterpret_cast<uint32_t*>(base);
+  t.key = reinterpret_cast<int32_t*>(t.lo + 2 * slots);
   t.cnt = reinterpret_cast<unsigned int*>(t.key + slots);
   t.slots = slots;
   t.nb = slots >> 2;
@@ -170,7 +170,8 @@ __device__ __forceinline__ void smem_agg_clear(const SmemAgg& t) {
   for (uint32_t i = threadIdx.x; i < t.slots; i += blockDim.x) {
     t.key[i] = kEmptyKey;
     t.cnt[i] = 0;
-    t.sum[i] = 0;
+    t.lo[i] = 0;
+    t.lo[t.slots + i] = 0;
   }
 }
 
@@ -214,7 +215,7 @@ __device__ __forceinline__ int smem_find_insert(const SmemAgg& t, int32_t k, uin
 __device__ __forceinline__ bool smem_agg_add(const SmemAgg& t, int32_t k, uint64_t s, uint32_t c) {
   const int i = smem_find_insert(t, k, t.home(k));
   if (i < 0) return false;
-  smem_add_u64(t.sum + i, s);
+  smem_add_split(t.lo, t.slots, i, s);
   atomicAdd(t.cnt + i, c);
   return true;
 }
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(kAggThreads) group_hash_smem_kernel(int64_t n,
   if ((threadIdx.x & 31) == 0 && wbad) atomicAdd(range_err, static_cast<unsigned long long>(wbad));
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x)
-    if (st.key[i] != kEmptyKey) global_add(t, st.key[i], st.sum[i], st.cnt[i]);
+    if (st.key[i] != kEmptyKey) global_add(t, st.key[i], st.sum(i), st.cnt[i]);
 }
 
 // ---- batched shared-table updates -------------------------------------------
@@ -374,7 +375,7 @@ __device__ __forceinline__ uint32_t smem_agg_rows(const SmemAgg& t, const int32_
   uint32_t old[R];
 #pragma unroll
   for (int r = 0; r < R; ++r)
-    old[r] = s[r] >= 0 ? atomicAdd(reinterpret_cast<uint32_t*>(t.sum + s[r]), static_cast<uint32_t>(v[r])) : 0u;
+    old[r] = s[r] >= 0 ? atomicAdd(t.lo + s[r], static_cast<uint32_t>(v[r])) : 0u;
 #pragma unroll
   for (int r = 0; r < R; ++r)
     if (s[r] >= 0) atomicAdd(t.cnt + s[r], 1u);
@@ -383,7 +384,7 @@ __device__ __forceinline__ uint32_t smem_agg_rows(const SmemAgg& t, const int32_
     if (s[r] < 0) continue;
     const uint32_t lo = static_cast<uint32_t>(v[r]);
     const uint32_t hi = static_cast<uint32_t>(static_cast<uint64_t>(v[r]) >> 32) + ((old[r] + lo) < old[r] ? 1u : 0u);
-    if (hi) atomicAdd(reinterpret_cast<uint32_t*>(t.sum + s[r]) + 1, hi);
+    if (hi) atomicAdd(t.lo + t.slots + s[r], hi);
   }
   return lost;
 }
@@ -476,7 +477,7 @@ __global__ void __launch_bounds__(kRowsThreads) group_hash_rows_kernel(int64_t n
   if ((threadIdx.x & 31) == 0 && wbad) atomicAdd(range_err, static_cast<unsigned long long>(wbad));
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x)
-    if (t.key[i] != kEmptyKey && t.cnt[i]) global_add(g, t.key[i], t.sum[i], t.cnt[i]);
+    if (t.key[i] != kEmptyKey && t.cnt[i]) global_add(g, t.key[i], t.sum(i), t.cnt[i]);
 }
 
 // Plan 2.  Partition of a key: the top bits of its hash (the shared tables
@@ -826,7 +827,7 @@ __global__ void __launch_bounds__(kAggThreads) group_part_agg_kernel(
       continue;
     }
     out_keys[o] = st.key[i];
-    out_sums[o] = static_cast<int64_t>(st.sum[i]);
+    out_sums[o] = static_cast<int64_t>(st.sum(i));
     if (out_counts) out_counts[o] = static_cast<int64_t>(st.cnt[i]);
   }
 }

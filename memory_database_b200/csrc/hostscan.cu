@@ -114,12 +114,12 @@ __global__ void __launch_bounds__(kHostScanThreads) starjoin_hostscan_kernel(con
     }
     const int64_t v0 = agg_value(p.agg0, x, y);
     tot0 += v0;
-    if (SACC) smem_add_u64(&sacc[g], static_cast<uint64_t>(v0));
+    if (SACC) smem_add_split(reinterpret_cast<uint32_t*>(sacc), nacc, g, static_cast<uint64_t>(v0));
     else atomicAdd(&p.out[g], static_cast<unsigned long long>(v0));
     if (p.n_aggs > 1) {
       const int64_t v1 = agg_value(p.agg1, x, y);
       tot1 += v1;
-      if (SACC) smem_add_u64(&sacc[n_groups + g], static_cast<uint64_t>(v1));
+      if (SACC) smem_add_split(reinterpret_cast<uint32_t*>(sacc), nacc, n_groups + g, static_cast<uint64_t>(v1));
       else atomicAdd(&p.out[n_groups + g], static_cast<unsigned long long>(v1));
     }
   };
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(kHostScanThreads) starjoin_hostscan_kernel(con
   }
   if (SACC) {
     for (int64_t i = tid; i < nacc; i += blockDim.x) {
-      const unsigned long long v = sacc[i];
+      const unsigned long long v = smem_split_get(reinterpret_cast<const uint32_t*>(sacc), nacc, i);
       if (v) atomicAdd(&p.out[i], v);
     }
   }

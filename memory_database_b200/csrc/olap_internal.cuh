@@ -253,6 +253,22 @@ __device__ __forceinline__ void smem_add_u64(unsigned long long* slot, uint64_t 
   if (hi) atomicAdd(w + 1, hi);
 }
 
+
+// The same accumulation with the words in two arrays: slot i's low word at
+// lo[i] and its high word at lo[n + i].  Consecutive slots' low words then
+// sit in consecutive banks, so the random low-word atomics of a warp spread
+// over all 32 banks instead of the 16 even ones of an array of 64-bit slots.
+__device__ __forceinline__ void smem_add_split(uint32_t* lo, int64_t n, int64_t i, uint64_t v) {
+  const uint32_t l = static_cast<uint32_t>(v);
+  uint32_t h = static_cast<uint32_t>(v >> 32);
+  const uint32_t old = atomicAdd(lo + i, l);
+  h += (old + l) < old ? 1u : 0u;
+  if (h) atomicAdd(lo + n + i, h);
+}
+__device__ __forceinline__ uint64_t smem_split_get(const uint32_t* lo, int64_t n, int64_t i) {
+  return (static_cast<uint64_t>(lo[n + i]) << 32) | lo[i];
+}
+
 // ---- bulk asynchronous copies (TMA, untiled) and mbarriers ----------------
 // cp.async.bulk global -> shared: both addresses and the size 16-byte
 // aligned; completion is counted in bytes on an mbarrier of this CTA.  No

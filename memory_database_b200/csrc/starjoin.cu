@@ -203,8 +203,9 @@ __device__ __forceinline__ void finish_block(const StarParams& p, int64_t tot0, 
     }
   }
   if (ACC == ACC_SMEM) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(sacc);
     for (int64_t i = tid; i < nacc; i += blockDim.x) {
-      const unsigned long long v = sacc[i];
+      const unsigned long long v = smem_split_get(w, nacc, i);
       if (v) atomicAdd(&p.out[i], v);
     }
   }
@@ -237,6 +238,7 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
   constexpr int NG = V / 4;
   unsigned char* sdim = smem;
   unsigned long long* sacc = reinterpret_cast<unsigned long long*>(smem + p.smem_dim_bytes);
+  uint32_t* sw = reinterpret_cast<uint32_t*>(sacc);  // accumulator words: low words, then high words
   const int tid = threadIdx.x;
   const int64_t nacc = p.n_groups * p.n_aggs;
   if (tid == 0) red_bad = 0;
@@ -519,11 +521,11 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
         v1 = p.n_aggs > 1 ? agg_value(p.agg1, x, y) : 0;
       }
       tot0 += v0;
-      if (ACC == ACC_SMEM) smem_add_u64(&sacc[gg], static_cast<uint64_t>(v0));
+      if (ACC == ACC_SMEM) smem_add_split(sw, nacc, gg, static_cast<uint64_t>(v0));
       if (ACC == ACC_GLOBAL) atomicAdd(&p.out[gg], static_cast<unsigned long long>(v0));
       if (AGGK == AGGK_M1_M1M2 || (AGGK == AGGK_GENERIC && p.n_aggs > 1)) {
         tot1 += v1;
-        if (ACC == ACC_SMEM) smem_add_u64(&sacc[n_groups + gg], static_cast<uint64_t>(v1));
+        if (ACC == ACC_SMEM) smem_add_split(sw, nacc, n_groups + gg, static_cast<uint64_t>(v1));
         if (ACC == ACC_GLOBAL) atomicAdd(&p.out[n_groups + gg], static_cast<unsigned long long>(v1));
       }
     };
@@ -639,12 +641,12 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
       const int32_t x = p.need_m1 ? p.m1[r] : 0, y = p.need_m2 ? p.m2[r] : 0;
       const int64_t v0 = agg_value(p.agg0, x, y);
       tot0 += v0;
-      if (ACC == ACC_SMEM) smem_add_u64(&sacc[g], static_cast<uint64_t>(v0));
+      if (ACC == ACC_SMEM) smem_add_split(sw, nacc, g, static_cast<uint64_t>(v0));
       if (ACC == ACC_GLOBAL) atomicAdd(&p.out[g], static_cast<unsigned long long>(v0));
       if (p.n_aggs > 1) {
         const int64_t v1 = agg_value(p.agg1, x, y);
         tot1 += v1;
-        if (ACC == ACC_SMEM) smem_add_u64(&sacc[p.n_groups + g], static_cast<uint64_t>(v1));
+        if (ACC == ACC_SMEM) smem_add_split(sw, nacc, p.n_groups + g, static_cast<uint64_t>(v1));
         if (ACC == ACC_GLOBAL) atomicAdd(&p.out[p.n_groups + g], static_cast<unsigned long long>(v1));
       }
     };
@@ -665,6 +667,7 @@ __global__ void __launch_bounds__(1024, 1) starjoin_scalar_kernel(const StarPara
   __shared__ int32_t s_code_nz[OLAP_MAX_DIMS];
   unsigned char* sdim = smem;
   unsigned long long* sacc = reinterpret_cast<unsigned long long*>(smem + p.smem_dim_bytes);
+  uint32_t* sw = reinterpret_cast<uint32_t*>(sacc);  // accumulator words: low words, then high words
   const int tid = threadIdx.x;
   const int64_t nacc = p.n_groups * p.n_aggs;
   if (tid == 0) red_bad = 0;
@@ -724,12 +727,12 @@ __global__ void __launch_bounds__(1024, 1) starjoin_scalar_kernel(const StarPara
     }
     const int64_t v0 = agg_value(p.agg0, x, y);
     tot0 += v0;
-    if (ACC == ACC_SMEM) smem_add_u64(&sacc[g], static_cast<uint64_t>(v0));
+    if (ACC == ACC_SMEM) smem_add_split(sw, nacc, g, static_cast<uint64_t>(v0));
     if (ACC == ACC_GLOBAL) atomicAdd(&p.out[g], static_cast<unsigned long long>(v0));
     if (p.n_aggs > 1) {
       const int64_t v1 = agg_value(p.agg1, x, y);
       tot1 += v1;
-      if (ACC == ACC_SMEM) smem_add_u64(&sacc[p.n_groups + g], static_cast<uint64_t>(v1));
+      if (ACC == ACC_SMEM) smem_add_split(sw, nacc, p.n_groups + g, static_cast<uint64_t>(v1));
       if (ACC == ACC_GLOBAL) atomicAdd(&p.out[p.n_groups + g], static_cast<unsigned long long>(v1));
     }
   }

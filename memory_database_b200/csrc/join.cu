@@ -300,6 +300,18 @@ __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const l
   }
 }
 
+// Half a bucket (two slots) of the hash table, marked evict-last in L2: every
+// probe re-reads the table at random while the probe keys stream past it once,
+// so the part of the table that L2 holds should stay there.  The address is
+// always inside the table (the callers' guards may be moved past this load).
+__device__ __forceinline__ ulonglong2 ld_bucket_half(const uint64_t* p) {
+  ulonglong2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.u64 {%0,%1}, [%2], %3;"
+      : "=l"(v.x), "=l"(v.y)
+      : "l"(p), "l"(policy_evict_last()));
+  return v;
+}
+
 // Probe: SUM of matched payloads and the match count; optionally the matches
 // (probe row, payload) compacted in probe-row order by the caller's second
 // pass (see ProbeOp).
@@ -308,8 +320,8 @@ __device__ __forceinline__ bool hash_lookup_from(const uint64_t* __restrict__ sl
   for (uint64_t step = 0; step <= mask; step += 4) {
     // the 4-slot bucket holding h (one 32-byte sector), starting at h
     const uint64_t b = h & ~3ull;
-    const ulonglong2 lo = __ldg(reinterpret_cast<const ulonglong2*>(slots + b));
-    const ulonglong2 hi = __ldg(reinterpret_cast<const ulonglong2*>(slots + b + 2));
+    const ulonglong2 lo = ld_bucket_half(slots + b);
+    const ulonglong2 hi = ld_bucket_half(slots + b + 2);
     const uint64_t s[4] = {lo.x, lo.y, hi.x, hi.y};
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -346,8 +358,8 @@ __device__ __forceinline__ uint32_t hash_lookup4(const uint64_t* __restrict__ sl
     h[j] = hash32(static_cast<uint32_t>(k[j])) & mask;
     const uint64_t b = h[j] & ~3ull;
     const bool w = (want >> j) & 1u;
-    lo[j] = w ? __ldg(reinterpret_cast<const ulonglong2*>(slots + b)) : none;
-    hi[j] = w ? __ldg(reinterpret_cast<const ulonglong2*>(slots + b + 2)) : none;
+    lo[j] = w ? ld_bucket_half(slots + b) : none;
+    hi[j] = w ? ld_bucket_half(slots + b + 2) : none;
   }
   uint32_t found = 0;
 #pragma unroll

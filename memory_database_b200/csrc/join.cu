@@ -138,13 +138,19 @@ __global__ void hash_build_kernel(const int32_t* __restrict__ keys, int64_t n, u
   }
 }
 
+// Slots [0, cap): (key, row) becomes (key, payload[row]).  The payload reads
+// are random over the whole payload column; marked evict-last in L2, the
+// column (4 bytes per build row) stays there while the table streams past,
+// so each payload sector comes from DRAM about once.
 __global__ void hash_finish_kernel(uint64_t* __restrict__ slots, int64_t cap, const int32_t* __restrict__ payload) {
+  const uint64_t keep = policy_evict_last();
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < cap; i += stride) {
     const uint64_t v = slots[i];
-    if (v == kEmptySlot) continue;
-    const uint32_t row = static_cast<uint32_t>(v);
-    slots[i] = (v & 0xffffffff00000000ull) | static_cast<uint32_t>(payload[row]);
+    const bool full = v != kEmptySlot;
+    const uint32_t row = full ? static_cast<uint32_t>(v) : 0u;  // a valid row whether or not the slot is full
+    const int32_t pay = ld_probe_s32(payload + row, keep);
+    if (full) slots[i] = (v & 0xffffffff00000000ull) | static_cast<uint32_t>(pay);
   }
 }
 
@@ -172,12 +178,24 @@ __device__ __forceinline__ uint32_t build_region(int32_t k, const BuildPlan& bp)
   return static_cast<uint32_t>((hash32(static_cast<uint32_t>(k)) & bp.mask) >> bp.region_shift);
 }
 
-// The histogram and scatter passes run warp-uniform loops and aggregate a
-// warp's rows per region (match_any): one shared atomic per region present in
-// the warp instead of one per row (a table has few regions, so most rows of a
-// warp share theirs).
+// The histogram and scatter passes run warp-uniform loops, 4 rows per lane
+// (16-byte loads when the keys are aligned), and aggregate a warp's rows per
+// region (match_any): one shared atomic per region present in the warp
+// instead of one per row (a table has few regions, so most rows of a warp
+// share theirs).
+__device__ __forceinline__ void build_keys4(const int32_t* __restrict__ keys, int64_t r, int64_t e, bool vec,
+                                            int32_t (&k)[4]) {
+  if (vec && r + 4 <= e) {
+    const int4 v = ld_stream_v4(keys + r, policy_evict_first());
+    k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w;
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) k[u] = r + u < e ? keys[r + u] : INT32_MIN;
+  }
+}
+
 __global__ void __launch_bounds__(kBuildPartThreads) build_hist_kernel(BuildPlan bp, const int32_t* __restrict__ keys,
-                                                                      unsigned int* __restrict__ hist,
+                                                                      int vec, unsigned int* __restrict__ hist,
                                                                       unsigned long long* range_err) {
   extern __shared__ unsigned int s_cnt[];
   for (int p = threadIdx.x; p < bp.n_regions; p += blockDim.x) s_cnt[p] = 0;
@@ -185,15 +203,20 @@ __global__ void __launch_bounds__(kBuildPartThreads) build_hist_kernel(BuildPlan
   const int64_t b = static_cast<int64_t>(blockIdx.x) * bp.per;
   const int64_t e = b + bp.per < bp.n ? b + bp.per : bp.n;
   const int lane = threadIdx.x & 31;
+  const int64_t step = 4 * static_cast<int64_t>(blockDim.x);
   unsigned int bad = 0;
-  for (int64_t r0 = b + (threadIdx.x - lane); r0 < e; r0 += blockDim.x) {
-    const int64_t r = r0 + lane;
-    const int32_t k = r < e ? keys[r] : INT32_MIN;
-    if (r < e && k == INT32_MIN) ++bad;
-    const bool live = k != INT32_MIN;
-    const uint32_t reg = live ? build_region(k, bp) : 0xFFFFFFFFu;
-    const unsigned int m = __match_any_sync(0xffffffffu, reg);
-    if (live && lane == __ffs(m) - 1) atomicAdd(&s_cnt[reg], static_cast<unsigned int>(__popc(m)));
+  for (int64_t r0 = b + 4 * static_cast<int64_t>(threadIdx.x - lane); r0 < e; r0 += step) {
+    const int64_t r = r0 + 4 * lane;
+    int32_t k[4];
+    build_keys4(keys, r, e, vec, k);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool live = k[u] != INT32_MIN;
+      if (r + u < e && !live) ++bad;
+      const uint32_t reg = live ? build_region(k[u], bp) : 0xFFFFFFFFu;
+      const unsigned int m = __match_any_sync(0xffffffffu, reg);
+      if (live && lane == __ffs(m) - 1) atomicAdd(&s_cnt[reg], static_cast<unsigned int>(__popc(m)));
+    }
   }
   if (bad) atomicAdd(range_err, static_cast<unsigned long long>(bad));
   __syncthreads();
@@ -244,7 +267,7 @@ __global__ void __launch_bounds__(1024) build_scan_kernel(BuildPlan bp, const un
 // Shared memory: the block's run starts (P x u64), then its positions taken
 // so far in each run (P x u32).
 __global__ void __launch_bounds__(kBuildPartThreads) build_scatter_kernel(BuildPlan bp,
-                                                                         const int32_t* __restrict__ keys,
+                                                                         const int32_t* __restrict__ keys, int vec,
                                                                          const unsigned long long* __restrict__ offs,
                                                                          uint64_t* __restrict__ tuples) {
   extern __shared__ unsigned long long s_start[];
@@ -257,46 +280,78 @@ __global__ void __launch_bounds__(kBuildPartThreads) build_scatter_kernel(BuildP
   const int64_t b = static_cast<int64_t>(blockIdx.x) * bp.per;
   const int64_t e = b + bp.per < bp.n ? b + bp.per : bp.n;
   const int lane = threadIdx.x & 31;
-  for (int64_t r0 = b + (threadIdx.x - lane); r0 < e; r0 += blockDim.x) {
-    const int64_t r = r0 + lane;
-    const int32_t k = r < e ? keys[r] : INT32_MIN;
-    const bool live = k != INT32_MIN;
-    const uint32_t reg = live ? build_region(k, bp) : 0xFFFFFFFFu;
-    const unsigned int m = __match_any_sync(0xffffffffu, reg);
-    if (live) {
-      const int leader = __ffs(m) - 1;
-      unsigned int at = 0;
-      if (lane == leader) at = atomicAdd(&s_taken[reg], static_cast<unsigned int>(__popc(m)));
-      at = __shfl_sync(m, at, leader) + __popc(m & ((1u << lane) - 1u));
-      tuples[s_start[reg] + at] = (static_cast<uint64_t>(static_cast<uint32_t>(k)) << 32) | static_cast<uint32_t>(r);
+  const int64_t step = 4 * static_cast<int64_t>(blockDim.x);
+  for (int64_t r0 = b + 4 * static_cast<int64_t>(threadIdx.x - lane); r0 < e; r0 += step) {
+    const int64_t r = r0 + 4 * lane;
+    int32_t k[4];
+    build_keys4(keys, r, e, vec, k);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool live = k[u] != INT32_MIN;
+      const uint32_t reg = live ? build_region(k[u], bp) : 0xFFFFFFFFu;
+      const unsigned int m = __match_any_sync(0xffffffffu, reg);
+      if (live) {
+        const int leader = __ffs(m) - 1;
+        unsigned int at = 0;
+        if (lane == leader) at = atomicAdd(&s_taken[reg], static_cast<unsigned int>(__popc(m)));
+        at = __shfl_sync(m, at, leader) + __popc(m & ((1u << lane) - 1u));
+        tuples[s_start[reg] + at] = (static_cast<uint64_t>(static_cast<uint32_t>(k[u])) << 32) |
+                                    static_cast<uint32_t>(r + u);
+      }
     }
   }
 }
 
-// Inserts region p's rows (tuples [region_begin[p], region_begin[p+1])).
+// Inserts `mine` = (key << 32 | row) into the table from slot h on (linear
+// probing); a key already present keeps its largest row.  False when the
+// table has no free slot.
+__device__ __forceinline__ bool insert_from(uint64_t* __restrict__ slots, uint64_t mask, uint64_t h,
+                                            uint64_t mine) {
+  const uint32_t k = static_cast<uint32_t>(mine >> 32);
+  for (uint64_t step = 0; step <= mask; ++step) {
+    unsigned long long* s = reinterpret_cast<unsigned long long*>(slots + h);
+    const unsigned long long prev = atomicCAS(s, kEmptySlot, mine);
+    if (prev == kEmptySlot) return true;
+    if ((prev >> 32) == k) {
+      atomicMax(s, mine);  // same key in the high word: keeps the largest row
+      return true;
+    }
+    h = (h + 1) & mask;
+  }
+  return false;
+}
+
+// Inserts region p's rows (tuples [region_begin[p], region_begin[p+1])), four
+// per thread with their first CAS issued together (the region's slots are in
+// L2, so the inserts are bound by the atomics' round trips, not by DRAM).
 __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const long long* __restrict__ region_begin,
                                     int p, uint64_t* __restrict__ slots, uint64_t mask,
                                     unsigned long long* overflow) {
   const int64_t b = region_begin[p], e = region_begin[p + 1];
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t i = b + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < e; i += stride) {
-    const uint64_t mine = tuples[i];
-    const uint32_t k = static_cast<uint32_t>(mine >> 32);
-    uint64_t h = hash32(k) & mask;
-    bool done = false;
-    for (uint64_t step = 0; step <= mask && !done; ++step) {
-      unsigned long long* s = reinterpret_cast<unsigned long long*>(slots + h);
-      const unsigned long long prev = atomicCAS(s, kEmptySlot, mine);
-      if (prev == kEmptySlot) {
-        done = true;
-      } else if ((prev >> 32) == k) {
-        atomicMax(s, mine);  // same key: keeps the largest row
-        done = true;
-      } else {
-        h = (h + 1) & mask;
+  for (int64_t i = b + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < e; i += 4 * stride) {
+    uint64_t mine[4], h[4];
+    unsigned long long prev[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int64_t t = i + u * stride;
+      mine[u] = t < e ? tuples[t] : 0ull;
+      h[u] = hash32(static_cast<uint32_t>(mine[u] >> 32)) & mask;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      prev[u] = i + u * stride < e ? atomicCAS(reinterpret_cast<unsigned long long*>(slots + h[u]), kEmptySlot,
+                                               static_cast<unsigned long long>(mine[u]))
+                                   : kEmptySlot;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (i + u * stride >= e || prev[u] == kEmptySlot) continue;
+      if ((prev[u] >> 32) == (mine[u] >> 32)) {
+        atomicMax(reinterpret_cast<unsigned long long*>(slots + h[u]), static_cast<unsigned long long>(mine[u]));
+      } else if (!insert_from(slots, mask, (h[u] + 1) & mask, mine[u])) {
+        atomicAdd(overflow, 1ull);
       }
     }
-    if (!done) atomicAdd(overflow, 1ull);
   }
 }
 
@@ -625,7 +680,8 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
   const bool partitioned = capacity > olap::kBuildRegionSlots && n >= (int64_t(1) << 16) &&
                            ctx->tune[olap::TUNE_JOIN_BUILD] != 2;
   if (n && partitioned) {
-    const olap::BuildPlan bp = olap::region_plan(ctx, n, capacity, 1);
+    const olap::BuildPlan bp = olap::region_plan(ctx, n, capacity, 4);
+    const int vec = olap::al16(keys);
     OLAP_REQUIRE(ctx, bp.n_regions <= 2048, "hash table capacity above 2^33 slots");
     const size_t hist_bytes = sizeof(unsigned int) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
     const size_t offs_bytes = sizeof(unsigned long long) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
@@ -640,9 +696,10 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
     const size_t hsm = sizeof(unsigned int) * bp.n_regions;
     const size_t csm = (sizeof(unsigned long long) + sizeof(unsigned int)) * bp.n_regions;
     olap::build_hist_kernel<<<bp.n_blocks, olap::kBuildPartThreads, hsm, ctx->stream>>>(
-        bp, keys, hist, &ctx->counters->range_errors);
+        bp, keys, vec, hist, &ctx->counters->range_errors);
     olap::build_scan_kernel<<<1, 1024, 0, ctx->stream>>>(bp, hist, offs, rbegin);
-    olap::build_scatter_kernel<<<bp.n_blocks, olap::kBuildPartThreads, csm, ctx->stream>>>(bp, keys, offs, tuples);
+    olap::build_scatter_kernel<<<bp.n_blocks, olap::kBuildPartThreads, csm, ctx->stream>>>(bp, keys, vec, offs,
+                                                                                          tuples);
     const unsigned ig = static_cast<unsigned>(ctx->sm_count) * 8;
     for (int p = 0; p < bp.n_regions; ++p)
       olap::build_insert_kernel<<<ig, 256, 0, ctx->stream>>>(tuples, rbegin, p, table, bp.mask, overflow);

@@ -321,9 +321,9 @@ __device__ __forceinline__ bool insert_from(uint64_t* __restrict__ slots, uint64
   return false;
 }
 
-// Inserts region p's rows (tuples [region_begin[p], region_begin[p+1])).
-// The region's slots were brought into L2 just before (region_prefetch), so
-// the CAS round trips stay in L2.
+// Inserts region p's rows (tuples [region_begin[p], region_begin[p+1])): the
+// region's 32 MB of slots are read from DRAM once, and every later CAS on
+// them is an L2 round trip.
 __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const long long* __restrict__ region_begin,
                                     int p, uint64_t* __restrict__ slots, uint64_t mask,
                                     unsigned long long* overflow) {
@@ -333,22 +333,6 @@ __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const l
     const uint64_t mine = tuples[i];
     if (!insert_from(slots, mask, hash32(static_cast<uint32_t>(mine >> 32)) & mask, mine)) atomicAdd(overflow, 1ull);
   }
-}
-
-// Bulk L2 prefetch of `bytes` (a multiple of 16) from a 16-byte aligned
-// address, 64 KB per thread (the copy engine streams it; nothing lands in
-// registers or shared memory).  Marked evict-last, so the region stays while
-// its inserts run.
-__global__ void region_prefetch_kernel(const uint64_t* base, int64_t bytes) {
-  constexpr int64_t kChunk = 64 << 10;
-  const int64_t off = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * kChunk;
-  if (off >= bytes) return;
-  const int64_t len = bytes - off < kChunk ? bytes - off : kChunk;
-  const char* a = reinterpret_cast<const char*>(base) + off;
-  asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;"
-               :
-               : "l"(a), "r"(static_cast<uint32_t>(len)), "l"(policy_evict_last())
-               : "memory");
 }
 
 // Half a bucket (two slots) of the hash table, marked evict-last in L2: every
@@ -697,13 +681,8 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
     olap::build_scatter_kernel<<<bp.n_blocks, olap::kBuildPartThreads, csm, ctx->stream>>>(bp, keys, vec, offs,
                                                                                           tuples);
     const unsigned ig = static_cast<unsigned>(ctx->sm_count) * 8;
-    const int64_t region_bytes = sizeof(uint64_t) << bp.region_shift;
-    const unsigned pg = static_cast<unsigned>((region_bytes / (64 << 10) + 255) / 256);
-    for (int p = 0; p < bp.n_regions; ++p) {
-      olap::region_prefetch_kernel<<<pg, 256, 0, ctx->stream>>>(table + (int64_t(p) << bp.region_shift),
-                                                               region_bytes);
+    for (int p = 0; p < bp.n_regions; ++p)
       olap::build_insert_kernel<<<ig, 256, 0, ctx->stream>>>(tuples, rbegin, p, table, bp.mask, overflow);
-    }
     olap::hash_finish_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, payload);
   } else if (n) {
     olap::hash_build_kernel<<<olap::grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(

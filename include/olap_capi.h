@@ -160,8 +160,10 @@ typedef struct olap_starjoin_query {
 OLAP_API int olap_starjoin_groupsum(olap_ctx* ctx, const olap_starjoin_query* q,
                            int64_t* group_sums, int64_t* totals);
 /* Kernels one olap_starjoin_groupsum call of this query launches with the
- * context's current knobs (the star-join plus one prepass per dimension
- * staged as a pass bitmap or as 4-bit codes); nothing is launched. */
+ * context's current knobs (the star-join, one prepass per dimension staged
+ * as a pass bitmap or as 4-bit codes, and after the 16-byte-aligned kernel
+ * its range pass, which counts the rows with keys out of range when that
+ * kernel met one and returns at once otherwise); nothing is launched. */
 OLAP_API int olap_starjoin_launch_count(olap_ctx* ctx, const olap_starjoin_query* q, int want_groups,
                                         int* kernels);
 

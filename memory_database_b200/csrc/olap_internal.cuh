@@ -24,7 +24,8 @@ struct DeviceCounters {
   unsigned long long range_errors;  // rows dropped: fk or group id out of range
   unsigned long long wait_timeouts;  // bounded device waits that gave up
   unsigned long long host_sectors;   // 32-byte host-memory sectors read in place
-  unsigned long long pad[13];
+  unsigned long long oob_seen;       // star-join: nonzero once a key out of range was met (see range pass)
+  unsigned long long pad[12];
 };
 
 }  // namespace olap

@@ -68,6 +68,7 @@ struct StarParams {
   int32_t cmp_off;             // CMP: per-warp survivor buffers (shared-memory offset)
   int32_t merge_global;        // probe consecutive global int8 dimensions together
   unsigned long long* wait_timeouts;
+  unsigned long long* oob_seen;  // vec kernel: set when a key is out of range (the range pass counts them)
 };
 
 enum { ACC_NONE = 0, ACC_SMEM = 1, ACC_GLOBAL = 2 };
@@ -383,9 +384,10 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
       return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
     };
     // Range check of every key (registers only).  A row with a key out of
-    // range is dropped; it is a range error unless one of its in-range keys
-    // meets DIM_NULL (then a filter drops it anyway), which counts the same
-    // whatever order the dimensions are probed in.  Rare: off the hot path.
+    // range is dropped here and only flagged: whether it is a range error
+    // (none of its in-range keys meets DIM_NULL) is decided by the range pass
+    // that runs after this kernel when the flag is set, so the rare case adds
+    // nothing to this loop's registers.
     uint32_t oob = 0;
 #pragma unroll
     for (int r = 0; r < V; ++r) {
@@ -396,17 +398,7 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
     }
     oob &= alive;
     if (oob) {
-#pragma unroll
-      for (int r = 0; r < V; ++r) {
-        if (!((oob >> r) & 1u)) continue;
-        bool filtered = false;
-#pragma unroll
-        for (int j = 0; j < ND; ++j) {
-          const uint32_t k = key(r, j);
-          if (k < p.dim[j].len && p.dim[j].vec[k] == OLAP_DIM_NULL) filtered = true;
-        }
-        bad += filtered ? 0u : 1u;
-      }
+      *reinterpret_cast<volatile unsigned long long*>(p.oob_seen) = 1ull;
       alive &= ~oob;
       // keys of dropped rows to 0: every key left in registers addresses
       // its vector, so no probe below can leave it, predicated or not
@@ -619,12 +611,8 @@ __global__ void __launch_bounds__(V == 8 ? 512 : 1024, 1) starjoin_vec_kernel(co
         k[j] = static_cast<uint32_t>(p.dim[j].fk[r]);
         ok &= k[j] < p.dim[j].len;
       }
-      if (!ok) {  // a range error unless an in-range key meets DIM_NULL
-        bool filtered = false;
-#pragma unroll
-        for (int j = 0; j < ND; ++j)
-          if (k[j] < p.dim[j].len && p.dim[j].vec[k[j]] == OLAP_DIM_NULL) filtered = true;
-        bad += filtered ? 0u : 1u;
+      if (!ok) {  // dropped and flagged; the range pass decides whether it is a range error
+        *reinterpret_cast<volatile unsigned long long*>(p.oob_seen) = 1ull;
         return;
       }
       int64_t g = 0;
@@ -740,6 +728,45 @@ __global__ void __launch_bounds__(1024, 1) starjoin_scalar_kernel(const StarPara
 }
 
 using StarKernel = void (*)(const StarParams);
+
+// Range pass of the 128-bit kernel.  That kernel drops a row with a key out
+// of range and only sets p.oob_seen; when the flag is set, this pass counts
+// the rows of [row_begin, row_end) with a key out of range and no in-range
+// key meeting DIM_NULL (the rows the plain path counts as range errors).
+// With the flag clear (the normal case) every block returns at once.
+template <int ND>
+__global__ void __launch_bounds__(256) starjoin_range_pass_kernel(const StarParams p) {
+  if (*reinterpret_cast<const volatile unsigned long long*>(p.oob_seen) == 0ull) return;
+  unsigned int bad = 0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t r = p.row_begin + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < p.row_end;
+       r += stride) {
+    uint32_t k[ND > 0 ? ND : 1];
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      k[j] = static_cast<uint32_t>(p.dim[j].fk[r]);
+      ok &= k[j] < p.dim[j].len;
+    }
+    if (ok) continue;
+    bool filtered = false;
+#pragma unroll
+    for (int j = 0; j < ND; ++j)
+      if (k[j] < p.dim[j].len && p.dim[j].vec[k[j]] == OLAP_DIM_NULL) filtered = true;
+    bad += filtered ? 0u : 1u;
+  }
+  const unsigned int wbad = __reduce_add_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0 && wbad) atomicAdd(p.range_err, static_cast<unsigned long long>(wbad));
+}
+
+static StarKernel pick_range_pass(int nd) {
+  switch (nd) {
+    case 1: return starjoin_range_pass_kernel<1>;
+    case 2: return starjoin_range_pass_kernel<2>;
+    case 3: return starjoin_range_pass_kernel<3>;
+    default: return starjoin_range_pass_kernel<4>;
+  }
+}
 
 template <int ND, int ACC, bool ASYNC>
 static StarKernel pick_vec_a(int aggk, int v) {
@@ -1015,6 +1042,7 @@ int plan_starjoin(olap_ctx* ctx, const olap_starjoin_query* q, int64_t* group_su
   // Bulk-copy prefetch: per warp, 32 vectors of each streamed column for each
   // group of 4 rows per thread, and one mbarrier; only when it fits.
   sp->wait_timeouts = &ctx->counters->wait_timeouts;
+  sp->oob_seen = &ctx->counters->oob_seen;
   sp->merge_global = tune_or(ctx, TUNE_MERGE_PROBES, 2) == 1 ? 1 : 0;
   pl->async = false;
   if (vec && tune_or(ctx, TUNE_ASYNC_LOADS, 1) == 2 && nd + (need_m1 ? 1 : 0) + (need_m2 ? 1 : 0) > 0) {
@@ -1080,8 +1108,14 @@ int launch_starjoin(olap_ctx* ctx, StarPlan& pl, cudaStream_t stream) {
   int64_t grid = static_cast<int64_t>(ctx->sm_count) * bps;
   grid = std::min<int64_t>(grid, (work_items + pl.block - 1) / pl.block);
   grid = std::max<int64_t>(grid, 1);
+  const bool range_pass = pl.vec && pl.nd >= 1;
+  if (range_pass) OLAP_CUDA_TRY(ctx, cudaMemsetAsync(sp.oob_seen, 0, sizeof(unsigned long long), stream));
   k<<<static_cast<unsigned>(grid), pl.block, pl.smem, stream>>>(sp);
   OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  if (range_pass) {
+    pick_range_pass(pl.nd)<<<static_cast<unsigned>(ctx->sm_count) * 8, 256, 0, stream>>>(sp);
+    OLAP_CUDA_TRY(ctx, cudaGetLastError());
+  }
   return OLAP_OK;
 }
 
@@ -1347,7 +1381,8 @@ int olap_starjoin_launch_count(olap_ctx* ctx, const olap_starjoin_query* q, int 
   int64_t probe = 0;  // only its address: the plan records the output pointers
   const int st = olap::plan_starjoin(ctx, q, want_groups ? &probe : nullptr, &probe, ar, &pl);
   if (st != OLAP_OK) return st;
-  *kernels = q->row_end > q->row_begin ? 1 + pl.nbits + pl.nnib : 0;
+  // the star-join, its prepasses, and the range pass after the 128-bit kernel
+  *kernels = q->row_end > q->row_begin ? 1 + pl.nbits + pl.nnib + (pl.vec && pl.nd >= 1 ? 1 : 0) : 0;
   return OLAP_OK;
 }
 

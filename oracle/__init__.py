@@ -402,6 +402,21 @@ def vector_group(idx, m1, m2, G, want_counts=True):
     return tot, gv, cnt, err.value
 
 
+def hash_group(keys, vals, vals2=None):
+    """Per-key (keys ascending, int64 SUM of vals + vals2, COUNT) of a hash
+    group-by: ``hashtable_group`` (code/group/test_group_option.cpp:71-88)
+    adds m1[i] + m2[i] into ``group_hashtable[vecInx[i] - 1]``; this keeps
+    every key's exact int64 sum and its row count, which the reference's
+    32-bit map values and its returned total over keys 0..size-1 are checked
+    against (tests/test_oracle_ops.py)."""
+    keys = np.ascontiguousarray(keys, np.int32)
+    v = np.asarray(vals, np.int64) + (np.asarray(vals2, np.int64) if vals2 is not None else 0)
+    uk, inv = np.unique(keys, return_inverse=True)
+    sums = np.zeros(len(uk), np.int64)
+    np.add.at(sums, inv, v)
+    return uk, sums, np.bincount(inv, minlength=len(uk)).astype(np.int64)
+
+
 def agg_fixed(price, qty, tax):
     p, q, t = _c32(price), _c32(qty), _c32(tax)
     return oracle_lib().oracle_agg_fixed(len(p), _p(p), _p(q), _p(t))

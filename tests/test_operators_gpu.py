@@ -290,11 +290,7 @@ def test_starjoin_operator(ctx):
 
 
 def _group_expect(keys, vals, vals2):
-    v = vals.astype(np.int64) + (vals2.astype(np.int64) if vals2 is not None else 0)
-    uk, inv = np.unique(keys, return_inverse=True)
-    sums = np.zeros(len(uk), np.int64)
-    np.add.at(sums, inv, v)
-    return uk, sums, np.bincount(inv, minlength=len(uk))
+    return oracle.hash_group(keys, vals, vals2)
 
 
 @pytest.mark.parametrize("dist,G,n,two", [

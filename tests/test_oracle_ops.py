@@ -76,6 +76,10 @@ def test_group_matches_reference():
         assert err == 0 and tot == t_ref and np.array_equal(gv.astype(np.int32), gv_ref)
         assert cnt.sum() == n
         assert ref.ref_hashtable_group(n, oracle._p(idx), oracle._p(m1), oracle._p(m2)) == tot
+        # the per-key hash group-by restatement: keys vecInx - 1, int32 map values
+        uk, sums, cnts = oracle.hash_group(idx - 1, m1, m2)
+        assert np.array_equal(uk, np.arange(G)) and sums.sum() == t_ref and cnts.sum() == n
+        assert np.array_equal(sums.astype(np.int32), gv_ref)
 
 
 def test_aggregation_matches_reference():

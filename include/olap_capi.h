@@ -349,9 +349,10 @@ OLAP_API int olap_gather_i32(olap_ctx* ctx, const int32_t* rowids, int64_t k, in
                              const int32_t* const* cols, int64_t col_len, int32_t* const* outs);
 
 /* ---- joins (code/join) -------------------------------------------------------
- * Hash table: capacity 64-bit slots (a power of two > n; use
- * olap_hashtable_capacity(n), which keeps the load <= 1/2), 16-byte aligned,
- * caller-allocated.  A duplicate build key keeps the payload of its last
+ * Hash table: capacity 64-bit slots (a multiple of 8 in (n, 2^32]; use
+ * olap_hashtable_capacity(n), about 4n/3 slots: load <= 3/4), 16-byte
+ * aligned, caller-allocated.  A key's home slot is its hash scaled onto the
+ * capacity (linear probing from there).  A duplicate build key keeps the payload of its last
  * row, as the reference's sequential build does.  Key INT32_MIN marks empty
  * slots and cannot be built (counted as a range error). */
 OLAP_API int64_t olap_hashtable_capacity(int64_t n_build);

@@ -31,6 +31,16 @@ __host__ __device__ __forceinline__ uint32_t hash32(uint32_t x) {  // murmur3 fi
   return x;
 }
 
+// Home slot of key k in a table of `cap` slots: the hash scaled onto
+// [0, cap) by a multiply and shift, so the capacity need not be a power of
+// two (the table is sized at 4/3 of the build rows: at a 3/4 load the
+// table of 2^24 keys is 179 MB instead of 256 MB, and more of it stays in
+// L2).  Linear probing moves forward and wraps at the end.
+__host__ __device__ __forceinline__ uint64_t home_slot(uint32_t k, uint64_t cap) {
+  return (static_cast<uint64_t>(hash32(k)) * cap) >> 32;
+}
+__host__ __device__ __forceinline__ uint64_t next_slot(uint64_t h, uint64_t cap) { return h + 1 == cap ? 0 : h + 1; }
+
 // Blocked Bloom filter of the build keys (a format of this library, built
 // beside the table): 2^w 64-bit words, about 8 bits per build key; a key sets
 // four bits of one word (the word from the top bits of hash32, the bits from
@@ -111,7 +121,7 @@ __global__ void fill_u64_kernel(uint64_t* p, int64_t n, uint64_t v) {
 }
 
 __global__ void hash_build_kernel(const int32_t* __restrict__ keys, int64_t n, uint64_t* __restrict__ slots,
-                                  uint64_t mask, unsigned long long* range_err, unsigned long long* overflow) {
+                                  uint64_t cap, unsigned long long* range_err, unsigned long long* overflow) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
     const int32_t k = keys[r];
@@ -120,9 +130,9 @@ __global__ void hash_build_kernel(const int32_t* __restrict__ keys, int64_t n, u
       continue;
     }
     const uint64_t mine = (static_cast<uint64_t>(static_cast<uint32_t>(k)) << 32) | static_cast<uint32_t>(r);
-    uint64_t h = hash32(static_cast<uint32_t>(k)) & mask;
+    uint64_t h = home_slot(static_cast<uint32_t>(k), cap);
     bool done = false;
-    for (uint64_t step = 0; step <= mask && !done; ++step) {
+    for (uint64_t step = 0; step < cap && !done; ++step) {
       unsigned long long* s = reinterpret_cast<unsigned long long*>(slots + h);
       const unsigned long long prev = atomicCAS(s, kEmptySlot, mine);
       if (prev == kEmptySlot) {
@@ -131,7 +141,7 @@ __global__ void hash_build_kernel(const int32_t* __restrict__ keys, int64_t n, u
         atomicMax(s, mine);  // same key in the high word: keeps the largest row
         done = true;
       } else {
-        h = (h + 1) & mask;
+        h = next_slot(h, cap);
       }
     }
     if (!done) atomicAdd(overflow, 1ull);
@@ -169,13 +179,13 @@ struct BuildPlan {
   int64_t n;
   int64_t per;         // rows per block of the histogram and scatter passes
   int32_t n_blocks;
-  int32_t n_regions;   // P, a power of two
+  int32_t n_regions;   // P = ceil(capacity / kBuildRegionSlots)
   int32_t region_shift;
-  uint64_t mask;       // capacity - 1
+  uint64_t cap;        // table slots
 };
 
 __device__ __forceinline__ uint32_t build_region(int32_t k, const BuildPlan& bp) {
-  return static_cast<uint32_t>((hash32(static_cast<uint32_t>(k)) & bp.mask) >> bp.region_shift);
+  return static_cast<uint32_t>(home_slot(static_cast<uint32_t>(k), bp.cap) >> bp.region_shift);
 }
 
 // The histogram and scatter passes run warp-uniform loops, 4 rows per lane
@@ -305,10 +315,10 @@ __global__ void __launch_bounds__(kBuildPartThreads) build_scatter_kernel(BuildP
 // Inserts `mine` = (key << 32 | row) into the table from slot h on (linear
 // probing); a key already present keeps its largest row.  False when the
 // table has no free slot.
-__device__ __forceinline__ bool insert_from(uint64_t* __restrict__ slots, uint64_t mask, uint64_t h,
+__device__ __forceinline__ bool insert_from(uint64_t* __restrict__ slots, uint64_t cap, uint64_t h,
                                             uint64_t mine) {
   const uint32_t k = static_cast<uint32_t>(mine >> 32);
-  for (uint64_t step = 0; step <= mask; ++step) {
+  for (uint64_t step = 0; step < cap; ++step) {
     unsigned long long* s = reinterpret_cast<unsigned long long*>(slots + h);
     const unsigned long long prev = atomicCAS(s, kEmptySlot, mine);
     if (prev == kEmptySlot) return true;
@@ -316,7 +326,7 @@ __device__ __forceinline__ bool insert_from(uint64_t* __restrict__ slots, uint64
       atomicMax(s, mine);  // same key in the high word: keeps the largest row
       return true;
     }
-    h = (h + 1) & mask;
+    h = next_slot(h, cap);
   }
   return false;
 }
@@ -325,13 +335,13 @@ __device__ __forceinline__ bool insert_from(uint64_t* __restrict__ slots, uint64
 // region's 32 MB of slots are read from DRAM once, and every later CAS on
 // them is an L2 round trip.
 __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const long long* __restrict__ region_begin,
-                                    int p, uint64_t* __restrict__ slots, uint64_t mask,
+                                    int p, uint64_t* __restrict__ slots, uint64_t cap,
                                     unsigned long long* overflow) {
   const int64_t b = region_begin[p], e = region_begin[p + 1];
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = b + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < e; i += stride) {
     const uint64_t mine = tuples[i];
-    if (!insert_from(slots, mask, hash32(static_cast<uint32_t>(mine >> 32)) & mask, mine)) atomicAdd(overflow, 1ull);
+    if (!insert_from(slots, cap, home_slot(static_cast<uint32_t>(mine >> 32), cap), mine)) atomicAdd(overflow, 1ull);
   }
 }
 
@@ -350,9 +360,9 @@ __device__ __forceinline__ ulonglong2 ld_bucket_half(const uint64_t* p) {
 // Probe: SUM of matched payloads and the match count; optionally the matches
 // (probe row, payload) compacted in probe-row order by the caller's second
 // pass (see ProbeOp).
-__device__ __forceinline__ bool hash_lookup_from(const uint64_t* __restrict__ slots, uint64_t mask, uint64_t h,
+__device__ __forceinline__ bool hash_lookup_from(const uint64_t* __restrict__ slots, uint64_t cap, uint64_t h,
                                                  uint32_t uk, int32_t* payload) {
-  for (uint64_t step = 0; step <= mask; step += 4) {
+  for (uint64_t step = 0; step < cap; step += 4) {
     // the 4-slot bucket holding h (one 32-byte sector), starting at h
     const uint64_t b = h & ~3ull;
     const ulonglong2 lo = ld_bucket_half(slots + b);
@@ -367,14 +377,14 @@ __device__ __forceinline__ bool hash_lookup_from(const uint64_t* __restrict__ sl
         return true;
       }
     }
-    h = (b + 4) & mask;
+    h = b + 4 == cap ? 0 : b + 4;
   }
   return false;
 }
 
-__device__ __forceinline__ bool hash_lookup(const uint64_t* __restrict__ slots, uint64_t mask, int32_t k,
+__device__ __forceinline__ bool hash_lookup(const uint64_t* __restrict__ slots, uint64_t cap, int32_t k,
                                             int32_t* payload) {
-  return hash_lookup_from(slots, mask, hash32(static_cast<uint32_t>(k)) & mask, static_cast<uint32_t>(k), payload);
+  return hash_lookup_from(slots, cap, home_slot(static_cast<uint32_t>(k), cap), static_cast<uint32_t>(k), payload);
 }
 
 // Four lookups with their first buckets read together (8 x 16-byte loads in
@@ -382,7 +392,7 @@ __device__ __forceinline__ bool hash_lookup(const uint64_t* __restrict__ slots, 
 // bucket (rare at load <= 1/2) falls back to hash_lookup from the next one.
 // Returns the 4-bit mask of matches; pay[j] holds the matched payloads.
 // Only the keys in `want` are looked up (the others count as absent).
-__device__ __forceinline__ uint32_t hash_lookup4(const uint64_t* __restrict__ slots, uint64_t mask, const int4 k4,
+__device__ __forceinline__ uint32_t hash_lookup4(const uint64_t* __restrict__ slots, uint64_t cap, const int4 k4,
                                                  int32_t pay[4], uint32_t want = 0xFu) {
   const int32_t k[4] = {k4.x, k4.y, k4.z, k4.w};
   uint64_t h[4];
@@ -390,7 +400,7 @@ __device__ __forceinline__ uint32_t hash_lookup4(const uint64_t* __restrict__ sl
   const ulonglong2 none = make_ulonglong2(kEmptySlot, kEmptySlot);
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    h[j] = hash32(static_cast<uint32_t>(k[j])) & mask;
+    h[j] = home_slot(static_cast<uint32_t>(k[j]), cap);
     const uint64_t b = h[j] & ~3ull;
     const bool w = (want >> j) & 1u;
     lo[j] = w ? ld_bucket_half(slots + b) : none;
@@ -415,10 +425,11 @@ __device__ __forceinline__ uint32_t hash_lookup4(const uint64_t* __restrict__ sl
     }
     if (state == 0) {
       int32_t p = 0;
-      const uint64_t next = ((h[j] & ~3ull) + 4) & mask;
+      const uint64_t b4 = (h[j] & ~3ull) + 4;
+      const uint64_t next = b4 == cap ? 0 : b4;
       // continue the run from the next bucket: a key whose home slot is
       // `next` has the same probe sequence from there on
-      if (hash_lookup_from(slots, mask, next, uk, &p)) {
+      if (hash_lookup_from(slots, cap, next, uk, &p)) {
         pay[j] = p;
         state = 1;
       }
@@ -430,7 +441,7 @@ __device__ __forceinline__ uint32_t hash_lookup4(const uint64_t* __restrict__ sl
 
 template <bool kFilter>
 __global__ void __launch_bounds__(512, 2) hash_probe_sum_kernel(const int32_t* __restrict__ keys, int64_t n,
-                                                                const uint64_t* __restrict__ slots, uint64_t mask,
+                                                                const uint64_t* __restrict__ slots, uint64_t cap,
                                                                 Bloom filter, int vec, unsigned long long* sum,
                                                                 unsigned long long* matches) {
   __shared__ long long s_red[16][2];
@@ -443,13 +454,13 @@ __global__ void __launch_bounds__(512, 2) hash_probe_sum_kernel(const int32_t* _
   for (int64_t i = tid; i < n4; i += stride) {
     const int4 k = ld_stream_v4(keys + 4 * i, pol);
     int32_t p[4];
-    const uint32_t f = hash_lookup4(slots, mask, k, p, bloom_pass4<kFilter>(filter, k, keep));
+    const uint32_t f = hash_lookup4(slots, cap, k, p, bloom_pass4<kFilter>(filter, k, keep));
     s += static_cast<int64_t>(p[0]) + p[1] + static_cast<int64_t>(p[2]) + p[3];  // 0 where absent
     c += __popc(f);
   }
   for (int64_t r = 4 * n4 + tid; r < n; r += stride) {
     int32_t p = 0;
-    if (bloom_pass<kFilter>(filter, keys[r]) && hash_lookup(slots, mask, keys[r], &p)) {
+    if (bloom_pass<kFilter>(filter, keys[r]) && hash_lookup(slots, cap, keys[r], &p)) {
       s += p;
       ++c;
     }
@@ -480,7 +491,7 @@ struct ProbeOp {
   static constexpr int kGroups = kCompactGroups;
   const int32_t* keys;
   const uint64_t* slots;
-  uint64_t mask;
+  uint64_t cap;
   Bloom filter;
   int32_t* out_rows;
   int32_t* out_payload;
@@ -506,11 +517,11 @@ struct ProbeOp {
     uint32_t m = 0;
     if (nv == 4) {
       const int4 k4 = make_int4(k[0], k[1], k[2], k[3]);
-      m = hash_lookup4(slots, mask, k4, p, bloom_pass4<kFilter>(filter, k4, policy_evict_last()));
+      m = hash_lookup4(slots, cap, k4, p, bloom_pass4<kFilter>(filter, k4, policy_evict_last()));
     } else {
 #pragma unroll
       for (int j = 0; j < 4; ++j)
-        if (j < nv && bloom_pass<kFilter>(filter, k[j]) && hash_lookup(slots, mask, k[j], &p[j])) m |= 1u << j;
+        if (j < nv && bloom_pass<kFilter>(filter, k[j]) && hash_lookup(slots, cap, k[j], &p[j])) m |= 1u << j;
     }
     pay[u] = make_int4(p[0], p[1], p[2], p[3]);
     return m;
@@ -587,14 +598,14 @@ static bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) =
 
 // Matched pairs of n probe keys through the order-preserving compaction.
 template <bool kFilter>
-int probe_pairs(olap_ctx* ctx, Arena& ar, const uint64_t* table, uint64_t mask, const Bloom& bloom,
+int probe_pairs(olap_ctx* ctx, Arena& ar, const uint64_t* table, uint64_t cap, const Bloom& bloom,
                 const int32_t* keys, int64_t n, unsigned long long* total, int32_t* out_rows,
                 int32_t* out_payload) {
   ProbeOp<kFilter> op;
   std::memset(&op, 0, sizeof(op));
   op.keys = keys;
   op.slots = table;
-  op.mask = mask;
+  op.cap = cap;
   op.filter = bloom;
   op.out_rows = out_rows;
   op.out_payload = out_payload;
@@ -618,13 +629,11 @@ static unsigned grid_for(const olap_ctx* ctx, int64_t items, int threads) {
 static BuildPlan region_plan(const olap_ctx* ctx, int64_t n, int64_t capacity, int64_t align) {
   BuildPlan bp;
   bp.n = n;
-  bp.mask = static_cast<uint64_t>(capacity - 1);
-  bp.n_regions = static_cast<int32_t>(capacity / kBuildRegionSlots);
-  int lg_cap = 0;
-  while ((int64_t(1) << lg_cap) < capacity) ++lg_cap;
-  int lg_p = 0;
-  while ((1 << lg_p) < bp.n_regions) ++lg_p;
-  bp.region_shift = lg_cap - lg_p;
+  bp.cap = static_cast<uint64_t>(capacity);
+  bp.n_regions = static_cast<int32_t>((capacity + kBuildRegionSlots - 1) / kBuildRegionSlots);
+  int lg_r = 0;
+  while ((int64_t(1) << lg_r) < kBuildRegionSlots) ++lg_r;
+  bp.region_shift = lg_r;
   bp.n_blocks = ctx->sm_count * 2;
   bp.per = ((n + bp.n_blocks - 1) / bp.n_blocks + align - 1) / align * align;
   return bp;
@@ -635,9 +644,9 @@ static BuildPlan region_plan(const olap_ctx* ctx, int64_t n, int64_t capacity, i
 extern "C" {
 
 int64_t olap_hashtable_capacity(int64_t n_build) {
-  int64_t cap = 8;
-  while (cap < 2 * n_build) cap <<= 1;
-  return cap;
+  if (n_build < 0) n_build = 0;
+  const int64_t cap = (n_build + n_build / 3 + 8) & ~int64_t(7);  // load <= 3/4, a multiple of 8
+  return cap < 8 ? 8 : cap;
 }
 
 int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* payload, int64_t n,
@@ -646,8 +655,8 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
   std::lock_guard<std::mutex> lk(ctx->mu);
   OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   OLAP_REQUIRE(ctx, n >= 0 && n <= UINT32_MAX - 1, "n must be in [0, 2^32-1)");
-  OLAP_REQUIRE(ctx, capacity >= 8 && (capacity & (capacity - 1)) == 0 && capacity > n,
-               "capacity must be a power of two larger than n (see olap_hashtable_capacity)");
+  OLAP_REQUIRE(ctx, capacity >= 8 && capacity % 8 == 0 && capacity <= (int64_t(1) << 32) && capacity > n,
+               "capacity must be a multiple of 8 in (n, 2^32] (see olap_hashtable_capacity)");
   OLAP_REQUIRE(ctx, table && (olap::al16(table)), "table must be 16-byte aligned");
   OLAP_REQUIRE(ctx, n == 0 || (keys && payload), "null keys or payload");
   olap::Arena ar(ctx);
@@ -662,7 +671,7 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
   if (n && partitioned) {
     const olap::BuildPlan bp = olap::region_plan(ctx, n, capacity, 4);
     const int vec = olap::al16(keys);
-    OLAP_REQUIRE(ctx, bp.n_regions <= 2048, "hash table capacity above 2^33 slots");
+    OLAP_REQUIRE(ctx, bp.n_regions <= 2048, "hash table capacity above 2^33 slots");  // never: cap <= 2^32
     const size_t hist_bytes = sizeof(unsigned int) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
     const size_t offs_bytes = sizeof(unsigned long long) * static_cast<size_t>(bp.n_blocks) * bp.n_regions;
     const size_t begin_bytes = sizeof(long long) * (bp.n_regions + 1);
@@ -682,11 +691,11 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
                                                                                           tuples);
     const unsigned ig = static_cast<unsigned>(ctx->sm_count) * 8;
     for (int p = 0; p < bp.n_regions; ++p)
-      olap::build_insert_kernel<<<ig, 256, 0, ctx->stream>>>(tuples, rbegin, p, table, bp.mask, overflow);
+      olap::build_insert_kernel<<<ig, 256, 0, ctx->stream>>>(tuples, rbegin, p, table, bp.cap, overflow);
     olap::hash_finish_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, payload);
   } else if (n) {
     olap::hash_build_kernel<<<olap::grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(
-        keys, n, table, static_cast<uint64_t>(capacity - 1), &ctx->counters->range_errors, overflow);
+        keys, n, table, static_cast<uint64_t>(capacity), &ctx->counters->range_errors, overflow);
     olap::hash_finish_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, payload);
   }
   OLAP_CUDA_TRY(ctx, cudaGetLastError());
@@ -733,7 +742,7 @@ int olap_hashjoin_probe_filtered(olap_ctx* ctx, const uint64_t* table, int64_t c
   std::lock_guard<std::mutex> lk(ctx->mu);
   OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   OLAP_REQUIRE(ctx, n >= 0 && n <= INT32_MAX, "n must be in [0, 2^31)");
-  OLAP_REQUIRE(ctx, capacity >= 8 && (capacity & (capacity - 1)) == 0 && table, "bad table");
+  OLAP_REQUIRE(ctx, capacity >= 8 && capacity % 8 == 0 && capacity <= (int64_t(1) << 32) && table, "bad table");
   OLAP_REQUIRE(ctx, n == 0 || keys, "null keys");
   OLAP_REQUIRE(ctx, d_sum || (out_rows && out_payload), "nothing to compute");
   OLAP_REQUIRE(ctx, !filter || (words >= 1 && words <= (int64_t(1) << 31) && (words & (words - 1)) == 0),
@@ -747,7 +756,7 @@ int olap_hashjoin_probe_filtered(olap_ctx* ctx, const uint64_t* table, int64_t c
     bloom.shift = 32 - lg;
   }
   olap::Arena ar(ctx);
-  const uint64_t mask = static_cast<uint64_t>(capacity - 1);
+  const uint64_t cap = static_cast<uint64_t>(capacity);
   if (d_sum) {
     unsigned long long* m = d_matches ? reinterpret_cast<unsigned long long*>(d_matches)
                                       : ar.take<unsigned long long>(1);
@@ -758,10 +767,10 @@ int olap_hashjoin_probe_filtered(olap_ctx* ctx, const uint64_t* table, int64_t c
     if (n) {
       const dim3 grid(olap::grid_for(ctx, (n + 3) / 4, 512));
       if (filter)
-        olap::hash_probe_sum_kernel<true><<<grid, 512, 0, ctx->stream>>>(keys, n, table, mask, bloom,
+        olap::hash_probe_sum_kernel<true><<<grid, 512, 0, ctx->stream>>>(keys, n, table, cap, bloom,
                                                                         olap::al16(keys), ds, m);
       else
-        olap::hash_probe_sum_kernel<false><<<grid, 512, 0, ctx->stream>>>(keys, n, table, mask, bloom,
+        olap::hash_probe_sum_kernel<false><<<grid, 512, 0, ctx->stream>>>(keys, n, table, cap, bloom,
                                                                          olap::al16(keys), ds, m);
     }
     OLAP_CUDA_TRY(ctx, cudaGetLastError());
@@ -770,8 +779,8 @@ int olap_hashjoin_probe_filtered(olap_ctx* ctx, const uint64_t* table, int64_t c
     unsigned long long* total = (!d_sum && d_matches) ? reinterpret_cast<unsigned long long*>(d_matches)
                                                       : ar.take<unsigned long long>(1);
     if (!total) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
-    const int rc = filter ? olap::probe_pairs<true>(ctx, ar, table, mask, bloom, keys, n, total, out_rows, out_payload)
-                          : olap::probe_pairs<false>(ctx, ar, table, mask, bloom, keys, n, total, out_rows,
+    const int rc = filter ? olap::probe_pairs<true>(ctx, ar, table, cap, bloom, keys, n, total, out_rows, out_payload)
+                          : olap::probe_pairs<false>(ctx, ar, table, cap, bloom, keys, n, total, out_rows,
                                                      out_payload);
     if (rc != OLAP_OK) return rc;
   }

@@ -346,9 +346,40 @@ def test_bounded_device_wait_reports_timeout_and_context_survives(ctx):
     assert np.array_equal(host(ops.select_rowids(dev(col), 99, ctx=ctx)), np.arange(100, dtype=np.int32))
 
 
+@pytest.mark.parametrize("cap,n", [(8, 7), (64, 63), (1000, 999), (200_008, 150_000)])
+def test_hash_join_any_capacity(ctx, cap, n):
+    """Tables of any capacity that is a multiple of 8 above the build rows:
+    nearly full ones (probe runs that wrap past the last slot) and a 3/4-full
+    one; sums, matches and pairs equal the oracle's.  Capacities that are
+    not multiples of 8, or not above n, are rejected."""
+    rng = np.random.default_rng(cap)
+    rk = rng.permutation(np.arange(-n // 2, n - n // 2)).astype(np.int32)
+    rp = rng.integers(-1000, 1000, n).astype(np.int32)
+    sk = rng.integers(-n, n, 4 * n + 3).astype(np.int32)
+    L, h = _lib.lib, ctx.handle
+    table = torch.empty(cap, dtype=torch.int64, device="cuda")
+    _lib.check(L.olap_hashjoin_build(h, dev(rk).data_ptr(), dev(rp).data_ptr(), n, table.data_ptr(), cap), h)
+    s_, m_ = torch.zeros(1, dtype=torch.int64, device="cuda"), torch.zeros(1, dtype=torch.int64, device="cuda")
+    dk = dev(sk)
+    _lib.check(L.olap_hashjoin_probe_filtered(h, table.data_ptr(), cap, None, 0, dk.data_ptr(), len(sk),
+                                              s_.data_ptr(), m_.data_ptr(), None, None), h)
+    es, em = oracle.hashjoin(rk, rp, sk)
+    assert (int(s_.item()), int(m_.item())) == (es, em)
+    rows = torch.empty(len(sk), dtype=torch.int32, device="cuda")
+    pay = torch.empty(len(sk), dtype=torch.int32, device="cuda")
+    _lib.check(L.olap_hashjoin_probe_filtered(h, table.data_ptr(), cap, None, 0, dk.data_ptr(), len(sk), None,
+                                              m_.data_ptr(), rows.data_ptr(), pay.data_ptr()), h)
+    k = int(m_.item())
+    _, _, erows, epay = oracle.hashjoin(rk, rp, sk, want_pairs=True)
+    assert np.array_equal(host(rows[:k]), erows) and np.array_equal(host(pay[:k]), epay)
+    for bad in (cap + 4, n):
+        with pytest.raises(_lib.OlapError):
+            _lib.check(L.olap_hashjoin_build(h, dev(rk).data_ptr(), dev(rp).data_ptr(), n, table.data_ptr(), bad), h)
+
+
 @pytest.mark.parametrize("bloom", [True, False])
 def test_hash_join_probe_large_table(ctx, bloom):
-    """2^22 + 5 build rows (a 2^24-slot, 128 MB table: above one L2-sized
+    """2^22 + 5 build rows (a table of about 5.6M slots, 45 MB: above one L2-sized
     region) probed by 2^22 + 1001 keys, with and without the Bloom filter,
     aligned and unaligned, a ragged count and edge keys: the same (sum,
     matches) as the oracle."""
@@ -359,7 +390,7 @@ def test_hash_join_probe_large_table(ctx, bloom):
     sk = rng.integers(-(1 << 23), 1 << 23, (1 << 22) + 1001).astype(np.int32)
     sk[:7] = [np.iinfo(np.int32).min, np.iinfo(np.int32).max, 0, -1, 1, rk[0], rk[-1]]
     ht = ops.HashTable(n, ctx=ctx, bloom=bloom).build(dev(rk), dev(rp))
-    assert ht.capacity == 1 << 24
+    assert ht.capacity > 1 << 22  # above one 32 MB region
     d = dev(sk)
     assert ht.probe(d) == oracle.hashjoin(rk, rp, sk)
     assert ht.probe(d[1:]) == oracle.hashjoin(rk, rp, sk[1:])
@@ -368,7 +399,7 @@ def test_hash_join_probe_large_table(ctx, bloom):
 @pytest.mark.parametrize("mode", [0, 2])
 def test_hash_join_region_build(ctx, mode):
     """A build side whose table is larger than one 32 MB region (2^22 rows:
-    2^23 slots, 64 MB) is built region by region by default (mode 0) or
+    about 5.6M slots, 45 MB) is built region by region by default (mode 0) or
     directly (OLAP_TUNE_JOIN_BUILD = 2): duplicate keys keep their last row,
     the reserved key is counted, and probes equal the oracle's either way."""
     rng = np.random.default_rng(31)
@@ -382,7 +413,7 @@ def test_hash_join_region_build(ctx, mode):
         ht = ops.HashTable(n, ctx=ctx).build(dev(rk), dev(rp))
     finally:
         ctx.set_tuning(_lib.TUNE_JOIN_BUILD, 0)
-    assert ht.capacity == 1 << 23
+    assert ht.capacity > 1 << 22  # above one 32 MB region
     assert ctx.take_range_errors() == int((rk == np.iinfo(np.int32).min).sum())
     assert ht.probe(dev(sk)) == oracle.hashjoin(rk, rp, sk)
     rows, pay = ht.probe_pairs(dev(sk[:300_000]))

@@ -358,7 +358,8 @@ def test_hash_join_any_capacity(ctx, cap, n):
     sk = rng.integers(-n, n, 4 * n + 3).astype(np.int32)
     L, h = _lib.lib, ctx.handle
     table = torch.empty(cap, dtype=torch.int64, device="cuda")
-    _lib.check(L.olap_hashjoin_build(h, dev(rk).data_ptr(), dev(rp).data_ptr(), n, table.data_ptr(), cap), h)
+    drk, drp = dev(rk), dev(rp)  # kept alive across the calls
+    _lib.check(L.olap_hashjoin_build(h, drk.data_ptr(), drp.data_ptr(), n, table.data_ptr(), cap), h)
     s_, m_ = torch.zeros(1, dtype=torch.int64, device="cuda"), torch.zeros(1, dtype=torch.int64, device="cuda")
     dk = dev(sk)
     _lib.check(L.olap_hashjoin_probe_filtered(h, table.data_ptr(), cap, None, 0, dk.data_ptr(), len(sk),
@@ -374,7 +375,7 @@ def test_hash_join_any_capacity(ctx, cap, n):
     assert np.array_equal(host(rows[:k]), erows) and np.array_equal(host(pay[:k]), epay)
     for bad in (cap + 4, n):
         with pytest.raises(_lib.OlapError):
-            _lib.check(L.olap_hashjoin_build(h, dev(rk).data_ptr(), dev(rp).data_ptr(), n, table.data_ptr(), bad), h)
+            _lib.check(L.olap_hashjoin_build(h, drk.data_ptr(), drp.data_ptr(), n, table.data_ptr(), bad), h)
 
 
 @pytest.mark.parametrize("bloom", [True, False])

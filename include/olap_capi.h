@@ -350,7 +350,7 @@ OLAP_API int olap_gather_i32(olap_ctx* ctx, const int32_t* rowids, int64_t k, in
 
 /* ---- joins (code/join) -------------------------------------------------------
  * Hash table: capacity 64-bit slots (a multiple of 8 in (n, 2^32]; use
- * olap_hashtable_capacity(n), about 4n/3 slots: load <= 3/4), 16-byte
+ * olap_hashtable_capacity(n), about 2n slots: load <= 1/2), 16-byte
  * aligned, caller-allocated.  A key's home slot is its hash scaled onto the
  * capacity (linear probing from there).  A duplicate build key keeps the payload of its last
  * row, as the reference's sequential build does.  Key INT32_MIN marks empty

@@ -380,7 +380,7 @@ def test_hash_join_any_capacity(ctx, cap, n):
 
 @pytest.mark.parametrize("bloom", [True, False])
 def test_hash_join_probe_large_table(ctx, bloom):
-    """2^22 + 5 build rows (a table of about 5.6M slots, 45 MB: above one L2-sized
+    """2^22 + 5 build rows (a table of about 8.4M slots, 67 MB: above one L2-sized
     region) probed by 2^22 + 1001 keys, with and without the Bloom filter,
     aligned and unaligned, a ragged count and edge keys: the same (sum,
     matches) as the oracle."""
@@ -400,7 +400,7 @@ def test_hash_join_probe_large_table(ctx, bloom):
 @pytest.mark.parametrize("mode", [0, 2])
 def test_hash_join_region_build(ctx, mode):
     """A build side whose table is larger than one 32 MB region (2^22 rows:
-    about 5.6M slots, 45 MB) is built region by region by default (mode 0) or
+    about 8.4M slots, 67 MB) is built region by region by default (mode 0) or
     directly (OLAP_TUNE_JOIN_BUILD = 2): duplicate keys keep their last row,
     the reserved key is counted, and probes equal the oracle's either way."""
     rng = np.random.default_rng(31)

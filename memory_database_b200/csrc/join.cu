@@ -647,7 +647,7 @@ int64_t olap_hashtable_capacity(int64_t n_build) {
   // load <= 1/2: at 3/4 (a 179 MB table for 2^24 keys instead of 256 MB)
   // more of the table stayed in L2, but the longer probe runs cost more
   // dependent round trips (probe 5.9 ms instead of 3.3 ms over 2^28 keys)
-  const int64_t cap = (2 * n_build + 8) & ~int64_t(7);
+  const int64_t cap = (2 * n_build + 7) & ~int64_t(7);
   return cap < 8 ? 8 : cap;
 }
 

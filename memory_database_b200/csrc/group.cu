@@ -16,6 +16,7 @@
 // every distinct key fits one table, else per partition of the key hash
 // (see the plans below).
 #include <algorithm>
+#include <vector>
 #include <cstring>
 
 #include "compact.cuh"
@@ -644,6 +645,7 @@ __global__ void __launch_bounds__(1024) group_part_scatter_kernel(PartPlan pp, c
 // partition's run.  Shared memory: tile counts, tile offsets and the block's
 // cursors (P each), then the sorted rows.
 constexpr int kScatterTile = 4096;
+constexpr int kMaxPartials = 256;  // partial tables of split partitions (128 KB each)
 constexpr int kTiledParts = 4096;
 
 template <bool HAS2>
@@ -750,21 +752,74 @@ __global__ void __launch_bounds__(1024) group_part_scatter_tiled_kernel(
   }
 }
 
-// One block per partition: aggregate in a shared table, then append the
-// groups to the outputs (positions from one global counter per block).
-template <bool HAS2>
-__global__ void __launch_bounds__(kAggThreads) group_part_agg_kernel(
-    const long long* __restrict__ part_begin, const typename PartRow<HAS2>::T* __restrict__ rows, int combine,
-    int64_t capacity, int32_t* __restrict__ out_keys, int64_t* __restrict__ out_sums,
-    int64_t* __restrict__ out_counts, unsigned long long* d_groups, unsigned long long* overflow) {
-  extern __shared__ __align__(16) unsigned char agg_smem[];
+// Appends the occupied slots of a block's shared table to the outputs
+// (positions from one global counter per block).  Every thread of the block
+// calls it (it synchronises the block).
+__device__ __forceinline__ void append_groups(const SmemAgg& st, int64_t capacity, int32_t* __restrict__ out_keys,
+                                              int64_t* __restrict__ out_sums, int64_t* __restrict__ out_counts,
+                                              unsigned long long* d_groups, unsigned long long* overflow) {
   __shared__ unsigned int s_n;
   __shared__ unsigned long long s_base;
-  const SmemAgg st = smem_agg(agg_smem, kAggSlots);
-  smem_agg_clear(st);
   if (threadIdx.x == 0) s_n = 0;
   __syncthreads();
-  const int64_t b = part_begin[blockIdx.x], e = part_begin[blockIdx.x + 1];
+  constexpr int kPer = kAggSlots / kAggThreads;
+  unsigned int pos[kPer];
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int i = j * kAggThreads + threadIdx.x;
+    pos[j] = st.key[i] != kEmptyKey ? atomicAdd(&s_n, 1u) : ~0u;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) s_base = s_n ? atomicAdd(d_groups, static_cast<unsigned long long>(s_n)) : 0ull;
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    if (pos[j] == ~0u) continue;
+    const int i = j * kAggThreads + threadIdx.x;
+    const unsigned long long o = s_base + pos[j];
+    if (o >= static_cast<unsigned long long>(capacity)) {  // more groups than the outputs hold
+      atomicAdd(overflow, 1ull);
+      continue;
+    }
+    out_keys[o] = st.key[i];
+    out_sums[o] = static_cast<int64_t>(st.sum(i));
+    if (out_counts) out_counts[o] = static_cast<int64_t>(st.cnt[i]);
+  }
+}
+
+// A block's share of the partitioned rows: a whole partition (partial < 0:
+// its groups go straight to the outputs), or a slice of a partition too
+// large for one block (its table is written whole to partial table
+// `partial`, and group_part_merge_kernel adds the slices' tables up).
+struct AggUnit {
+  long long begin, end;
+  int32_t partial;
+  int32_t pad;
+};
+
+// One block per unit (or, with units null, per partition): aggregate the
+// rows in a shared table, then append the groups or write the partial table.
+template <bool HAS2>
+__global__ void __launch_bounds__(kAggThreads) group_part_agg_kernel(
+    const long long* __restrict__ part_begin, const AggUnit* __restrict__ units,
+    const typename PartRow<HAS2>::T* __restrict__ rows, int combine, int64_t capacity,
+    int32_t* __restrict__ out_keys, int64_t* __restrict__ out_sums, int64_t* __restrict__ out_counts,
+    unsigned long long* d_groups, unsigned long long* overflow, int4* __restrict__ partials) {
+  extern __shared__ __align__(16) unsigned char agg_smem[];
+  const SmemAgg st = smem_agg(agg_smem, kAggSlots);
+  smem_agg_clear(st);
+  __syncthreads();
+  int64_t b, e;
+  int partial = -1;
+  if (units) {
+    const AggUnit u = units[blockIdx.x];
+    b = u.begin;
+    e = u.end;
+    partial = u.partial;
+  } else {
+    b = part_begin[blockIdx.x];
+    e = part_begin[blockIdx.x + 1];
+  }
   unsigned int lost = 0;
   // rows of the partition, 8 per thread in flight
   for (int64_t base = b; base < e; base += 8 * static_cast<int64_t>(blockDim.x)) {
@@ -807,29 +862,40 @@ __global__ void __launch_bounds__(kAggThreads) group_part_agg_kernel(
   }
   if (lost) atomicAdd(overflow, static_cast<unsigned long long>(lost));
   __syncthreads();
-  constexpr int kPer = kAggSlots / kAggThreads;
-  unsigned int pos[kPer];
-#pragma unroll
-  for (int j = 0; j < kPer; ++j) {
-    const int i = j * kAggThreads + threadIdx.x;
-    pos[j] = st.key[i] != kEmptyKey ? atomicAdd(&s_n, 1u) : ~0u;
+  if (partial >= 0) {  // the whole table, as laid out in shared memory (16 bytes per slot)
+    const int4* src = reinterpret_cast<const int4*>(agg_smem);
+    int4* dst = partials + static_cast<int64_t>(partial) * kAggSlots;
+    for (int i = threadIdx.x; i < kAggSlots; i += blockDim.x) dst[i] = src[i];
+    return;
   }
+  append_groups(st, capacity, out_keys, out_sums, out_counts, d_groups, overflow);
+}
+
+// One block per partition split over several units: adds up the partial
+// tables of its units (merge[b] = (first partial, count)) in a shared table
+// and appends the groups.
+__global__ void __launch_bounds__(kAggThreads) group_part_merge_kernel(
+    const int2* __restrict__ merge, const int4* __restrict__ partials, int64_t capacity,
+    int32_t* __restrict__ out_keys, int64_t* __restrict__ out_sums, int64_t* __restrict__ out_counts,
+    unsigned long long* d_groups, unsigned long long* overflow) {
+  extern __shared__ __align__(16) unsigned char agg_smem[];
+  const SmemAgg st = smem_agg(agg_smem, kAggSlots);
+  smem_agg_clear(st);
   __syncthreads();
-  if (threadIdx.x == 0) s_base = s_n ? atomicAdd(d_groups, static_cast<unsigned long long>(s_n)) : 0ull;
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < kPer; ++j) {
-    if (pos[j] == ~0u) continue;
-    const int i = j * kAggThreads + threadIdx.x;
-    const unsigned long long o = s_base + pos[j];
-    if (o >= static_cast<unsigned long long>(capacity)) {  // more groups than the outputs hold
-      atomicAdd(overflow, 1ull);
-      continue;
+  const int2 m = merge[blockIdx.x];
+  unsigned int lost = 0;
+  for (int q = 0; q < m.y; ++q) {
+    const SmemAgg pt = smem_agg(reinterpret_cast<unsigned char*>(const_cast<int4*>(partials) +
+                                                                 static_cast<int64_t>(m.x + q) * kAggSlots),
+                                kAggSlots);
+    for (int i = threadIdx.x; i < kAggSlots; i += blockDim.x) {
+      const int32_t k = pt.key[i];
+      if (k != kEmptyKey && !smem_agg_add(st, k, pt.sum(i), pt.cnt[i])) ++lost;
     }
-    out_keys[o] = st.key[i];
-    out_sums[o] = static_cast<int64_t>(st.sum(i));
-    if (out_counts) out_counts[o] = static_cast<int64_t>(st.cnt[i]);
   }
+  if (lost) atomicAdd(overflow, static_cast<unsigned long long>(lost));
+  __syncthreads();
+  append_groups(st, capacity, out_keys, out_sums, out_counts, d_groups, overflow);
 }
 
 // Compaction of the occupied slots into (key, sum, count) arrays.
@@ -1114,14 +1180,24 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
     // part_begin[P + 1], then ptot[P] and cursor[P] (zeroed together)
     const size_t begin_bytes = sizeof(long long) * (3 * static_cast<size_t>(pp.n_parts) + 1);
     const size_t row_bytes = vals2 ? 16 : 8;
-    const size_t bytes = hist_bytes + begin_bytes + static_cast<size_t>(n > 0 ? n : 1) * row_bytes + 256;
+    // after the rows: the work units, the merge list and the partial tables
+    // of partitions too large for one block (at most kMaxPartials of them)
+    const size_t rows_off = (begin_bytes + hist_bytes + 255) & ~size_t(255);
+    const size_t units_off = (rows_off + static_cast<size_t>(n > 0 ? n : 1) * row_bytes + 255) & ~size_t(255);
+    const size_t max_units = static_cast<size_t>(pp.n_parts) + olap::kMaxPartials;
+    const size_t merge_off = (units_off + sizeof(olap::AggUnit) * max_units + 255) & ~size_t(255);
+    const size_t part_off = (merge_off + sizeof(int2) * static_cast<size_t>(pp.n_parts) + 255) & ~size_t(255);
+    const size_t bytes = part_off + static_cast<size_t>(olap::kMaxPartials) * olap::kAggSlots * 16;
     mem = olap::big_scratch(ctx, bytes);
     if (!mem) return olap::set_error(ctx, OLAP_ERR_NOMEM, "device memory for the group partitions");
     long long* part_begin = reinterpret_cast<long long*>(mem);
     auto* ptot = reinterpret_cast<unsigned long long*>(part_begin + pp.n_parts + 1);
     auto* cursor = ptot + pp.n_parts;
     unsigned int* hist = reinterpret_cast<unsigned int*>(mem + begin_bytes);
-    char* rowbuf = mem + ((begin_bytes + hist_bytes + 255) & ~size_t(255));
+    char* rowbuf = mem + rows_off;
+    auto* d_units = reinterpret_cast<olap::AggUnit*>(mem + units_off);
+    auto* d_merge = reinterpret_cast<int2*>(mem + merge_off);
+    auto* d_partials = reinterpret_cast<int4*>(mem + part_off);
     e = cudaMemsetAsync(d_groups, 0, sizeof(int64_t), ctx->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(ptot, 0, sizeof(unsigned long long) * pp.n_parts, ctx->stream);
     const size_t psmem = sizeof(unsigned int) * pp.n_parts;
@@ -1151,11 +1227,58 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(olap::group_part_agg_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                static_cast<int>(asmem));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(olap::group_part_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(asmem));
     if (e == cudaSuccess) {
       olap::group_part_hist_kernel<<<pp.n_blocks, 1024, psmem, ctx->stream>>>(pp, keys, hist, ptot,
                                                                               &ctx->counters->range_errors);
       olap::group_part_scan_kernel<<<1, 1024, 0, ctx->stream>>>(pp, ptot, part_begin, cursor);
       auto* d_groups_u = reinterpret_cast<unsigned long long*>(d_groups);
+      // Partition sizes decide the blocks: a partition far above the average
+      // (skewed keys) is split into slices of at most `limit` rows whose
+      // partial tables are merged afterwards, so no single block gets it all.
+      std::vector<long long> pb(static_cast<size_t>(pp.n_parts) + 1);
+      e = cudaMemcpyAsync(pb.data(), part_begin, sizeof(long long) * pb.size(), cudaMemcpyDeviceToHost, ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+      std::vector<olap::AggUnit> units;
+      std::vector<int2> merges;
+      if (e == cudaSuccess) {
+        const int64_t avg = (n + pp.n_parts - 1) / pp.n_parts;
+        int64_t limit = std::max<int64_t>(2 * avg, int64_t(1) << 16);
+        auto slices = [&](int64_t lim) {
+          int64_t t = 0;
+          for (int p = 0; p < pp.n_parts; ++p) {
+            const int64_t sz = pb[p + 1] - pb[p];
+            if (sz > lim) t += (sz + lim - 1) / lim;
+          }
+          return t;
+        };
+        while (slices(limit) > olap::kMaxPartials) limit *= 2;
+        int32_t np = 0;
+        for (int p = 0; p < pp.n_parts; ++p) {
+          const int64_t sz = pb[p + 1] - pb[p];
+          if (sz <= limit) continue;
+          const int64_t k = (sz + limit - 1) / limit;
+          merges.push_back(make_int2(np, static_cast<int>(k)));
+          for (int64_t q = 0; q < k; ++q) {
+            const long long lo = pb[p] + q * limit, hi = std::min<long long>(pb[p + 1], lo + limit);
+            units.push_back(olap::AggUnit{lo, hi, np++, 0});
+          }
+        }
+        if (!merges.empty()) {
+          for (int p = 0; p < pp.n_parts; ++p)
+            if (pb[p + 1] - pb[p] <= limit) units.push_back(olap::AggUnit{pb[p], pb[p + 1], -1, 0});
+          e = cudaMemcpyAsync(d_units, units.data(), sizeof(olap::AggUnit) * units.size(), cudaMemcpyHostToDevice,
+                              ctx->stream);
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_merge, merges.data(), sizeof(int2) * merges.size(), cudaMemcpyHostToDevice,
+                                ctx->stream);
+        }
+      }
+      const olap::AggUnit* unit_arg = merges.empty() ? nullptr : d_units;
+      const unsigned agg_grid = merges.empty() ? static_cast<unsigned>(pp.n_parts)
+                                               : static_cast<unsigned>(units.size());
       const bool tiled = pp.n_parts <= olap::kTiledParts;
       const size_t tsmem = (vals2 ? 16 : 8) * static_cast<size_t>(olap::kScatterTile) + 3 * psmem;
       if (vals2) {
@@ -1166,8 +1289,10 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
         else
           olap::group_part_scatter_kernel<true><<<pp.n_blocks, 1024, psmem, ctx->stream>>>(pp, keys, vals, vals2,
                                                                                           hist, cursor, rows);
-        olap::group_part_agg_kernel<true><<<pp.n_parts, olap::kAggThreads, asmem, ctx->stream>>>(
-            part_begin, rows, combine, capacity, out_keys, out_sums, out_counts, d_groups_u, overflow);
+        if (e == cudaSuccess)
+          olap::group_part_agg_kernel<true><<<agg_grid, olap::kAggThreads, asmem, ctx->stream>>>(
+              part_begin, unit_arg, rows, combine, capacity, out_keys, out_sums, out_counts, d_groups_u, overflow,
+              d_partials);
       } else {
         auto* rows = reinterpret_cast<int2*>(rowbuf);
         if (tiled)
@@ -1177,10 +1302,16 @@ int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_o
           olap::group_part_scatter_kernel<false><<<pp.n_blocks, 1024, psmem, ctx->stream>>>(pp, keys, vals,
                                                                                            nullptr, hist, cursor,
                                                                                            rows);
-        olap::group_part_agg_kernel<false><<<pp.n_parts, olap::kAggThreads, asmem, ctx->stream>>>(
-            part_begin, rows, combine, capacity, out_keys, out_sums, out_counts, d_groups_u, overflow);
+        if (e == cudaSuccess)
+          olap::group_part_agg_kernel<false><<<agg_grid, olap::kAggThreads, asmem, ctx->stream>>>(
+              part_begin, unit_arg, rows, combine, capacity, out_keys, out_sums, out_counts, d_groups_u, overflow,
+              d_partials);
       }
-      e = cudaGetLastError();
+      if (e == cudaSuccess && !merges.empty())
+        olap::group_part_merge_kernel<<<static_cast<unsigned>(merges.size()), olap::kAggThreads, asmem,
+                                        ctx->stream>>>(d_merge, d_partials, capacity, out_keys, out_sums,
+                                                       out_counts, d_groups_u, overflow);
+      if (e == cudaSuccess) e = cudaGetLastError();
     }
   }
   if (e == cudaSuccess) e = cudaGetLastError();

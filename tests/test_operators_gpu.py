@@ -330,6 +330,32 @@ def test_group_hash_plans(ctx, dist, G, n, two):
     assert ctx.take_range_errors() == int((keys[:1000] == keys[0]).sum())
 
 
+@pytest.mark.parametrize("two", [False, True])
+def test_group_hash_hot_partition(ctx, two):
+    """Partitioned plan with one key in 90 % of the rows: its partition is
+    split over several blocks whose partial tables are merged; every group's
+    sum and count equal the oracle's, with and without a second value
+    column, and the combining path agrees."""
+    rng = np.random.default_rng(77)
+    n, G = 2_000_003, 1 << 16
+    keys = rng.integers(0, G, n).astype(np.int32)
+    keys[rng.random(n) < 0.9] = 7
+    vals = rng.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32)
+    vals2 = rng.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32) if two else None
+    ek, es, ec = oracle.hash_group(keys, vals, vals2)
+    try:
+        for combine in (2, 1):
+            ctx.set_tuning(_lib.TUNE_GROUP_PLAN, 2)
+            ctx.set_tuning(_lib.TUNE_GROUP_COMBINE, combine)
+            k, sm, c = ops.group_hash(dev(keys), dev(vals), dev(vals2) if two else None, max_groups=G, ctx=ctx)
+            order = np.argsort(host(k))
+            assert np.array_equal(host(k)[order], ek)
+            assert np.array_equal(host(sm)[order], es) and np.array_equal(host(c)[order], ec)
+    finally:
+        ctx.set_tuning(_lib.TUNE_GROUP_PLAN, 0)
+        ctx.set_tuning(_lib.TUNE_GROUP_COMBINE, 0)
+
+
 @pytest.mark.parametrize("max_groups,distinct", [(100, 5000), (5000, 40000)])
 def test_group_hash_more_keys_than_capacity_fails(ctx, max_groups, distinct):
     keys = np.arange(distinct, dtype=np.int32)

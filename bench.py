@@ -545,8 +545,13 @@ def operators_result(a) -> dict:
     del table, bloom, dense, bkeys, bpay, miss
     torch.cuda.empty_cache()
     vals = gen(n, 120, 1, 10000)
-    for G in (16, 1 << 12, 1 << 20, 1 << 22):
-        keys = gen(n, 121, 0, G - 1)
+    for G, dist in ((16, "uniform"), (1 << 12, "uniform"), (1 << 20, "uniform"), (1 << 22, "uniform"),
+                    (1 << 20, "zipf1.0")):
+        if dist == "uniform":
+            keys = gen(n, 121, 0, G - 1)
+        else:
+            keys = torch.empty(n, dtype=torch.int32, device="cuda")
+            _lib.check(L.olap_gen_zipf_i32_dev(h, _ptr(keys), n, 99, 122, G, 1.0), h)
         gcap = int(L.olap_group_hash_capacity(G))
         ok_, os_, oc_ = (torch.empty(gcap, dtype=t, device="cuda") for t in (torch.int32, torch.int64, torch.int64))
         g_ = torch.zeros(1, dtype=torch.int64, device="cuda")
@@ -563,7 +568,7 @@ def operators_result(a) -> dict:
         gs[ok_[:k].long()] = os_[:k]
         gc[ok_[:k].long()] = oc_[:k]
         ok = k == int((ec > 0).sum()) and torch.equal(gs, es) and torch.equal(gc, ec)
-        res.append(entry("hash group-by SUM/COUNT", ms, 8 * n, ok, groups=G))
+        res.append(entry("hash group-by SUM/COUNT", ms, 8 * n, ok, groups=G, keys=dist))
         del keys, ok_, os_, oc_
     clk.__exit__(None, None, None)
     line = {"metric": "operator rows/sec and HBM GB/s vs peak", "value": min(r["frac_of_peak"] for r in res),
@@ -572,7 +577,7 @@ def operators_result(a) -> dict:
             "clocks": clk.summary(),
             "config": {"workload": f"operator set at {n:,} int32 rows (select at 0.001/0.01/0.1/0.5, gather of 4 "
                                    "columns, hash join 2^24 build / uniform and Zipf(1.0) probes at 50% match, "
-                                   "hash group-by at 16/4096/2^20/2^22 groups)"},
+                                   "hash group-by at 16/4096/2^20/2^22 uniform groups and 2^20 Zipf(1.0) groups)"},
             "data": "synthetic (seeded counter-based generator, generated in HBM)"}
     ctx.close()
     return line

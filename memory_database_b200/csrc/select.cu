@@ -247,9 +247,22 @@ struct GatherParams {
   int ncols;
 };
 
+// One gathered value.  kSparse: the load asks L2 for a 64-byte fetch on a
+// miss; when the row ids are far apart (more than 16 rows, 64 bytes, between
+// neighbours on average) the rest of a larger fetch is never used.  volatile
+// keeps each load inside its guard, as __ldg's own asm does.
+template <bool kSparse>
+__device__ __forceinline__ int32_t ld_gather(const int32_t* p) {
+  if (!kSparse) return __ldg(p);
+  int32_t v;
+  asm volatile("ld.global.nc.L2::64B.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
 // outs[c][i] = cols[c][rowids[i]]: row ids read with 128-bit loads, values
 // gathered through L1/L2 and written with 128-bit stores.  A row id outside
 // [0, col_len) yields 0 and is counted.
+template <bool kSparse>
 __global__ void gather_kernel(const int32_t* __restrict__ rowids, int64_t k, const GatherParams gp, int vec) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -264,10 +277,10 @@ __global__ void gather_kernel(const int32_t* __restrict__ rowids, int64_t k, con
     for (int c = 0; c < gp.ncols; ++c) {
       const int32_t* col = gp.cols[c];
       int4 v;
-      v.x = ox ? __ldg(col + r.x) : 0;
-      v.y = oy ? __ldg(col + r.y) : 0;
-      v.z = oz ? __ldg(col + r.z) : 0;
-      v.w = ow ? __ldg(col + r.w) : 0;
+      v.x = ox ? ld_gather<kSparse>(col + r.x) : 0;
+      v.y = oy ? ld_gather<kSparse>(col + r.y) : 0;
+      v.z = oz ? ld_gather<kSparse>(col + r.z) : 0;
+      v.w = ow ? ld_gather<kSparse>(col + r.w) : 0;
       reinterpret_cast<int4*>(gp.outs[c])[i] = v;
     }
   }
@@ -275,7 +288,7 @@ __global__ void gather_kernel(const int32_t* __restrict__ rowids, int64_t k, con
     const int32_t r = rowids[j];
     const bool o = ok(r);
     bad += !o;
-    for (int c = 0; c < gp.ncols; ++c) gp.outs[c][j] = o ? __ldg(gp.cols[c] + r) : 0;
+    for (int c = 0; c < gp.ncols; ++c) gp.outs[c][j] = o ? ld_gather<kSparse>(gp.cols[c] + r) : 0;
   }
   if (bad) atomicAdd(gp.range_err, static_cast<unsigned long long>(bad));
 }
@@ -458,7 +471,12 @@ int olap_gather_i32(olap_ctx* ctx, const int32_t* rowids, int64_t k, int ncols,
     gp.outs[c] = outs[c];
     vec &= olap::al16(outs[c]);
   }
-  olap::gather_kernel<<<olap::stream_grid(ctx, (k + 3) / 4, 256), 256, 0, ctx->stream>>>(rowids, k, gp, vec);
+  // row ids more than 16 rows apart on average: 64-byte fetches
+  const unsigned grid = olap::stream_grid(ctx, (k + 3) / 4, 256);
+  if (col_len > 16 * k)
+    olap::gather_kernel<true><<<grid, 256, 0, ctx->stream>>>(rowids, k, gp, vec);
+  else
+    olap::gather_kernel<false><<<grid, 256, 0, ctx->stream>>>(rowids, k, gp, vec);
   OLAP_CUDA_TRY(ctx, cudaGetLastError());
   return OLAP_OK;
 }

@@ -413,7 +413,9 @@ OLAP_API int64_t olap_group_hash_capacity(int64_t max_groups);
  * (more give OLAP_ERR_CAPACITY).  Up to capacity 8192 each block aggregates
  * in a shared-memory table; above, the rows are first partitioned by key
  * hash (the context keeps a grow-only device buffer of about 8-16 bytes per
- * row for that).  Synchronous. */
+ * row, plus up to 32 MB of partial tables, for that), and a partition far
+ * above the average size (skewed keys) is split over several blocks whose
+ * tables are merged.  Synchronous. */
 OLAP_API int olap_group_hash(olap_ctx* ctx, int64_t n, const int32_t* keys, int32_t key_offset,
                              const int32_t* vals, const int32_t* vals2, int64_t capacity,
                              int32_t* out_keys, int64_t* out_sums, int64_t* out_counts,

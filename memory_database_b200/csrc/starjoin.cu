@@ -1113,7 +1113,7 @@ int launch_starjoin(olap_ctx* ctx, StarPlan& pl, cudaStream_t stream) {
   k<<<static_cast<unsigned>(grid), pl.block, pl.smem, stream>>>(sp);
   OLAP_CUDA_TRY(ctx, cudaGetLastError());
   if (range_pass) {
-    pick_range_pass(pl.nd)<<<static_cast<unsigned>(ctx->sm_count) * 8, 256, 0, stream>>>(sp);
+    pick_range_pass(pl.nd)<<<static_cast<unsigned>(ctx->sm_count) * 2, 256, 0, stream>>>(sp);
     OLAP_CUDA_TRY(ctx, cudaGetLastError());
   }
   return OLAP_OK;

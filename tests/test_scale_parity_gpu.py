@@ -3,9 +3,8 @@
 * The reference's ten OLAPcore.sh queries on its own data stream at SF=100
   (600,000,000 fact rows, glibc rand() from its default seed): the B200
   kernel must reproduce the grand totals the reference published
-  (GPU/plot/old.py), and for q2.1 and q4.1 the oracle's per-group sums.  The
-  other eight queries are marked slow (a minute of host-side generation
-  each).
+  (GPU/plot/old.py), all ten of them (about 10 s of host-side generation
+  each), and for q2.1 and q4.1 the oracle's per-group sums too.
 * The 600M-row star-join the benchmark times, with the plan the autotuner
   picks for it and with the plan the benchmark recorded: per-group int64
   SUM(m1) and SUM(m1*m2) equal the oracle's on the same table (regenerated
@@ -42,8 +41,7 @@ def sf100_fk():
     del bufs
 
 
-@pytest.mark.parametrize("q", [pytest.param(q, id=_qid(q), marks=() if q["sqlnum"] in PER_GROUP else pytest.mark.slow)
-                               for q in GOLDEN])
+@pytest.mark.parametrize("q", [pytest.param(q, id=_qid(q)) for q in GOLDEN])
 def test_published_sf100_totals(ctx, q, sf100_fk):
     dv, fk, _, _ = oracle.gen_olapcore_compat(100.0, q["sele"], q["bitmap"], q["groups"], measures=False,
                                               fk_out=sf100_fk)

@@ -52,7 +52,7 @@ extern "C" {
 #define OLAP_ERR_RANGE (-5)       /* rows dropped: fk or group id out of range     */
 #define OLAP_ERR_CAPACITY (-6)    /* scratch arena or table capacity exceeded      */
 #define OLAP_ERR_TIMEOUT (-7)     /* a bounded device wait expired                 */
-#define OLAP_ERR_UNSUPPORTED (-8) /* shape not supported by this build             */
+#define OLAP_ERR_UNSUPPORTED (-8) /* shape not supported by this library           */
 
 /* Aggregate expressions of the star-join (per surviving fact row). */
 #define OLAP_AGG_M1_PLUS_M2 0  /* M1 + M2: the reference's SUM (cpp:360, :428) */

@@ -83,8 +83,10 @@ extern "C" {
                                        3 in place always */
 #define OLAP_TUNE_MERGE_PROBES 14   /* star-join: 1 probes consecutive L2 int8 dimensions together, 2 off */
 #define OLAP_TUNE_PROBE_ORDER 15    /* star-join: 1 probes the dimensions staged as int8 last, 2 first */
-#define OLAP_TUNE_JOIN_BUILD 16     /* hash join build: 1 region by region (the default for tables above
-                                       32 MB), 2 direct (one random DRAM sector per insert) */
+#define OLAP_TUNE_JOIN_BUILD 16     /* hash join build of tables above 32 MB: 1 (default) 128 KB regions
+                                       built in shared memory up to 2^27 slots, 32 MB regions in L2
+                                       above; 2 direct (one random DRAM sector per insert); 3 32 MB
+                                       regions in L2 at every size */
 #define OLAP_TUNE_KNOBS 17          /* knobs olap_ctx_set_tuning accepts (the autotuner sets 0..15) */
 
 typedef struct olap_ctx olap_ctx;
@@ -358,10 +360,14 @@ OLAP_API int olap_gather_i32(olap_ctx* ctx, const int32_t* rowids, int64_t k, in
 OLAP_API int64_t olap_hashtable_capacity(int64_t n_build);
 /* build(relation_t*, std::unordered_map&) (join/test_join_option.cpp:44-50);
  * synchronous; OLAP_ERR_CAPACITY if the table fills.  A table above 32 MB is
- * built region by region (the rows scattered by the 32 MB region of their
- * home slot, then inserted one region at a time so that the inserts stay in
- * L2), with scratch of 8 bytes per build row from the context's grow-only
- * buffer; OLAP_TUNE_JOIN_BUILD = 2 inserts directly instead. */
+ * built region by region: up to 2^27 slots the rows are grouped by the
+ * 16,384-slot (128 KB) region of their home slot and each region is built in
+ * shared memory and written once, payloads in place (a row whose probe run
+ * leaves its region is inserted afterwards from the next region on, where
+ * linear probing over the whole table puts it); above, by 32 MB regions
+ * inserted one at a time in L2.  Scratch: 16 (8 above 2^27 slots) bytes per
+ * build row from the context's grow-only buffer.  OLAP_TUNE_JOIN_BUILD
+ * chooses the way (see its values). */
 OLAP_API int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* payload,
                                  int64_t n, uint64_t* table, int64_t capacity);
 /* probe(relation_t*, std::unordered_map&) (join:90-96): *d_sum = SUM of the

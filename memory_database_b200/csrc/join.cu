@@ -344,6 +344,203 @@ __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const l
   }
 }
 
+// ---- region build in shared memory ------------------------------------------
+// For tables up to 2^27 slots the rows are grouped by the 16,384-slot region
+// (128 KB) of their home slot, and one block builds each region in shared
+// memory: it inserts the region's rows with shared-memory CAS, then writes
+// the whole region (empty slots too) with the payloads already in place, so
+// the table needs no separate fill or finish pass and every slot crosses
+// DRAM once.  A row whose probe run would leave its region (every slot from
+// its home to the region's end taken) is set aside and inserted afterwards
+// into the finished table from the next region's first slot on, exactly where
+// linear probing over the whole table would have put it.
+constexpr int kSmemRegionSlots = 16384;
+constexpr int kSmemRegionShift = 14;
+constexpr int64_t kSmemRegionMaxRegions = 8192;
+constexpr int kSmemRegionThreads = 1024;
+
+// Region counts: per block in shared memory, then one global add per region.
+__global__ void __launch_bounds__(kBuildPartThreads) smem_region_count_kernel(
+    const int32_t* __restrict__ keys, int64_t n, int64_t per, uint64_t cap, int n_regions, int vec,
+    unsigned int* __restrict__ counts, unsigned long long* range_err) {
+  extern __shared__ unsigned int s_rc[];
+  for (int p = threadIdx.x; p < n_regions; p += blockDim.x) s_rc[p] = 0;
+  __syncthreads();
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * per;
+  const int64_t e = b + per < n ? b + per : n;
+  unsigned int bad = 0;
+  for (int64_t r = b + 4 * static_cast<int64_t>(threadIdx.x); r < e; r += 4 * static_cast<int64_t>(blockDim.x)) {
+    int32_t k[4];
+    build_keys4(keys, r, e, vec, k);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (r + u >= e) continue;
+      if (k[u] == INT32_MIN) {
+        ++bad;
+        continue;
+      }
+      atomicAdd(&s_rc[home_slot(static_cast<uint32_t>(k[u]), cap) >> kSmemRegionShift], 1u);
+    }
+  }
+  if (bad) atomicAdd(range_err, static_cast<unsigned long long>(bad));
+  __syncthreads();
+  for (int p = threadIdx.x; p < n_regions; p += blockDim.x)
+    if (s_rc[p]) atomicAdd(&counts[p], s_rc[p]);
+}
+
+// Exclusive scan of the region counts (one block): begin[p], begin[P] = all
+// rows, and cursor[p] = begin[p] for the scatter.
+__global__ void __launch_bounds__(1024) smem_region_scan_kernel(const unsigned int* __restrict__ counts, int n_regions,
+                                                                 long long* __restrict__ begin,
+                                                                 unsigned long long* __restrict__ cursor) {
+  __shared__ long long s_run[1024];
+  const int per = (n_regions + blockDim.x - 1) / blockDim.x;
+  const int lo = threadIdx.x * per, hi = lo + per < n_regions ? lo + per : n_regions;
+  long long mine = 0;
+  for (int p = lo; p < hi; ++p) mine += counts[p];
+  s_run[threadIdx.x] = mine;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const long long y = threadIdx.x >= o ? s_run[threadIdx.x - o] : 0;
+    __syncthreads();
+    s_run[threadIdx.x] += y;
+    __syncthreads();
+  }
+  long long run = s_run[threadIdx.x] - mine;
+  for (int p = lo; p < hi; ++p) {
+    begin[p] = run;
+    cursor[p] = static_cast<unsigned long long>(run);
+    run += counts[p];
+  }
+  if (threadIdx.x == blockDim.x - 1) begin[n_regions] = s_run[threadIdx.x];
+}
+
+// Scatter of the (key << 32 | row) tuples by region: a block counts its rows
+// per region, claims one run per region from the global cursors, then writes
+// its rows into its runs (its keys are read twice, the second time from L2).
+__global__ void __launch_bounds__(kBuildPartThreads) smem_region_scatter_kernel(
+    const int32_t* __restrict__ keys, int64_t n, int64_t per, uint64_t cap, int n_regions, int vec,
+    unsigned long long* __restrict__ cursor, uint64_t* __restrict__ tuples) {
+  extern __shared__ unsigned long long s_rs[];
+  unsigned int* s_cnt = reinterpret_cast<unsigned int*>(s_rs + n_regions);
+  for (int p = threadIdx.x; p < n_regions; p += blockDim.x) s_cnt[p] = 0;
+  __syncthreads();
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * per;
+  const int64_t e = b + per < n ? b + per : n;
+  const int64_t step = 4 * static_cast<int64_t>(blockDim.x);
+  for (int64_t r = b + 4 * static_cast<int64_t>(threadIdx.x); r < e; r += step) {
+    int32_t k[4];
+    build_keys4(keys, r, e, vec, k);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (r + u < e && k[u] != INT32_MIN)
+        atomicAdd(&s_cnt[home_slot(static_cast<uint32_t>(k[u]), cap) >> kSmemRegionShift], 1u);
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < n_regions; p += blockDim.x) {
+    const unsigned int c = s_cnt[p];
+    s_rs[p] = c ? atomicAdd(&cursor[p], static_cast<unsigned long long>(c)) : 0ull;
+    s_cnt[p] = 0;
+  }
+  __syncthreads();
+  for (int64_t r = b + 4 * static_cast<int64_t>(threadIdx.x); r < e; r += step) {
+    int32_t k[4];
+    build_keys4(keys, r, e, vec, k);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (r + u >= e || k[u] == INT32_MIN) continue;
+      const uint64_t reg = home_slot(static_cast<uint32_t>(k[u]), cap) >> kSmemRegionShift;
+      const unsigned int at = atomicAdd(&s_cnt[reg], 1u);
+      tuples[s_rs[reg] + at] = (static_cast<uint64_t>(static_cast<uint32_t>(k[u])) << 32) |
+                               static_cast<uint32_t>(r + u);
+    }
+  }
+}
+
+// One block per region: insert its rows in a shared-memory copy of the
+// region, set aside the rows whose run would leave it, then write the region
+// with (key, payload) in every taken slot and the empty marker elsewhere.
+// The payload reads are random over the payload column and marked
+// evict-last, so the column stays in L2 across the regions.
+__global__ void __launch_bounds__(kSmemRegionThreads) smem_region_build_kernel(
+    const uint64_t* __restrict__ tuples, const long long* __restrict__ begin, uint64_t* __restrict__ slots,
+    uint64_t cap, const int32_t* __restrict__ payload, uint64_t* __restrict__ spill,
+    unsigned long long* __restrict__ n_spill) {
+  extern __shared__ unsigned long long s_slot[];
+  const uint64_t base = static_cast<uint64_t>(blockIdx.x) << kSmemRegionShift;
+  const uint32_t len = static_cast<uint32_t>(cap - base < kSmemRegionSlots ? cap - base : kSmemRegionSlots);
+  for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) s_slot[i] = kEmptySlot;
+  __syncthreads();
+  const int64_t b = begin[blockIdx.x], e = begin[blockIdx.x + 1];
+  for (int64_t t = b + threadIdx.x; t < e; t += blockDim.x) {
+    const unsigned long long mine = tuples[t];
+    const uint32_t k = static_cast<uint32_t>(mine >> 32);
+    bool done = false;
+    for (uint32_t j = static_cast<uint32_t>(home_slot(k, cap) - base); j < len && !done; ++j) {
+      const unsigned long long prev = atomicCAS(&s_slot[j], kEmptySlot, mine);
+      if (prev == kEmptySlot) {
+        done = true;
+      } else if ((prev >> 32) == k) {
+        atomicMax(&s_slot[j], mine);  // same key: keeps the largest row
+        done = true;
+      }
+    }
+    if (!done) spill[atomicAdd(n_spill, 1ull)] = mine;  // the run reached the region's end
+  }
+  __syncthreads();
+  const uint64_t keep = policy_evict_last();
+  for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+    const uint64_t v = s_slot[i];
+    const bool full = v != kEmptySlot;
+    const int32_t pay = ld_probe_s32(payload + (full ? static_cast<uint32_t>(v) : 0u), keep);
+    slots[base + i] = full ? ((v & 0xffffffff00000000ull) | static_cast<uint32_t>(pay)) : kEmptySlot;
+  }
+}
+
+// The set-aside rows, into the finished table from the first slot after
+// their region on (linear probing across regions, wrapping at the end); the
+// slots they take are listed for the payload pass.  A key already there (an
+// earlier set-aside copy) keeps its largest row.
+__global__ void smem_region_spill_kernel(const uint64_t* __restrict__ spill, const unsigned long long* n_spill,
+                                         uint64_t* __restrict__ slots, uint64_t cap, uint64_t* __restrict__ taken,
+                                         unsigned long long* __restrict__ n_taken, unsigned long long* overflow) {
+  const int64_t n = static_cast<int64_t>(*n_spill);
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const unsigned long long mine = spill[i];
+    const uint32_t k = static_cast<uint32_t>(mine >> 32);
+    const uint64_t next = ((home_slot(k, cap) >> kSmemRegionShift) + 1) << kSmemRegionShift;
+    uint64_t h = next >= cap ? 0 : next;
+    bool done = false;
+    for (uint64_t step = 0; step < cap && !done; ++step) {
+      unsigned long long* s = reinterpret_cast<unsigned long long*>(slots + h);
+      const unsigned long long prev = atomicCAS(s, kEmptySlot, mine);
+      if (prev == kEmptySlot) {
+        taken[atomicAdd(n_taken, 1ull)] = h;
+        done = true;
+      } else if ((prev >> 32) == k) {
+        atomicMax(s, mine);
+        done = true;
+      } else {
+        h = next_slot(h, cap);
+      }
+    }
+    if (!done) atomicAdd(overflow, 1ull);
+  }
+}
+
+// Payloads into the slots the set-aside rows took.
+__global__ void smem_region_taken_kernel(const uint64_t* __restrict__ taken, const unsigned long long* n_taken,
+                                         uint64_t* __restrict__ slots, const int32_t* __restrict__ payload) {
+  const int64_t n = static_cast<int64_t>(*n_taken);
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint64_t s = taken[i];
+    const uint64_t v = slots[s];
+    slots[s] = (v & 0xffffffff00000000ull) | static_cast<uint32_t>(payload[static_cast<uint32_t>(v)]);
+  }
+}
+
 // Half a bucket (two slots) of the hash table, marked evict-last in L2: every
 // probe re-reads the table at random while the probe keys stream past it once,
 // so the part of the table that L2 holds should stay there.  The 64-byte
@@ -668,12 +865,59 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
   unsigned long long* overflow = ar.take<unsigned long long>(1);
   if (!overflow) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
   OLAP_CUDA_TRY(ctx, cudaMemsetAsync(overflow, 0, sizeof(*overflow), ctx->stream));
-  olap::fill_u64_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, olap::kEmptySlot);
-  // Tables larger than one region are built region by region, unless
-  // OLAP_TUNE_JOIN_BUILD = 2 asks for the direct build.
-  const bool partitioned = capacity > olap::kBuildRegionSlots && n >= (int64_t(1) << 16) &&
-                           ctx->tune[olap::TUNE_JOIN_BUILD] != 2;
-  if (n && partitioned) {
+  // Tables above 32 MB: built 128 KB region by 128 KB region in shared
+  // memory (up to 2^27 slots), or 32 MB region by 32 MB region in L2
+  // (OLAP_TUNE_JOIN_BUILD = 3, and above 2^27 slots); OLAP_TUNE_JOIN_BUILD = 2
+  // asks for the direct build.
+  const int64_t build_knob = ctx->tune[olap::TUNE_JOIN_BUILD];
+  const bool big = capacity > olap::kBuildRegionSlots && n >= (int64_t(1) << 16) && build_knob != 2;
+  const bool smem_regions = big && build_knob != 3 &&
+                            capacity <= olap::kSmemRegionMaxRegions * olap::kSmemRegionSlots;
+  const bool partitioned = big && !smem_regions;
+  if (n && smem_regions) {
+    const int P = static_cast<int>((capacity + olap::kSmemRegionSlots - 1) / olap::kSmemRegionSlots);
+    const int nb = ctx->sm_count * 2;
+    const int64_t per = ((n + nb - 1) / nb + 3) & ~int64_t(3);
+    const int vec = olap::al16(keys);
+    const uint64_t cap = static_cast<uint64_t>(capacity);
+    // counts[P] | n_spill | n_taken (zeroed together), begin[P+1], cursor[P], tuples[n] (then the taken
+    // slots), spill[n]
+    const size_t cnt_bytes = (sizeof(unsigned int) * P + 2 * sizeof(unsigned long long) + 255) & ~size_t(255);
+    const size_t begin_off = cnt_bytes;
+    const size_t cursor_off = (begin_off + sizeof(long long) * (P + 1) + 255) & ~size_t(255);
+    const size_t tup_off = (cursor_off + sizeof(unsigned long long) * P + 255) & ~size_t(255);
+    const size_t spill_off = (tup_off + sizeof(uint64_t) * static_cast<size_t>(n) + 255) & ~size_t(255);
+    char* mem = olap::big_scratch(ctx, spill_off + sizeof(uint64_t) * static_cast<size_t>(n));
+    if (!mem) return olap::set_error(ctx, OLAP_ERR_NOMEM, "device memory for the build regions");
+    auto* counts = reinterpret_cast<unsigned int*>(mem);
+    auto* n_spill = reinterpret_cast<unsigned long long*>(mem + ((sizeof(unsigned int) * P + 7) & ~size_t(7)));
+    auto* n_taken = n_spill + 1;
+    auto* begin = reinterpret_cast<long long*>(mem + begin_off);
+    auto* cursor = reinterpret_cast<unsigned long long*>(mem + cursor_off);
+    auto* tuples = reinterpret_cast<uint64_t*>(mem + tup_off);
+    auto* spill = reinterpret_cast<uint64_t*>(mem + spill_off);
+    const int rsm = static_cast<int>(sizeof(unsigned long long) * olap::kSmemRegionSlots);
+    const int ssm = static_cast<int>((sizeof(unsigned long long) + sizeof(unsigned int)) * P);
+    OLAP_CUDA_TRY(ctx, cudaMemsetAsync(mem, 0, cnt_bytes, ctx->stream));
+    OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::smem_region_build_kernel,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, rsm));
+    if (ssm > 48 * 1024)
+      OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::smem_region_scatter_kernel,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, ssm));
+    olap::smem_region_count_kernel<<<nb, olap::kBuildPartThreads, sizeof(unsigned int) * P, ctx->stream>>>(
+        keys, n, per, cap, P, vec, counts, &ctx->counters->range_errors);
+    olap::smem_region_scan_kernel<<<1, 1024, 0, ctx->stream>>>(counts, P, begin, cursor);
+    olap::smem_region_scatter_kernel<<<nb, olap::kBuildPartThreads, ssm, ctx->stream>>>(keys, n, per, cap, P, vec,
+                                                                                       cursor, tuples);
+    olap::smem_region_build_kernel<<<P, olap::kSmemRegionThreads, rsm, ctx->stream>>>(tuples, begin, table, cap,
+                                                                                      payload, spill, n_spill);
+    const unsigned sg = static_cast<unsigned>(ctx->sm_count) * 4;
+    olap::smem_region_spill_kernel<<<sg, 256, 0, ctx->stream>>>(spill, n_spill, table, cap, tuples, n_taken,
+                                                                overflow);
+    olap::smem_region_taken_kernel<<<sg, 256, 0, ctx->stream>>>(tuples, n_taken, table, payload);
+  } else if (n && partitioned) {
+    olap::fill_u64_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity,
+                                                                                       olap::kEmptySlot);
     const olap::BuildPlan bp = olap::region_plan(ctx, n, capacity, 4);
     const int vec = olap::al16(keys);
     OLAP_REQUIRE(ctx, bp.n_regions <= 2048, "hash table capacity above 2^33 slots");  // never: cap <= 2^32
@@ -698,7 +942,11 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
     for (int p = 0; p < bp.n_regions; ++p)
       olap::build_insert_kernel<<<ig, 256, 0, ctx->stream>>>(tuples, rbegin, p, table, bp.cap, overflow);
     olap::hash_finish_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, payload);
-  } else if (n) {
+  } else {
+    olap::fill_u64_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity,
+                                                                                       olap::kEmptySlot);
+  }
+  if (n && !smem_regions && !partitioned) {
     olap::hash_build_kernel<<<olap::grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(
         keys, n, table, static_cast<uint64_t>(capacity), &ctx->counters->range_errors, overflow);
     olap::hash_finish_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, payload);

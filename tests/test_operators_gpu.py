@@ -423,12 +423,66 @@ def test_hash_join_probe_large_table(ctx, bloom):
     assert ht.probe(d[1:]) == oracle.hashjoin(rk, rp, sk[1:])
 
 
-@pytest.mark.parametrize("mode", [0, 2])
+_M32 = 0xFFFFFFFF
+
+
+def _hash32(x):
+    x &= _M32
+    x ^= x >> 16
+    x = (x * 0x85EBCA6B) & _M32
+    x ^= x >> 13
+    x = (x * 0xC2B2AE35) & _M32
+    return x ^ (x >> 16)
+
+
+def _key_of_hash(h):
+    """The key whose 32-bit murmur finaliser is h (the finaliser is a bijection)."""
+    h ^= h >> 16
+    h = (h * pow(0xC2B2AE35, -1, 1 << 32)) & _M32
+    h ^= (h >> 13) ^ (h >> 26)
+    h = (h * pow(0x85EBCA6B, -1, 1 << 32)) & _M32
+    return h ^ (h >> 16)
+
+
+@pytest.mark.parametrize("mode", [0, 3])
+def test_hash_join_region_overflow_wraps(ctx, mode):
+    """30,000 distinct keys whose home slots all lie in the last 16,384-slot
+    region of a 2^23-slot table (plus 100,000 random keys and duplicates):
+    the region overflows, so its rows' probe runs cross the table's end and
+    wrap into the first region.  The shared-memory region build sets those
+    rows aside and inserts them where linear probing over the whole table
+    puts them; probes equal the oracle's, as with the L2 region build."""
+    rng = np.random.default_rng(41)
+    cap = 1 << 23
+    lo = ((cap - 16384) << 32) // cap + 1  # hashes whose home slot is in the last region
+    hs = rng.choice(np.arange(lo, 1 << 32, 97, dtype=np.int64), 30_000, replace=False)
+    hot = np.array([_key_of_hash(int(h)) for h in hs], dtype=np.uint32).view(np.int32)
+    assert all(((_hash32(int(k) & _M32) * cap) >> 32) >= cap - 16384 for k in hot[:100].view(np.uint32))
+    rk = np.concatenate([hot, rng.integers(-2**31 + 1, 2**31, 100_000).astype(np.int32), hot[:5000]])
+    rk = rk[rk != np.iinfo(np.int32).min]
+    rp = np.arange(len(rk), dtype=np.int32) * 3 - 7
+    sk = np.concatenate([rk[::3], rng.integers(-2**31 + 1, 2**31, 50_000).astype(np.int32)])
+    L, h = _lib.lib, ctx.handle
+    table = torch.empty(cap, dtype=torch.int64, device="cuda")
+    drk, drp, dsk = dev(rk), dev(rp), dev(sk)
+    ctx.set_tuning(_lib.TUNE_JOIN_BUILD, mode)
+    try:
+        _lib.check(L.olap_hashjoin_build(h, drk.data_ptr(), drp.data_ptr(), len(rk), table.data_ptr(), cap), h)
+    finally:
+        ctx.set_tuning(_lib.TUNE_JOIN_BUILD, 0)
+    s_, m_ = torch.zeros(1, dtype=torch.int64, device="cuda"), torch.zeros(1, dtype=torch.int64, device="cuda")
+    _lib.check(L.olap_hashjoin_probe_filtered(h, table.data_ptr(), cap, None, 0, dsk.data_ptr(), len(sk),
+                                              s_.data_ptr(), m_.data_ptr(), None, None), h)
+    assert (int(s_.item()), int(m_.item())) == oracle.hashjoin(rk, rp, sk)
+
+
+@pytest.mark.parametrize("mode", [0, 2, 3])
 def test_hash_join_region_build(ctx, mode):
     """A build side whose table is larger than one 32 MB region (2^22 rows:
-    about 8.4M slots, 67 MB) is built region by region by default (mode 0) or
-    directly (OLAP_TUNE_JOIN_BUILD = 2): duplicate keys keep their last row,
-    the reserved key is counted, and probes equal the oracle's either way."""
+    about 8.4M slots, 67 MB) is built by default 128 KB region by 128 KB
+    region in shared memory (mode 0), directly (OLAP_TUNE_JOIN_BUILD = 2) or
+    32 MB region by 32 MB region in L2 (3): duplicate keys keep their last
+    row, the reserved key is counted, and probes equal the oracle's."""
     rng = np.random.default_rng(31)
     n = 1 << 22
     rk = rng.integers(-(1 << 23), 1 << 23, n).astype(np.int32)  # about 1/4 duplicates, negatives

@@ -512,8 +512,8 @@ def operators_result(a) -> dict:
     bloom = torch.empty(words, dtype=torch.int64, device="cuda")
 
     def build_fn():
-        _lib.check(L.olap_hashjoin_build(h, _ptr(bkeys), _ptr(bpay), nb, _ptr(table), cap), h)
-        _lib.check(L.olap_hashjoin_build_filter(h, _ptr(bkeys), nb, _ptr(bloom), words), h)
+        _lib.check(L.olap_hashjoin_build_filtered(h, _ptr(bkeys), _ptr(bpay), nb, _ptr(table), cap, _ptr(bloom),
+                                                  words), h)
     ms = timed(build_fn, reps=3)
     res.append(entry("hash join build (2^24 unique keys; table + Bloom filter)", ms, 16 * nb, True, build_rows=nb,
                      capacity=cap, filter_bytes=8 * words))

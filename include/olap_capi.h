@@ -361,13 +361,15 @@ OLAP_API int64_t olap_hashtable_capacity(int64_t n_build);
 /* build(relation_t*, std::unordered_map&) (join/test_join_option.cpp:44-50);
  * synchronous; OLAP_ERR_CAPACITY if the table fills.  A table above 32 MB is
  * built region by region: up to 2^27 slots the rows are grouped by the
- * 16,384-slot (128 KB) region of their home slot and each region is built in
- * shared memory and written once, payloads in place (a row whose probe run
- * leaves its region is inserted afterwards from the next region on, where
- * linear probing over the whole table puts it); above, by 32 MB regions
- * inserted one at a time in L2.  Scratch: 16 (8 above 2^27 slots) bytes per
- * build row from the context's grow-only buffer.  OLAP_TUNE_JOIN_BUILD
- * chooses the way (see its values). */
+ * 16,384-slot (128 KB) region of their home slot (one scatter pass, each
+ * tuple carrying its payload) and each region is built in shared memory and
+ * written once,
+ * payloads in place (a row whose probe run leaves its region is inserted
+ * afterwards from the next region on, where linear probing over the whole
+ * table puts it); above, by 32 MB regions inserted one at a time in L2.
+ * Scratch: 20 (8 above 2^27 slots) bytes per build row from the context's
+ * grow-only buffer.  OLAP_TUNE_JOIN_BUILD chooses the way (see its
+ * values). */
 OLAP_API int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* payload,
                                  int64_t n, uint64_t* table, int64_t capacity);
 /* probe(relation_t*, std::unordered_map&) (join:90-96): *d_sum = SUM of the
@@ -387,6 +389,15 @@ OLAP_API int olap_hashjoin_probe(olap_ctx* ctx, const uint64_t* table, int64_t c
 OLAP_API int64_t olap_hashjoin_filter_words(int64_t n_build);
 OLAP_API int olap_hashjoin_build_filter(olap_ctx* ctx, const int32_t* keys, int64_t n, uint64_t* filter,
                                         int64_t words);
+/* olap_hashjoin_build and olap_hashjoin_build_filter of the same keys in one
+ * call, with the same table and filter as the two calls give.  The filter
+ * word of a key is the top bits of the hash that places it in the table, so
+ * on the shared-memory region build each region's block sets the filter
+ * bits of its own keys and stores its run of words whole (no separate pass
+ * over the keys, no global atomic per key).  Synchronous, like
+ * olap_hashjoin_build. */
+OLAP_API int olap_hashjoin_build_filtered(olap_ctx* ctx, const int32_t* keys, const int32_t* payload, int64_t n,
+                                          uint64_t* table, int64_t capacity, uint64_t* filter, int64_t words);
 /* olap_hashjoin_probe through the filter built from the same build keys
  * (filter NULL: no filter); the same results. */
 OLAP_API int olap_hashjoin_probe_filtered(olap_ctx* ctx, const uint64_t* table, int64_t capacity,

@@ -481,8 +481,8 @@ inline void build(Rel* R, std::unordered_map<int, int>& hashtable) {
   int32_t* dk = detail::put(0, R->key, n);
   int32_t* dp = detail::put(1, R->payload, n);
   if (!dk || !dp) return;
-  if (detail::ok(olap_hashjoin_build(ctx, dk, dp, static_cast<int64_t>(n), static_cast<uint64_t*>(tb.dev), cap)))
-    detail::ok(olap_hashjoin_build_filter(ctx, dk, static_cast<int64_t>(n), static_cast<uint64_t*>(tb.filter), words));
+  detail::ok(olap_hashjoin_build_filtered(ctx, dk, dp, static_cast<int64_t>(n), static_cast<uint64_t*>(tb.dev), cap,
+                                          static_cast<uint64_t*>(tb.filter), words));
 }
 
 /// probe(relation_t*, std::unordered_map<int,int>&) (test_join_option.cpp:90):

@@ -162,6 +162,7 @@ def _load() -> C.CDLL:
         "olap_hashjoin_probe": (C.c_int, [vp, vp, i64, vp, i64, vp, vp, vp, vp]),
         "olap_hashjoin_filter_words": (i64, [i64]),
         "olap_hashjoin_build_filter": (C.c_int, [vp, vp, i64, vp, i64]),
+        "olap_hashjoin_build_filtered": (C.c_int, [vp, vp, vp, i64, vp, i64, vp, i64]),
         "olap_hashjoin_probe_filtered": (C.c_int, [vp, vp, i64, vp, i64, vp, i64, vp, vp, vp, vp]),
         "olap_vecjoin_build": (C.c_int, [vp, vp, vp, i64, vp, i64]),
         "olap_vecjoin_probe": (C.c_int, [vp, vp, i64, vp, i64, vp]),

@@ -346,11 +346,12 @@ __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const l
 
 // ---- region build in shared memory ------------------------------------------
 // For tables up to 2^27 slots the rows are grouped by the 16,384-slot region
-// (128 KB) of their home slot, and one block builds each region in shared
-// memory: it inserts the region's rows with shared-memory CAS, then writes
-// the whole region (empty slots too) with the payloads already in place, so
-// the table needs no separate fill or finish pass and every slot crosses
-// DRAM once.  A row whose probe run would leave its region (every slot from
+// (128 KB of table) of their home slot, each tuple with its payload beside
+// it, and one block builds each region in shared memory: it inserts the
+// region's rows with shared-memory atomics, then writes the whole region
+// (empty slots too) with the payloads already in place, so the table needs no
+// separate fill or finish pass, every slot crosses DRAM once and no payload
+// is read at random.  A row whose probe run would leave its region (every slot from
 // its home to the region's end taken) is set aside and inserted afterwards
 // into the finished table from the next region's first slot on, exactly where
 // linear probing over the whole table would have put it.
@@ -359,9 +360,37 @@ constexpr int kSmemRegionShift = 14;
 constexpr int64_t kSmemRegionMaxRegions = 8192;
 constexpr int kSmemRegionThreads = 1024;
 
+// Home slot for a table of at most 2^32 - 1 slots (every table this build
+// path makes): the same value as home_slot, one 32-bit multiply-high.
+__device__ __forceinline__ uint32_t home32(uint32_t k, uint32_t cap32) { return __umulhi(hash32(k), cap32); }
+
+// Row offsets of a thread's 8 rows within a tile of kSmemTileRows rows:
+// 4 * tid + {0..3} and 4 * (tid + kSmemRegionThreads) + {0..3}, so the 16-byte
+// loads of a warp are coalesced.  The kernels below run kSmemRegionThreads
+// threads per block.
+constexpr int kSmemTileRows = 8 * kSmemRegionThreads;
+
+__device__ __forceinline__ int tile_off(int u) {
+  return 4 * static_cast<int>(threadIdx.x) + (u >> 2) * 4 * kSmemRegionThreads + (u & 3);
+}
+
+// A thread's 8 values of a tile starting at row r0; rows at or past e come
+// back as INT32_MIN.
+__device__ __forceinline__ void tile_load8(const int32_t* __restrict__ col, int64_t r0, int64_t e, bool vec,
+                                           int32_t (&x)[8]) {
+  int32_t a[4], b[4];
+  build_keys4(col, r0 + tile_off(0), e, vec, a);
+  build_keys4(col, r0 + tile_off(4), e, vec, b);
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    x[u] = a[u];
+    x[u + 4] = b[u];
+  }
+}
+
 // Region counts: per block in shared memory, then one global add per region.
-__global__ void __launch_bounds__(kBuildPartThreads) smem_region_count_kernel(
-    const int32_t* __restrict__ keys, int64_t n, int64_t per, uint64_t cap, int n_regions, int vec,
+__global__ void __launch_bounds__(kSmemRegionThreads) smem_region_count_kernel(
+    const int32_t* __restrict__ keys, int64_t n, int64_t per, uint32_t cap32, int n_regions, int vec,
     unsigned int* __restrict__ counts, unsigned long long* range_err) {
   extern __shared__ unsigned int s_rc[];
   for (int p = threadIdx.x; p < n_regions; p += blockDim.x) s_rc[p] = 0;
@@ -369,17 +398,18 @@ __global__ void __launch_bounds__(kBuildPartThreads) smem_region_count_kernel(
   const int64_t b = static_cast<int64_t>(blockIdx.x) * per;
   const int64_t e = b + per < n ? b + per : n;
   unsigned int bad = 0;
-  for (int64_t r = b + 4 * static_cast<int64_t>(threadIdx.x); r < e; r += 4 * static_cast<int64_t>(blockDim.x)) {
-    int32_t k[4];
-    build_keys4(keys, r, e, vec, k);
+  for (int64_t r0 = b; r0 < e; r0 += kSmemTileRows) {
+    const int lim = e - r0 < kSmemTileRows ? static_cast<int>(e - r0) : kSmemTileRows;
+    int32_t k[8];
+    tile_load8(keys, r0, e, vec, k);
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if (r + u >= e) continue;
+    for (int u = 0; u < 8; ++u) {
+      if (tile_off(u) >= lim) continue;
       if (k[u] == INT32_MIN) {
         ++bad;
         continue;
       }
-      atomicAdd(&s_rc[home_slot(static_cast<uint32_t>(k[u]), cap) >> kSmemRegionShift], 1u);
+      atomicAdd(&s_rc[home32(static_cast<uint32_t>(k[u]), cap32) >> kSmemRegionShift], 1u);
     }
   }
   if (bad) atomicAdd(range_err, static_cast<unsigned long long>(bad));
@@ -415,117 +445,307 @@ __global__ void __launch_bounds__(1024) smem_region_scan_kernel(const unsigned i
   if (threadIdx.x == blockDim.x - 1) begin[n_regions] = s_run[threadIdx.x];
 }
 
-// Scatter of the (key << 32 | row) tuples by region: a block counts its rows
-// per region, claims one run per region from the global cursors, then writes
-// its rows into its runs (its keys are read twice, the second time from L2).
-__global__ void __launch_bounds__(kBuildPartThreads) smem_region_scatter_kernel(
-    const int32_t* __restrict__ keys, int64_t n, int64_t per, uint64_t cap, int n_regions, int vec,
-    unsigned long long* __restrict__ cursor, uint64_t* __restrict__ tuples) {
-  extern __shared__ unsigned long long s_rs[];
-  unsigned int* s_cnt = reinterpret_cast<unsigned int*>(s_rs + n_regions);
-  for (int p = threadIdx.x; p < n_regions; p += blockDim.x) s_cnt[p] = 0;
-  __syncthreads();
+// Asks L2 to fetch the 16-byte aligned part of [p, p + bytes) ahead of the
+// loads that will read it (a bulk prefetch has no destination registers).
+__device__ __forceinline__ void prefetch_l2_range(const void* p, uint64_t bytes) {
+  const uint64_t a = (reinterpret_cast<uint64_t>(p) + 15) & ~uint64_t(15);
+  const uint64_t z = (reinterpret_cast<uint64_t>(p) + bytes) & ~uint64_t(15);
+  if (z > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(static_cast<uint32_t>(z - a)) : "memory");
+}
+
+// Scatter of the (key << 32 | row) tuples and their payloads by region (rows
+// with the key INT32_MIN are range errors and dropped).  A block takes its
+// rows a tile of 8,192 at a time: counting-sorts the tile by region in shared
+// memory, claims one piece of each region's output per tile from the global
+// cursors, and writes each region's rows as one contiguous piece.  Because
+// every tile claims afresh, a region's output fills from its start in the
+// order the tiles finish, so the piece that completes a partly written
+// 32-byte sector follows within microseconds and L2 merges the two: DRAM
+// sees whole sectors although a tile holds only about four rows per region.
+// (One claim per block and region made at the start, filled tile by tile,
+// left each sector partly written for the whole pass, and DRAM took twice
+// the bytes as read-modify-writes; two passes, into 256 groups of regions
+// and then into regions, wrote long pieces but cost a second pass; blocks of
+// 512 threads, two per SM, waited longer on their claims.)  The next tile is
+// prefetched into L2 while the current one is sorted and written.
+__global__ void __launch_bounds__(kSmemRegionThreads, 1) smem_region_scatter_kernel(
+    const int32_t* __restrict__ keys, const int32_t* __restrict__ payload, int64_t n, uint32_t cap32, int n_regions,
+    int vec_k, int vec_p, unsigned long long* __restrict__ cursor, uint64_t* __restrict__ out_tup,
+    int32_t* __restrict__ out_pay) {
+  constexpr int kTile = kSmemTileRows;
+  // the sorted tile (tuples, payloads, regions), then per region its tile
+  // offset, its destination base and its tile count
+  extern __shared__ unsigned long long s_stage[];
+  int32_t* s_pay = reinterpret_cast<int32_t*>(s_stage + kTile);
+  uint16_t* s_reg = reinterpret_cast<uint16_t*>(s_pay + kTile);
+  unsigned int* s_off = reinterpret_cast<unsigned int*>(s_reg + kTile);
+  unsigned int* s_dst = s_off + n_regions;
+  unsigned int* s_cnt = s_dst + n_regions;
+  __shared__ unsigned int s_wsum[33];
+  const int64_t per = ((n + gridDim.x - 1) / gridDim.x + 3) & ~int64_t(3);
   const int64_t b = static_cast<int64_t>(blockIdx.x) * per;
   const int64_t e = b + per < n ? b + per : n;
-  const int64_t step = 4 * static_cast<int64_t>(blockDim.x);
-  for (int64_t r = b + 4 * static_cast<int64_t>(threadIdx.x); r < e; r += step) {
-    int32_t k[4];
-    build_keys4(keys, r, e, vec, k);
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (r + u < e && k[u] != INT32_MIN)
-        atomicAdd(&s_cnt[home_slot(static_cast<uint32_t>(k[u]), cap) >> kSmemRegionShift], 1u);
-  }
+  for (int p = threadIdx.x; p < n_regions; p += kSmemRegionThreads) s_cnt[p] = 0;
+  const int cpt = (n_regions + kSmemRegionThreads - 1) / kSmemRegionThreads;  // regions per thread, at most 8
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  auto prefetch_tile = [&](int64_t r0) {
+    if (threadIdx.x != 0 || r0 >= e) return;
+    const int64_t m = e - r0 < kTile ? e - r0 : kTile;
+    prefetch_l2_range(keys + r0, 4 * m);
+    prefetch_l2_range(payload + r0, 4 * m);
+  };
+  prefetch_tile(b);
   __syncthreads();
-  for (int p = threadIdx.x; p < n_regions; p += blockDim.x) {
-    const unsigned int c = s_cnt[p];
-    s_rs[p] = c ? atomicAdd(&cursor[p], static_cast<unsigned long long>(c)) : 0ull;
-    s_cnt[p] = 0;
-  }
-  __syncthreads();
-  for (int64_t r = b + 4 * static_cast<int64_t>(threadIdx.x); r < e; r += step) {
-    int32_t k[4];
-    build_keys4(keys, r, e, vec, k);
+  for (int64_t r0 = b; r0 < e; r0 += kTile) {
+    const int lim = e - r0 < kTile ? static_cast<int>(e - r0) : kTile;
+    int32_t k[8], v[8];
+    tile_load8(keys, r0, e, vec_k, k);
+    tile_load8(payload, r0, e, vec_p, v);
+    prefetch_tile(r0 + kTile);
+    uint32_t slot[8];  // region << 14 | rank in the tile, or ~0u for no row
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if (r + u >= e || k[u] == INT32_MIN) continue;
-      const uint64_t reg = home_slot(static_cast<uint32_t>(k[u]), cap) >> kSmemRegionShift;
-      const unsigned int at = atomicAdd(&s_cnt[reg], 1u);
-      tuples[s_rs[reg] + at] = (static_cast<uint64_t>(static_cast<uint32_t>(k[u])) << 32) |
-                               static_cast<uint32_t>(r + u);
+    for (int u = 0; u < 8; ++u) {
+      slot[u] = ~0u;
+      if (tile_off(u) < lim && k[u] != INT32_MIN) {
+        const uint32_t reg = home32(static_cast<uint32_t>(k[u]), cap32) >> kSmemRegionShift;
+        slot[u] = (reg << 14) | atomicAdd(&s_cnt[reg], 1u);
+      }
     }
+    __syncthreads();
+    // exclusive scan of the tile counts over the regions, one claim per
+    // non-empty region (its result is first needed after the rows are
+    // placed, so the atomics' round trip overlaps the placing), and the
+    // counts cleared for the next tile
+    const int lo = threadIdx.x * cpt;
+    unsigned int sum = 0;
+    for (int j = 0; j < cpt && lo + j < n_regions; ++j) sum += s_cnt[lo + j];
+    unsigned int x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      const unsigned int w = s_wsum[lane];
+      unsigned int z = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, z, o);
+        if (lane >= o) z += y;
+      }
+      s_wsum[lane] = z - w;
+      if (lane == 31) s_wsum[32] = z;
+    }
+    __syncthreads();
+    unsigned int run = s_wsum[warp] + x - sum;
+    unsigned int claim[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int p = lo + j;
+      claim[j] = 0;
+      if (j < cpt && p < n_regions) {
+        const unsigned int c = s_cnt[p];
+        if (c) claim[j] = static_cast<unsigned int>(atomicAdd(&cursor[p], static_cast<unsigned long long>(c)));
+        s_off[p] = run;
+        s_cnt[p] = 0;
+        run += c;
+      }
+    }
+    __syncthreads();
+    const uint32_t row0 = static_cast<uint32_t>(r0);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      if (slot[u] == ~0u) continue;
+      const unsigned int at = s_off[slot[u] >> 14] + (slot[u] & 16383u);
+      s_stage[at] = (static_cast<uint64_t>(static_cast<uint32_t>(k[u])) << 32) |
+                    (row0 + static_cast<uint32_t>(tile_off(u)));
+      s_pay[at] = v[u];
+      s_reg[at] = static_cast<uint16_t>(slot[u] >> 14);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (j < cpt && lo + j < n_regions) s_dst[lo + j] = claim[j] - s_off[lo + j];
+    __syncthreads();
+    const unsigned int total = s_wsum[32];
+    for (unsigned int i = threadIdx.x; i < total; i += kSmemRegionThreads) {
+      const unsigned int d = s_dst[s_reg[i]] + i;
+      out_tup[d] = s_stage[i];
+      out_pay[d] = s_pay[i];
+    }
+    __syncthreads();
   }
 }
 
-// One block per region: insert its rows in a shared-memory copy of the
-// region, set aside the rows whose run would leave it, then write the region
-// with (key, payload) in every taken slot and the empty marker elsewhere.
-// The payload reads are random over the payload column and marked
-// evict-last, so the column stays in L2 across the regions.
-__global__ void __launch_bounds__(kSmemRegionThreads) smem_region_build_kernel(
-    const uint64_t* __restrict__ tuples, const long long* __restrict__ begin, uint64_t* __restrict__ slots,
-    uint64_t cap, const int32_t* __restrict__ payload, uint64_t* __restrict__ spill,
-    unsigned long long* __restrict__ n_spill) {
-  extern __shared__ unsigned long long s_slot[];
-  const uint64_t base = static_cast<uint64_t>(blockIdx.x) << kSmemRegionShift;
-  const uint32_t len = static_cast<uint32_t>(cap - base < kSmemRegionSlots ? cap - base : kSmemRegionSlots);
-  for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) s_slot[i] = kEmptySlot;
-  __syncthreads();
+// One block per region: insert its rows into a shared-memory copy of the
+// region (32-bit CAS on the key, 32-bit atomicMax on the row, so the last
+// duplicate row wins as in the sequential build; the payload rides with the
+// row), set aside the rows whose run would leave the region, then write the
+// region with (key, payload) in every taken slot and the empty marker
+// elsewhere.  Payloads of duplicate keys are settled by a second pass over
+// the region's rows, run only when the region met a duplicate.
+//
+// With a filter (filter != null), the block also sets the Bloom bits of its
+// rows (set-aside rows included): the filter word of a key is the top bits
+// of the same hash that places it in the table, so a region's keys fall in
+// one run of at most kSmemFilterWords words, kept in shared memory (low and
+// high halves apart, for 32-bit atomics) and stored whole; the run's first
+// and last words may be shared with the neighbouring regions and are ORed
+// into the (zeroed) filter instead.
+constexpr uint32_t kEmptyKey = 0x80000000u;  // INT32_MIN, the reserved empty key
+constexpr int kSmemFilterWords = 2064;  // a region's run with olap_hashjoin_filter_words is at most 2050
+
+__global__ void __launch_bounds__(kSmemRegionThreads, 1) smem_region_build_kernel(
+    const uint64_t* __restrict__ tuples, const int32_t* __restrict__ pays, const long long* __restrict__ begin,
+    uint64_t* __restrict__ slots, uint32_t cap32, uint64_t* __restrict__ spill, unsigned long long* __restrict__ n_spill,
+    uint64_t* __restrict__ filter, int fshift) {
+  extern __shared__ uint32_t s_key[];
+  uint32_t* s_row = s_key + kSmemRegionSlots;
+  int32_t* s_val = reinterpret_cast<int32_t*>(s_row + kSmemRegionSlots);
+  uint32_t* s_flo = reinterpret_cast<uint32_t*>(s_val + kSmemRegionSlots);
+  uint32_t* s_fhi = s_flo + kSmemFilterWords;
+  __shared__ int s_dup;
+  const uint32_t base = blockIdx.x << kSmemRegionShift;
+  const uint32_t len = cap32 - base < kSmemRegionSlots ? cap32 - base : kSmemRegionSlots;
+  // hashes whose home slot lies in this region: [h_lo, h_hi)
+  const uint64_t h_lo = ((static_cast<uint64_t>(blockIdx.x) << (32 + kSmemRegionShift)) + cap32 - 1) / cap32;
+  const uint64_t h_hi = (((static_cast<uint64_t>(blockIdx.x) + 1) << (32 + kSmemRegionShift)) + cap32 - 1) / cap32;
+  const uint32_t w_lo = fshift >= 32 ? 0u : static_cast<uint32_t>(h_lo >> fshift);
+  const uint32_t w_hi = fshift >= 32 ? 0u : static_cast<uint32_t>(((h_hi < (uint64_t(1) << 32) ? h_hi : (uint64_t(1) << 32)) - 1) >> fshift);
+  const uint32_t n_words = filter ? w_hi - w_lo + 1 : 0;
+  for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+    s_key[i] = kEmptyKey;
+    s_row[i] = 0;
+  }
+  for (uint32_t i = threadIdx.x; i < n_words; i += blockDim.x) {
+    s_flo[i] = 0;
+    s_fhi[i] = 0;
+  }
+  if (threadIdx.x == 0) s_dup = 0;
   const int64_t b = begin[blockIdx.x], e = begin[blockIdx.x + 1];
-  for (int64_t t = b + threadIdx.x; t < e; t += blockDim.x) {
-    const unsigned long long mine = tuples[t];
-    const uint32_t k = static_cast<uint32_t>(mine >> 32);
-    bool done = false;
-    for (uint32_t j = static_cast<uint32_t>(home_slot(k, cap) - base); j < len && !done; ++j) {
-      const unsigned long long prev = atomicCAS(&s_slot[j], kEmptySlot, mine);
-      if (prev == kEmptySlot) {
-        done = true;
-      } else if ((prev >> 32) == k) {
-        atomicMax(&s_slot[j], mine);  // same key: keeps the largest row
-        done = true;
-      }
+  __syncthreads();
+  const int64_t chunk = 8 * static_cast<int64_t>(blockDim.x);
+  for (int64_t t0 = b; t0 < e; t0 += chunk) {
+    uint64_t tu[8];
+    int32_t pv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t t = t0 + threadIdx.x + u * static_cast<int64_t>(blockDim.x);
+      tu[u] = t < e ? tuples[t] : 0ull;
+      pv[u] = t < e ? pays[t] : 0;
     }
-    if (!done) spill[atomicAdd(n_spill, 1ull)] = mine;  // the run reached the region's end
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      if (t0 + threadIdx.x + u * static_cast<int64_t>(blockDim.x) >= e) continue;
+      const uint32_t k = static_cast<uint32_t>(tu[u] >> 32), row = static_cast<uint32_t>(tu[u]);
+      const uint32_t h = hash32(k);
+      if (filter) {
+        const uint32_t w = (fshift >= 32 ? 0u : h >> fshift) - w_lo;
+        const uint64_t bits = bloom_bits(k);
+        if (static_cast<uint32_t>(bits)) atomicOr(&s_flo[w], static_cast<uint32_t>(bits));
+        if (bits >> 32) atomicOr(&s_fhi[w], static_cast<uint32_t>(bits >> 32));
+      }
+      bool done = false;
+      for (uint32_t j = __umulhi(h, cap32) - base; j < len; ++j) {
+        const uint32_t prev = atomicCAS(&s_key[j], kEmptyKey, k);
+        if (prev == kEmptyKey) {
+          atomicMax(&s_row[j], row);
+          s_val[j] = pv[u];
+          done = true;
+          break;
+        }
+        if (prev == k) {
+          atomicMax(&s_row[j], row);
+          s_dup = 1;
+          done = true;
+          break;
+        }
+      }
+      if (!done) spill[atomicAdd(n_spill, 1ull)] = tu[u];  // the run reached the region's end
+    }
   }
   __syncthreads();
-  const uint64_t keep = policy_evict_last();
+  if (s_dup) {  // a key met twice: the payload of its largest row
+    for (int64_t t = b + threadIdx.x; t < e; t += blockDim.x) {
+      const uint64_t mine = tuples[t];
+      const uint32_t k = static_cast<uint32_t>(mine >> 32), row = static_cast<uint32_t>(mine);
+      for (uint32_t j = home32(k, cap32) - base; j < len; ++j) {
+        if (s_key[j] != k) continue;
+        if (s_row[j] == row) s_val[j] = pays[t];
+        break;
+      }
+    }
+    __syncthreads();
+  }
   for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
-    const uint64_t v = s_slot[i];
-    const bool full = v != kEmptySlot;
-    const int32_t pay = ld_probe_s32(payload + (full ? static_cast<uint32_t>(v) : 0u), keep);
-    slots[base + i] = full ? ((v & 0xffffffff00000000ull) | static_cast<uint32_t>(pay)) : kEmptySlot;
+    const uint32_t k = s_key[i];
+    slots[base + i] = k != kEmptyKey ? (static_cast<uint64_t>(k) << 32) | static_cast<uint32_t>(s_val[i]) : kEmptySlot;
+  }
+  for (uint32_t i = threadIdx.x; i < n_words; i += blockDim.x) {
+    const uint64_t v = (static_cast<uint64_t>(s_fhi[i]) << 32) | s_flo[i];
+    if (i == 0 || i == n_words - 1) {
+      if (v) atomicOr(reinterpret_cast<unsigned long long*>(filter + w_lo + i), static_cast<unsigned long long>(v));
+    } else {
+      filter[w_lo + i] = v;
+    }
   }
 }
 
 // The set-aside rows, into the finished table from the first slot after
 // their region on (linear probing across regions, wrapping at the end); the
 // slots they take are listed for the payload pass.  A key already there (an
-// earlier set-aside copy) keeps its largest row.
+// earlier set-aside copy) keeps its largest row.  One warp per row: the warp
+// reads 32 consecutive slots at a time, takes the first that is empty or
+// holds its key (ballot) with one CAS, and on a lost race reads on from
+// there, so a row costs one or two round trips instead of one CAS per slot.
 __global__ void smem_region_spill_kernel(const uint64_t* __restrict__ spill, const unsigned long long* n_spill,
                                          uint64_t* __restrict__ slots, uint64_t cap, uint64_t* __restrict__ taken,
                                          unsigned long long* __restrict__ n_taken, unsigned long long* overflow) {
   const int64_t n = static_cast<int64_t>(*n_spill);
-  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+  const int lane = threadIdx.x & 31;
+  const int64_t n_warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < n; i += n_warps) {
     const unsigned long long mine = spill[i];
     const uint32_t k = static_cast<uint32_t>(mine >> 32);
     const uint64_t next = ((home_slot(k, cap) >> kSmemRegionShift) + 1) << kSmemRegionShift;
-    uint64_t h = next >= cap ? 0 : next;
+    uint64_t h = next >= cap ? 0 : next;  // first slot of the window
+    uint64_t seen = 0;
     bool done = false;
-    for (uint64_t step = 0; step < cap && !done; ++step) {
-      unsigned long long* s = reinterpret_cast<unsigned long long*>(slots + h);
-      const unsigned long long prev = atomicCAS(s, kEmptySlot, mine);
-      if (prev == kEmptySlot) {
-        taken[atomicAdd(n_taken, 1ull)] = h;
+    while (!done && seen < cap) {
+      uint64_t at = h + lane;
+      if (at >= cap) at -= cap;
+      const uint64_t v = *reinterpret_cast<volatile const uint64_t*>(slots + at);
+      const uint32_t vk = static_cast<uint32_t>(v >> 32);
+      const unsigned int m = __ballot_sync(0xffffffffu, vk == kEmptyKey || vk == k);
+      if (m == 0) {
+        h = h + 32 >= cap ? h + 32 - cap : h + 32;
+        seen += 32;
+        continue;
+      }
+      const int f = __ffs(m) - 1;
+      int ok = 0;
+      if (lane == f) {
+        unsigned long long* sl = reinterpret_cast<unsigned long long*>(slots + at);
+        const unsigned long long prev = atomicCAS(sl, kEmptySlot, mine);
+        if (prev == kEmptySlot) {
+          taken[atomicAdd(n_taken, 1ull)] = at;
+          ok = 1;
+        } else if ((prev >> 32) == k) {
+          atomicMax(sl, mine);
+          ok = 1;
+        }
+      }
+      ok = __shfl_sync(0xffffffffu, ok, f);
+      if (ok) {
         done = true;
-      } else if ((prev >> 32) == k) {
-        atomicMax(s, mine);
-        done = true;
-      } else {
-        h = next_slot(h, cap);
+      } else {  // another key took the slot first: read on after it
+        const uint64_t after = h + f + 1;
+        h = after >= cap ? after - cap : after;
+        seen += f + 1;
       }
     }
-    if (!done) atomicAdd(overflow, 1ull);
+    if (!done && lane == 0) atomicAdd(overflow, 1ull);
   }
 }
 
@@ -851,16 +1071,31 @@ int64_t olap_hashtable_capacity(int64_t n_build) {
   return cap < 8 ? 8 : cap;
 }
 
-int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* payload, int64_t n,
-                        uint64_t* table, int64_t capacity) {
-  if (!ctx) return OLAP_ERR_INVALID;
-  std::lock_guard<std::mutex> lk(ctx->mu);
+}  // extern "C"
+
+namespace olap {
+namespace {
+
+// The table build, and with `filter` the Bloom filter of the same keys; the
+// caller holds the context lock.
+int hashjoin_build_locked(olap_ctx* ctx, const int32_t* keys, const int32_t* payload, int64_t n, uint64_t* table,
+                          int64_t capacity, uint64_t* filter, int64_t words) {
   OLAP_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   OLAP_REQUIRE(ctx, n >= 0 && n <= UINT32_MAX - 1, "n must be in [0, 2^32-1)");
   OLAP_REQUIRE(ctx, capacity >= 8 && capacity % 8 == 0 && capacity <= (int64_t(1) << 32) && capacity > n,
                "capacity must be a multiple of 8 in (n, 2^32] (see olap_hashtable_capacity)");
   OLAP_REQUIRE(ctx, table && (olap::al16(table)), "table must be 16-byte aligned");
   OLAP_REQUIRE(ctx, n == 0 || (keys && payload), "null keys or payload");
+  int fshift = 32;
+  if (filter) {
+    OLAP_REQUIRE(ctx, words >= 1 && words <= (int64_t(1) << 31) && (words & (words - 1)) == 0 &&
+                          (reinterpret_cast<uintptr_t>(filter) & 7) == 0,
+                 "filter must hold a power of two of words (see olap_hashjoin_filter_words)");
+    int lg = 0;
+    while ((int64_t(1) << lg) < words) ++lg;
+    fshift = 32 - lg;
+    OLAP_CUDA_TRY(ctx, cudaMemsetAsync(filter, 0, sizeof(uint64_t) * words, ctx->stream));
+  }
   olap::Arena ar(ctx);
   unsigned long long* overflow = ar.take<unsigned long long>(1);
   if (!overflow) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "scratch arena exhausted");
@@ -874,47 +1109,58 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
   const bool smem_regions = big && build_knob != 3 &&
                             capacity <= olap::kSmemRegionMaxRegions * olap::kSmemRegionSlots;
   const bool partitioned = big && !smem_regions;
+  // the region blocks set the filter bits too when a region's keys fall in
+  // at most kSmemFilterWords filter words
+  const uint64_t region_hashes = ((uint64_t(1) << (32 + olap::kSmemRegionShift)) + capacity - 1) / capacity;
+  const bool fused_filter = filter && smem_regions && (region_hashes >> fshift) + 2 <= olap::kSmemFilterWords;
   if (n && smem_regions) {
     const int P = static_cast<int>((capacity + olap::kSmemRegionSlots - 1) / olap::kSmemRegionSlots);
-    const int nb = ctx->sm_count * 2;
+    const int nb = ctx->sm_count;
     const int64_t per = ((n + nb - 1) / nb + 3) & ~int64_t(3);
-    const int vec = olap::al16(keys);
+    const int vec_k = olap::al16(keys), vec_p = olap::al16(payload);
     const uint64_t cap = static_cast<uint64_t>(capacity);
-    // counts[P] | n_spill | n_taken (zeroed together), begin[P+1], cursor[P], tuples[n] (then the taken
-    // slots), spill[n]
-    const size_t cnt_bytes = (sizeof(unsigned int) * P + 2 * sizeof(unsigned long long) + 255) & ~size_t(255);
+    const uint32_t cap32 = static_cast<uint32_t>(capacity);  // at most 2^27 here
+    // counts[P] | n_spill | n_taken (zeroed together), begin[P+1], cursor[P], region-ordered tuples[n] (then
+    // the taken slots) and payloads[n], set-aside rows[n]
+    auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t nn = static_cast<size_t>(n);
+    const size_t cnt_bytes = up(sizeof(unsigned int) * P + 2 * sizeof(unsigned long long));
     const size_t begin_off = cnt_bytes;
-    const size_t cursor_off = (begin_off + sizeof(long long) * (P + 1) + 255) & ~size_t(255);
-    const size_t tup_off = (cursor_off + sizeof(unsigned long long) * P + 255) & ~size_t(255);
-    const size_t spill_off = (tup_off + sizeof(uint64_t) * static_cast<size_t>(n) + 255) & ~size_t(255);
-    char* mem = olap::big_scratch(ctx, spill_off + sizeof(uint64_t) * static_cast<size_t>(n));
+    const size_t cur_off = up(begin_off + sizeof(long long) * (P + 1));
+    const size_t tup_off = up(cur_off + sizeof(unsigned long long) * P);
+    const size_t pay_off = up(tup_off + sizeof(uint64_t) * nn);
+    const size_t spill_off = up(pay_off + sizeof(int32_t) * nn);
+    char* mem = olap::big_scratch(ctx, spill_off + sizeof(uint64_t) * nn);
     if (!mem) return olap::set_error(ctx, OLAP_ERR_NOMEM, "device memory for the build regions");
     auto* counts = reinterpret_cast<unsigned int*>(mem);
     auto* n_spill = reinterpret_cast<unsigned long long*>(mem + ((sizeof(unsigned int) * P + 7) & ~size_t(7)));
     auto* n_taken = n_spill + 1;
     auto* begin = reinterpret_cast<long long*>(mem + begin_off);
-    auto* cursor = reinterpret_cast<unsigned long long*>(mem + cursor_off);
+    auto* cursor = reinterpret_cast<unsigned long long*>(mem + cur_off);
     auto* tuples = reinterpret_cast<uint64_t*>(mem + tup_off);
+    auto* pays = reinterpret_cast<int32_t*>(mem + pay_off);
     auto* spill = reinterpret_cast<uint64_t*>(mem + spill_off);
-    const int rsm = static_cast<int>(sizeof(unsigned long long) * olap::kSmemRegionSlots);
-    const int ssm = static_cast<int>((sizeof(unsigned long long) + sizeof(unsigned int)) * P);
+    uint64_t* taken = tuples;  // free once the region build has read it
+    const int rsm = static_cast<int>(3 * sizeof(uint32_t) * olap::kSmemRegionSlots +
+                                     2 * sizeof(uint32_t) * olap::kSmemFilterWords);
+    // sorted tile (tuple, payload, region: 14 B a row), then 12 B a region
+    const int ssm = static_cast<int>(14 * olap::kSmemTileRows + 12 * P);
     OLAP_CUDA_TRY(ctx, cudaMemsetAsync(mem, 0, cnt_bytes, ctx->stream));
     OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::smem_region_build_kernel,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, rsm));
-    if (ssm > 48 * 1024)
-      OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::smem_region_scatter_kernel,
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize, ssm));
-    olap::smem_region_count_kernel<<<nb, olap::kBuildPartThreads, sizeof(unsigned int) * P, ctx->stream>>>(
-        keys, n, per, cap, P, vec, counts, &ctx->counters->range_errors);
+    OLAP_CUDA_TRY(ctx, cudaFuncSetAttribute(olap::smem_region_scatter_kernel,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, ssm));
+    olap::smem_region_count_kernel<<<nb, olap::kSmemRegionThreads, sizeof(unsigned int) * P, ctx->stream>>>(
+        keys, n, per, cap32, P, vec_k, counts, &ctx->counters->range_errors);
     olap::smem_region_scan_kernel<<<1, 1024, 0, ctx->stream>>>(counts, P, begin, cursor);
-    olap::smem_region_scatter_kernel<<<nb, olap::kBuildPartThreads, ssm, ctx->stream>>>(keys, n, per, cap, P, vec,
-                                                                                       cursor, tuples);
-    olap::smem_region_build_kernel<<<P, olap::kSmemRegionThreads, rsm, ctx->stream>>>(tuples, begin, table, cap,
-                                                                                      payload, spill, n_spill);
+    olap::smem_region_scatter_kernel<<<nb, olap::kSmemRegionThreads, ssm, ctx->stream>>>(
+        keys, payload, n, cap32, P, vec_k, vec_p, cursor, tuples, pays);
+    olap::smem_region_build_kernel<<<P, olap::kSmemRegionThreads, rsm, ctx->stream>>>(
+        tuples, pays, begin, table, cap32, spill, n_spill, fused_filter ? filter : nullptr, fshift);
     const unsigned sg = static_cast<unsigned>(ctx->sm_count) * 4;
-    olap::smem_region_spill_kernel<<<sg, 256, 0, ctx->stream>>>(spill, n_spill, table, cap, tuples, n_taken,
+    olap::smem_region_spill_kernel<<<sg, 256, 0, ctx->stream>>>(spill, n_spill, table, cap, taken, n_taken,
                                                                 overflow);
-    olap::smem_region_taken_kernel<<<sg, 256, 0, ctx->stream>>>(tuples, n_taken, table, payload);
+    olap::smem_region_taken_kernel<<<sg, 256, 0, ctx->stream>>>(taken, n_taken, table, payload);
   } else if (n && partitioned) {
     olap::fill_u64_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity,
                                                                                        olap::kEmptySlot);
@@ -951,12 +1197,34 @@ int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* paylo
         keys, n, table, static_cast<uint64_t>(capacity), &ctx->counters->range_errors, overflow);
     olap::hash_finish_kernel<<<olap::grid_for(ctx, capacity, 256), 256, 0, ctx->stream>>>(table, capacity, payload);
   }
+  if (filter && !fused_filter && n)
+    olap::bloom_build_kernel<<<olap::grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(keys, n, filter, fshift);
   OLAP_CUDA_TRY(ctx, cudaGetLastError());
   unsigned long long ov = 0;
   OLAP_CUDA_TRY(ctx, cudaMemcpyAsync(&ov, overflow, sizeof(ov), cudaMemcpyDeviceToHost, ctx->stream));
   OLAP_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (ov) return olap::set_error(ctx, OLAP_ERR_CAPACITY, "hash table full");
   return OLAP_OK;
+}
+
+}  // namespace
+}  // namespace olap
+
+extern "C" {
+
+int olap_hashjoin_build(olap_ctx* ctx, const int32_t* keys, const int32_t* payload, int64_t n,
+                        uint64_t* table, int64_t capacity) {
+  if (!ctx) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return olap::hashjoin_build_locked(ctx, keys, payload, n, table, capacity, nullptr, 0);
+}
+
+int olap_hashjoin_build_filtered(olap_ctx* ctx, const int32_t* keys, const int32_t* payload, int64_t n,
+                                 uint64_t* table, int64_t capacity, uint64_t* filter, int64_t words) {
+  if (!ctx) return OLAP_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  OLAP_REQUIRE(ctx, filter, "null filter (olap_hashjoin_build builds the table alone)");
+  return olap::hashjoin_build_locked(ctx, keys, payload, n, table, capacity, filter, words);
 }
 
 int64_t olap_hashjoin_filter_words(int64_t n_build) {

@@ -160,10 +160,12 @@ class HashTable:
 
     def build(self, keys, payload) -> "HashTable":
         c = _ctx(self.ctx)
-        check(lib.olap_hashjoin_build(c.handle, _ptr(keys), _ptr(payload), _nelem(keys), _ptr(self.table),
-                                      self.capacity), c.handle)
-        if self.filter is not None:
-            check(lib.olap_hashjoin_build_filter(c.handle, _ptr(keys), _nelem(keys), _ptr(self.filter), self.words),
+        if self.filter is None:
+            check(lib.olap_hashjoin_build(c.handle, _ptr(keys), _ptr(payload), _nelem(keys), _ptr(self.table),
+                                          self.capacity), c.handle)
+        else:  # table and filter in one call
+            check(lib.olap_hashjoin_build_filtered(c.handle, _ptr(keys), _ptr(payload), _nelem(keys),
+                                                   _ptr(self.table), self.capacity, _ptr(self.filter), self.words),
                   c.handle)
         return self
 

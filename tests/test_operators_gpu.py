@@ -500,3 +500,50 @@ def test_hash_join_region_build(ctx, mode):
     rows, pay = ht.probe_pairs(dev(sk[:300_000]))
     _, _, erows, epay = oracle.hashjoin(rk, rp, sk[:300_000], want_pairs=True)
     assert np.array_equal(host(rows), erows) and np.array_equal(host(pay), epay)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [0, 2, 3])
+@pytest.mark.parametrize("words", ["default", "one", "wide"])
+def test_hash_join_build_filtered_matches_two_calls(ctx, mode, words):
+    """olap_hashjoin_build_filtered gives the filter words, bit for bit, and
+    the full slots that olap_hashjoin_build followed by
+    olap_hashjoin_build_filter give: on the shared-memory region build (mode
+    0, where the region blocks set the filter bits; with one filter word, and
+    with a filter too wide for a region's run of words, which falls back to
+    the separate pass), directly (2) and by L2 regions (3).  A table of a
+    capacity that is not a power of two, duplicates, the reserved key."""
+    L, h = _lib.lib, ctx.handle
+    rng = np.random.default_rng(47)
+    n = (1 << 21) + 12_345
+    rk = rng.integers(-(1 << 22), 1 << 22, n).astype(np.int32)
+    rk[::70_001] = np.iinfo(np.int32).min
+    rp = rng.integers(-(1 << 31), 1 << 31, n).astype(np.int32)
+    cap = int(L.olap_hashtable_capacity(n))
+    assert cap > 1 << 22 and cap & (cap - 1)
+    w = {"default": int(L.olap_hashjoin_filter_words(n)), "one": 1, "wide": 1 << 20}[words]
+    drk, drp = dev(rk), dev(rp)
+    ta = torch.empty(cap, dtype=torch.int64, device="cuda")
+    tb = torch.empty(cap, dtype=torch.int64, device="cuda")
+    fa = torch.empty(w, dtype=torch.int64, device="cuda")
+    fb = torch.empty(w, dtype=torch.int64, device="cuda")
+    ctx.set_tuning(_lib.TUNE_JOIN_BUILD, mode)
+    try:
+        _lib.check(L.olap_hashjoin_build_filtered(h, drk.data_ptr(), drp.data_ptr(), n, ta.data_ptr(), cap,
+                                                  fa.data_ptr(), w), h)
+        _lib.check(L.olap_hashjoin_build(h, drk.data_ptr(), drp.data_ptr(), n, tb.data_ptr(), cap), h)
+        _lib.check(L.olap_hashjoin_build_filter(h, drk.data_ptr(), n, fb.data_ptr(), w), h)
+        torch.cuda.synchronize()
+    finally:
+        ctx.set_tuning(_lib.TUNE_JOIN_BUILD, 0)
+    assert ctx.take_range_errors() == 2 * int((rk == np.iinfo(np.int32).min).sum())
+    assert torch.equal(fa, fb)
+    empty = np.int64(np.uint64(0x80000000FFFFFFFF).astype(np.int64))
+    sa, sb = host(ta), host(tb)
+    assert np.array_equal(np.sort(sa[sa != empty]), np.sort(sb[sb != empty]))
+    sk = rng.integers(-(1 << 22), 1 << 22, 1 << 22).astype(np.int32)
+    s_, m_ = torch.zeros(1, dtype=torch.int64, device="cuda"), torch.zeros(1, dtype=torch.int64, device="cuda")
+    dsk = dev(sk)
+    _lib.check(L.olap_hashjoin_probe_filtered(h, ta.data_ptr(), cap, fa.data_ptr(), w, dsk.data_ptr(), len(sk),
+                                              s_.data_ptr(), m_.data_ptr(), None, None), h)
+    assert (int(s_.item()), int(m_.item())) == oracle.hashjoin(rk, rp, sk)

@@ -445,14 +445,6 @@ __global__ void __launch_bounds__(1024) smem_region_scan_kernel(const unsigned i
   if (threadIdx.x == blockDim.x - 1) begin[n_regions] = s_run[threadIdx.x];
 }
 
-// Asks L2 to fetch the 16-byte aligned part of [p, p + bytes) ahead of the
-// loads that will read it (a bulk prefetch has no destination registers).
-__device__ __forceinline__ void prefetch_l2_range(const void* p, uint64_t bytes) {
-  const uint64_t a = (reinterpret_cast<uint64_t>(p) + 15) & ~uint64_t(15);
-  const uint64_t z = (reinterpret_cast<uint64_t>(p) + bytes) & ~uint64_t(15);
-  if (z > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(static_cast<uint32_t>(z - a)) : "memory");
-}
-
 // Scatter of the (key << 32 | row) tuples and their payloads by region (rows
 // with the key INT32_MIN are range errors and dropped).  A block takes its
 // rows a tile of 8,192 at a time: counting-sorts the tile by region in shared

@@ -164,6 +164,14 @@ __device__ __forceinline__ uint64_t policy_evict_last() {
 }
 
 // 128-bit streaming load: read-only path, no L1 allocation, L2 evict-first.
+// Asks L2 to fetch the 16-byte aligned part of [p, p + bytes) ahead of the
+// loads that will read it (a bulk prefetch has no destination registers).
+__device__ __forceinline__ void prefetch_l2_range(const void* p, uint64_t bytes) {
+  const uint64_t a = (reinterpret_cast<uint64_t>(p) + 15) & ~uint64_t(15);
+  const uint64_t z = (reinterpret_cast<uint64_t>(p) + bytes) & ~uint64_t(15);
+  if (z > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(static_cast<uint32_t>(z - a)) : "memory");
+}
+
 __device__ __forceinline__ int4 ld_stream_v4(const int32_t* p, uint64_t pol) {
   int4 v;
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"

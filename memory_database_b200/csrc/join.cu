@@ -351,10 +351,10 @@ __global__ void build_insert_kernel(const uint64_t* __restrict__ tuples, const l
 // region's rows with shared-memory atomics, then writes the whole region
 // (empty slots too) with the payloads already in place, so the table needs no
 // separate fill or finish pass, every slot crosses DRAM once and no payload
-// is read at random.  A row whose probe run would leave its region (every slot from
-// its home to the region's end taken) is set aside and inserted afterwards
-// into the finished table from the next region's first slot on, exactly where
-// linear probing over the whole table would have put it.
+// is read at random.  A row whose probe run would leave its region (every
+// slot from its home to the region's end taken) is set aside and inserted
+// afterwards into the finished table from the next region's first slot on,
+// where linear probing over the whole table finds it.
 constexpr int kSmemRegionSlots = 16384;
 constexpr int kSmemRegionShift = 14;
 constexpr int64_t kSmemRegionMaxRegions = 8192;

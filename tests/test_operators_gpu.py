@@ -503,6 +503,29 @@ def test_hash_join_region_build(ctx, mode):
 
 
 @pytest.mark.gpu
+def test_hash_join_region_build_heavy_duplicates(ctx):
+    """Half of 2^21 + 1,000 build rows share one key, so one 16,384-slot region of
+    the shared-memory build holds a million rows (its block works through
+    them in many rounds and then settles the duplicate's payload), and the
+    rest are 1,000 keys repeated about a thousand times each: every key
+    keeps the payload of its last row, through the filter or not."""
+    rng = np.random.default_rng(53)
+    n = (1 << 21) + 1000  # a table just above 2^22 slots: the shared-memory build
+    rk = rng.integers(-500, 500, n).astype(np.int32)
+    rk[rng.permutation(n)[: n // 2]] = 123_456_789
+    rp = rng.integers(-(1 << 31), 1 << 31, n).astype(np.int32)
+    sk = np.concatenate([np.arange(-600, 600, dtype=np.int32), np.full(1000, 123_456_789, np.int32),
+                         rng.integers(-700, 700, 1 << 20).astype(np.int32)])
+    for bloom in (True, False):
+        ht = ops.HashTable(n, ctx=ctx, bloom=bloom).build(dev(rk), dev(rp))
+        assert ht.capacity > 1 << 22
+        assert ht.probe(dev(sk)) == oracle.hashjoin(rk, rp, sk)
+        rows, pay = ht.probe_pairs(dev(sk[:5000]))
+        _, _, erows, epay = oracle.hashjoin(rk, rp, sk[:5000], want_pairs=True)
+        assert np.array_equal(host(rows), erows) and np.array_equal(host(pay), epay)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("mode", [0, 2, 3])
 @pytest.mark.parametrize("words", ["default", "one", "wide"])
 def test_hash_join_build_filtered_matches_two_calls(ctx, mode, words):

@@ -163,7 +163,9 @@ __global__ void hash_finish_kernel(uint64_t* __restrict__ slots, int64_t cap, co
   }
 }
 
-// ---- partitioned build ------------------------------------------------------
+// ---- partitioned build in L2 -------------------------------------------------
+// (Tables above 2^27 slots, which the shared-memory build below does not
+// take, or any table above 32 MB with OLAP_TUNE_JOIN_BUILD = 3.)
 // A table larger than L2 takes one random DRAM sector per CAS.  For such
 // tables the build rows are first scattered by the region of the table their
 // home slot falls in (regions of kBuildRegionSlots slots, 32 MB, which L2
